@@ -1,0 +1,149 @@
+/* p3mg — P3M electrostatics on one NVIDIA B200 (sm_100a), C ABI.
+ *
+ * Drop-in GPU replacement for the k-space force path and the real-space
+ * pair loop of the p3m-standalone program.  The reference's plugin table is
+ *   method_t { id, name, short_name, flags, Init, Influence_function,
+ *              Kspace_force, Error, Error_k }          (types.h:306-316)
+ * with the methods registered under ids 0/1/2/3/6/7 (p3m-ik.c:46-49,
+ * p3m-ik-i.c:40-43, p3m-ad.c:39-41, p3m-ad-i.c:39-41, p3m-ik-real.c:43-46,
+ * p3m-ad-real.c:39-41).  Each entry below names the reference interface it
+ * replaces.  Conventions:
+ *   - every function returns a status: P3MG_OK (0) or a negative P3MG_ERR_*;
+ *     the library never calls exit() (the reference does: parameters.c:137,
+ *     io.c:81-84, main.c:341-344);
+ *   - particle data are caller-owned SoA host arrays of doubles, one array
+ *     per coordinate (the reference's vector_array_t fields, types.h:126-132);
+ *   - force outputs ACCUMULATE (+=) exactly like Kspace_force and Realteil;
+ *   - a context owns all device memory and one CUDA stream; contexts are
+ *     independent, a single context is not re-entrant.
+ */
+#ifndef P3MG_H
+#define P3MG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* status codes */
+#define P3MG_OK 0
+#define P3MG_ERR_ARG (-1)       /* NULL pointer, n < 0, L <= 0, ... */
+#define P3MG_ERR_METHOD (-2)    /* method id not in {0,1,2,3,6,7} (main.c:341-344 exits 126) */
+#define P3MG_ERR_CAO (-3)       /* cao not in 1..7 (charge-assign.c:209-211 prints and skips) */
+#define P3MG_ERR_MESH (-4)      /* mesh < max(cao,4), > 512, prime factor > 7, or odd for methods 6/7 */
+#define P3MG_ERR_NOSYS (-5)     /* no particles set yet */
+#define P3MG_ERR_CUDA (-6)      /* CUDA runtime error (see p3mg_last_cuda_error) */
+#define P3MG_ERR_ALLOC (-7)     /* device allocation failed */
+#define P3MG_ERR_STATE (-8)     /* influence function not computed for this context */
+#define P3MG_ERR_PRECISION (-9) /* unknown precision mode */
+#define P3MG_ERR_NOBUF (-10)    /* capacity of a caller-provided buffer exceeded */
+
+/* precision modes */
+#define P3MG_FP64 0       /* everything in FP64: parity path (<= 1e-10 relative RMS vs the reference) */
+#define P3MG_FP32_MIXED 1 /* FP32 mesh, FFTs, weights and pair forces; FP64 G_opt, self-force and geometry */
+
+/* method ids: the reference's enum (types.h:109-118) */
+#define P3MG_METHOD_IK 0
+#define P3MG_METHOD_IK_I 1
+#define P3MG_METHOD_AD 2
+#define P3MG_METHOD_AD_I 3
+#define P3MG_METHOD_IK_R 6
+#define P3MG_METHOD_AD_R 7
+
+typedef struct p3mg_ctx p3mg_ctx;
+
+/* Create a context on the current CUDA device for one method and mesh.
+ * mc is the aliasing-sum range P3M_BRILLOUIN (p3m-common.c:33, CLI "mc").
+ * Replaces method.Init (e.g. Init_ik p3m-ik.c:75-90, Init_ad_r
+ * p3m-ad-real.c:54-67) and Init_data (p3m-common.c:145-232). */
+int p3mg_create(p3mg_ctx **ctx, int method_id, int mesh, int cao, int mc, int precision);
+
+/* Release all device memory of the context (Free_data, p3m-common.c:234). */
+void p3mg_destroy(p3mg_ctx *ctx);
+
+/* Load n particles (host arrays) and the box length.  Positions are
+ * expected in [0, L) like the reference's (charge-assign.c:37-40); other
+ * values are folded into the box.  Replaces filling system_t (types.h:163-183). */
+int p3mg_set_system(p3mg_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *q,
+                    double L);
+
+/* Same with DEVICE pointers (on the context's device); the data are copied
+ * into the context on its stream. */
+int p3mg_set_system_device(p3mg_ctx *ctx, int n, const double *x, const double *y, const double *z,
+                           const double *q, double L);
+
+/* Optimal influence function G_opt for this alpha on the GPU in FP64, and
+ * for methods 2 and 7 the ad self-force coefficients.  Replaces
+ * method.Influence_function (p3m-ik.c:135-173, p3m-ik-i.c:126-166,
+ * p3m-ad.c:111-158 + p3m-ad-self-forces.c:93-112, p3m-ad-i.c:121-150). */
+int p3mg_influence(p3mg_ctx *ctx, double alpha);
+
+/* k-space forces accumulated into fk (+=); for methods 2 and 7 the
+ * self-force correction is subtracted from ft (may be NULL to skip).
+ * Replaces method.Kspace_force (P3M_ik p3m-ik.c:179-245, P3M_ik_i
+ * p3m-ik-i.c:169-246, P3M_ad p3m-ad.c:161-210, P3M_ad_i p3m-ad-i.c:153-203,
+ * P3M_ik_r p3m-ik-real.c:83-147, P3M_ad_r p3m-ad-real.c:69-118). */
+int p3mg_kspace_forces(p3mg_ctx *ctx, double *fk_x, double *fk_y, double *fk_z, double *ft_x, double *ft_y,
+                       double *ft_z);
+
+/* Real-space erfc pair forces for all ordered pairs i != j with
+ * minimum-image distance <= rcut, accumulated into fr (+=); *energy
+ * (may be NULL) receives the pair energy sum 1/2 q_i q_j erfc(alpha r)/r.
+ * Replaces Realteil (realpart.c:124-167). */
+int p3mg_real_forces(p3mg_ctx *ctx, double rcut, double alpha, double *fr_x, double *fr_y, double *fr_z,
+                     double *energy);
+
+/* One force evaluation exactly like Calculate_forces (common.c:268-327):
+ * f, f_k and f_r are ZEROED, then real space (skipped when rcut == 0),
+ * k-space and self-force, then f += f_k + f_r.  Any of fk_*, fr_* may be
+ * NULL; f_* may not.  Uses the alpha of the last p3mg_influence. */
+int p3mg_calculate_forces(p3mg_ctx *ctx, double rcut, double *f_x, double *f_y, double *f_z, double *fk_x,
+                          double *fk_y, double *fk_z, double *fr_x, double *fr_y, double *fr_z, double *energy);
+
+/* The same step with inputs and outputs resident in device memory: runs
+ * on the context's stream and returns without synchronising.  Results are
+ * read with p3mg_get_forces / p3mg_get_forces_device. */
+int p3mg_compute(p3mg_ctx *ctx, double rcut);
+
+/* Copy the forces of the last p3mg_compute to host arrays (any may be NULL). */
+int p3mg_get_forces(p3mg_ctx *ctx, double *f_x, double *f_y, double *f_z, double *fk_x, double *fk_y,
+                    double *fk_z, double *fr_x, double *fr_y, double *fr_z, double *energy);
+
+/* Device pointers to the context's force arrays (3n doubles each: x block,
+ * y block, z block), valid until the next p3mg_set_system or p3mg_destroy. */
+int p3mg_get_forces_device(p3mg_ctx *ctx, const double **f, const double **fk, const double **fr);
+
+/* Stage times of the last step in milliseconds, measured with CUDA events
+ * on the context's stream: t[0] charge assignment, t[1] FFTs and
+ * convolution, t[2] force assignment and self-force, t[3] real space.
+ * Mirrors the reference's tuning timers t_c/t_g/t_f (p3m-common.h:48-57).
+ * Stage timing is on only after p3mg_enable_timing(ctx, 1). */
+int p3mg_enable_timing(p3mg_ctx *ctx, int on);
+int p3mg_stage_times(p3mg_ctx *ctx, double t[4]);
+
+/* Copy the FP64 influence function (mesh^3 doubles, full mesh, index
+ * (i*mesh + j)*mesh + k as r_ind, p3m-common.h:25) and the 81 ad self-force
+ * coefficients (zeros for other methods) to host memory; either may be NULL. */
+int p3mg_get_influence(p3mg_ctx *ctx, double *G, double *self_coeffs81);
+
+/* The context's CUDA stream (cudaStream_t) as an opaque pointer. */
+void *p3mg_stream(p3mg_ctx *ctx);
+
+/* Human-readable text for a status code. */
+const char *p3mg_strerror(int status);
+
+/* Text of the last CUDA runtime error seen by any context ("" if none). */
+const char *p3mg_last_cuda_error(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* P3MG_H */

@@ -1,0 +1,441 @@
+// C ABI of the p3mg library (declared in include/p3mg.h): context
+// lifecycle, host/device particle I/O and the step orchestration that
+// mirrors Calculate_forces (common.c:268-327).
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "p3mg_internal.cuh"
+
+namespace p3mg {
+
+static char g_last_cuda_error[256] = "";
+
+void record_cuda_error(cudaError_t e) {
+  snprintf(g_last_cuda_error, sizeof(g_last_cuda_error), "%s: %s", cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+int fft_factor(int m, int *radix, int *npass);
+
+namespace {
+
+__global__ void combine_kernel(double *__restrict__ f, const double *__restrict__ fk, const double *__restrict__ fr,
+                               size_t n3) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n3) f[t] += fk[t] + fr[t];
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+}  // namespace
+
+int zero_forces(Ctx *c) {
+  const size_t b = 3 * (size_t)c->n * sizeof(double);
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->f, 0, b, c->stream));
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->fk, 0, b, c->stream));
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->fr, 0, b, c->stream));
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->energy, 0, 2 * sizeof(double), c->stream));
+  return P3MG_OK;
+}
+
+int combine_forces(Ctx *c) {
+  const size_t n3 = 3 * (size_t)c->n;
+  if (n3 == 0) return P3MG_OK;
+  combine_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, c->stream>>>(c->f, c->fk, c->fr, n3);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
+int alloc_system(Ctx *c, int n) {
+  if (n <= c->cap && c->x) {
+    c->n = n;
+    return P3MG_OK;
+  }
+  dfree(c->x);
+  dfree(c->y);
+  dfree(c->z);
+  dfree(c->q);
+  dfree(c->f);
+  dfree(c->fk);
+  dfree(c->fr);
+  dfree(c->part_key);
+  dfree(c->sorted_idx);
+  dfree(c->sorted_xyzq);
+  dfree(c->cell_key);
+  dfree(c->cell_idx);
+  dfree(c->cell_pos);
+  const size_t cap = (size_t)(n > 0 ? n : 1);
+  P3MG_CUDA_TRY(cudaMalloc(&c->x, cap * sizeof(double)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->y, cap * sizeof(double)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->z, cap * sizeof(double)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->q, cap * sizeof(double)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->f, 3 * cap * sizeof(double)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->fk, 3 * cap * sizeof(double)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->fr, 3 * cap * sizeof(double)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->part_key, cap * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->sorted_idx, cap * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->sorted_xyzq, cap * sizeof(double4)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->cell_key, cap * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->cell_idx, cap * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->cell_pos, cap * sizeof(double4)));
+  c->cap = (int)cap;
+  c->n = n;
+  return P3MG_OK;
+}
+
+int free_all(Ctx *c) {
+  dfree(c->x);
+  dfree(c->y);
+  dfree(c->z);
+  dfree(c->q);
+  dfree(c->f);
+  dfree(c->fk);
+  dfree(c->fr);
+  dfree(c->energy);
+  dfree(c->brick_count);
+  dfree(c->brick_start);
+  dfree(c->brick_fill);
+  dfree(c->part_key);
+  dfree(c->sorted_idx);
+  dfree(c->sorted_xyzq);
+  dfree(c->cell_count);
+  dfree(c->cell_start);
+  dfree(c->cell_fill);
+  dfree(c->cell_key);
+  dfree(c->cell_idx);
+  dfree(c->cell_pos);
+  dfree(c->Q);
+  dfree(c->F);
+  dfree(c->G);
+  dfree(c->G32);
+  dfree(c->self_b);
+  dfree(c->scan_tmp);
+  fft_plan_free(c);
+  if (c->ev_ok)
+    for (int i = 0; i < 5; i++) cudaEventDestroy(c->ev[i]);
+  c->ev_ok = false;
+  if (c->stream) cudaStreamDestroy(c->stream);
+  c->stream = nullptr;
+  return P3MG_OK;
+}
+
+static int step_device(Ctx *c, double rcut) {
+  P3MG_TRY(zero_forces(c));
+  if (c->timing && c->ev_ok) cudaEventRecord(c->ev[4], c->stream);
+  // real space when rcut != 0 (common.c:290-294)
+  if (rcut != 0.0) P3MG_TRY(pairs_run(c, rcut, c->alpha));
+  if (c->n > 0) {
+    P3MG_TRY(kspace_prepare(c));
+    P3MG_TRY(kspace_run(c));
+  }
+  P3MG_TRY(combine_forces(c));
+  c->stage_pending = c->timing && c->ev_ok;
+  return P3MG_OK;
+}
+
+static void collect_stage_times(Ctx *c) {
+  if (!c->stage_pending) return;
+  cudaEventSynchronize(c->ev[3]);
+  float t;
+  // ev[4] start of pairs, ev[0] start of scatter (after binning), ev[1] end
+  // of scatter, ev[2] end of FFT/convolution, ev[3] end of gather
+  if (cudaEventElapsedTime(&t, c->ev[4], c->ev[0]) == cudaSuccess) c->stage_ms[3] = t;
+  if (cudaEventElapsedTime(&t, c->ev[0], c->ev[1]) == cudaSuccess) c->stage_ms[0] = t;
+  if (cudaEventElapsedTime(&t, c->ev[1], c->ev[2]) == cudaSuccess) c->stage_ms[1] = t;
+  if (cudaEventElapsedTime(&t, c->ev[2], c->ev[3]) == cudaSuccess) c->stage_ms[2] = t;
+  c->stage_pending = false;
+}
+
+static int check_ctx(Ctx *c) {
+  if (!c) return P3MG_ERR_ARG;
+  return P3MG_OK;
+}
+
+}  // namespace p3mg
+
+using namespace p3mg;
+
+struct p3mg_ctx {
+  Ctx c;
+};
+
+extern "C" {
+
+const char *p3mg_strerror(int s) {
+  switch (s) {
+    case P3MG_OK: return "ok";
+    case P3MG_ERR_ARG: return "invalid argument";
+    case P3MG_ERR_METHOD: return "unknown method id (supported: 0, 1, 2, 3, 6, 7)";
+    case P3MG_ERR_CAO: return "charge assignment order must be 1..7";
+    case P3MG_ERR_MESH: return "unsupported mesh size (need max(cao,4) <= mesh <= 512, prime factors 2,3,5,7, even for methods 6/7)";
+    case P3MG_ERR_NOSYS: return "no particles set";
+    case P3MG_ERR_CUDA: return "CUDA runtime error";
+    case P3MG_ERR_ALLOC: return "device memory allocation failed";
+    case P3MG_ERR_STATE: return "influence function not computed (call p3mg_influence first)";
+    case P3MG_ERR_PRECISION: return "unknown precision mode";
+    case P3MG_ERR_NOBUF: return "buffer capacity exceeded";
+  }
+  return "unknown status";
+}
+
+const char *p3mg_last_cuda_error(void) { return g_last_cuda_error; }
+
+int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int precision) {
+  if (!out) return P3MG_ERR_ARG;
+  *out = nullptr;
+  if (!(method_id == 0 || method_id == 1 || method_id == 2 || method_id == 3 || method_id == 6 || method_id == 7))
+    return P3MG_ERR_METHOD;
+  if (cao < 1 || cao > P3MG_MAX_CAO) return P3MG_ERR_CAO;
+  if (precision != P3MG_FP64 && precision != P3MG_FP32_MIXED) return P3MG_ERR_PRECISION;
+  if (mc < 0) return P3MG_ERR_ARG;
+  int rad[24], np;
+  if (mesh < 4 || mesh < cao || mesh > P3MG_MAX_MESH || fft_factor(mesh, rad, &np) != 0) return P3MG_ERR_MESH;
+  if ((method_id == 6 || method_id == 7) && (mesh % 2)) return P3MG_ERR_MESH;
+  p3mg_ctx *h = new (std::nothrow) p3mg_ctx();
+  if (!h) return P3MG_ERR_ALLOC;
+  Ctx *c = &h->c;
+  c->method = method_id;
+  c->mesh = mesh;
+  c->cao = cao;
+  c->mc = mc;
+  c->precision = precision;
+  c->M = (size_t)mesh * mesh * mesh;
+  int st = P3MG_OK;
+  do {
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) {
+      record_cuda_error(e);
+      st = P3MG_ERR_CUDA;
+      break;
+    }
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      record_cuda_error(e);
+      st = P3MG_ERR_CUDA;
+      break;
+    }
+    const size_t csz = (precision == P3MG_FP64) ? sizeof(double2) : sizeof(float2);
+    // brick edge for the tiled charge assignment
+    c->brick = (mesh >= 64) ? 8 : 4;
+    c->nbrick1 = (mesh + c->brick - 1) / c->brick;
+    const int nbr = c->nbrick1 * c->nbrick1 * c->nbrick1;
+#define ALLOC(ptr, bytes)                              \
+  e = cudaMalloc((void **)&(ptr), (bytes));            \
+  if (e != cudaSuccess) {                              \
+    record_cuda_error(e);                              \
+    st = P3MG_ERR_ALLOC;                               \
+    break;                                             \
+  }
+    ALLOC(c->Q, c->M * csz);
+    if (!method_ad(method_id)) {
+      ALLOC(c->F, 3 * c->M * csz);
+    }
+    ALLOC(c->G, c->M * sizeof(double));
+    if (precision != P3MG_FP64) {
+      ALLOC(c->G32, c->M * sizeof(float));
+    }
+    ALLOC(c->self_b, 81 * sizeof(double));
+    ALLOC(c->energy, 2 * sizeof(double));
+    ALLOC(c->brick_count, nbr * sizeof(int));
+    ALLOC(c->brick_start, (nbr + 1) * sizeof(int));
+    ALLOC(c->brick_fill, nbr * sizeof(int));
+#undef ALLOC
+    cudaMemset(c->self_b, 0, 81 * sizeof(double));
+    memset(c->self_b_host, 0, sizeof(c->self_b_host));
+    st = fft_plan_init(c);
+    if (st != P3MG_OK) break;
+    c->ev_ok = true;
+    for (int i = 0; i < 5; i++)
+      if (cudaEventCreate(&c->ev[i]) != cudaSuccess) c->ev_ok = false;
+  } while (0);
+  if (st != P3MG_OK) {
+    free_all(c);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return P3MG_OK;
+}
+
+void p3mg_destroy(p3mg_ctx *h) {
+  if (!h) return;
+  cudaSetDevice(h->c.device);
+  if (h->c.stream) cudaStreamSynchronize(h->c.stream);
+  free_all(&h->c);
+  delete h;
+}
+
+static int set_system_common(Ctx *c, int n, const double *x, const double *y, const double *z, const double *q,
+                             double L, cudaMemcpyKind kind) {
+  if (n < 0 || !(L > 0.0) || !isfinite(L)) return P3MG_ERR_ARG;
+  if (n > 0 && (!x || !y || !z || !q)) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  P3MG_TRY(alloc_system(c, n));
+  c->L = L;
+  const size_t b = (size_t)n * sizeof(double);
+  if (n > 0) {
+    P3MG_CUDA_TRY(cudaMemcpyAsync(c->x, x, b, kind, c->stream));
+    P3MG_CUDA_TRY(cudaMemcpyAsync(c->y, y, b, kind, c->stream));
+    P3MG_CUDA_TRY(cudaMemcpyAsync(c->z, z, b, kind, c->stream));
+    P3MG_CUDA_TRY(cudaMemcpyAsync(c->q, q, b, kind, c->stream));
+  }
+  c->have_G = false;  // G depends on L
+  return P3MG_OK;
+}
+
+int p3mg_set_system(p3mg_ctx *h, int n, const double *x, const double *y, const double *z, const double *q, double L) {
+  if (!h) return P3MG_ERR_ARG;
+  return set_system_common(&h->c, n, x, y, z, q, L, cudaMemcpyHostToDevice);
+}
+
+int p3mg_set_system_device(p3mg_ctx *h, int n, const double *x, const double *y, const double *z, const double *q,
+                           double L) {
+  if (!h) return P3MG_ERR_ARG;
+  return set_system_common(&h->c, n, x, y, z, q, L, cudaMemcpyDeviceToDevice);
+}
+
+int p3mg_influence(p3mg_ctx *h, double alpha) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!isfinite(alpha) || alpha < 0.0) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  return influence_compute(c, alpha);
+}
+
+static int copy_out3(Ctx *c, const double *src, double *hx, double *hy, double *hz, bool accumulate) {
+  const size_t n = (size_t)c->n;
+  if (n == 0) return P3MG_OK;
+  double *dst[3] = {hx, hy, hz};
+  if (!accumulate) {
+    for (int d = 0; d < 3; d++)
+      if (dst[d]) P3MG_CUDA_TRY(cudaMemcpyAsync(dst[d], src + d * n, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return P3MG_OK;
+  }
+  double *tmp = (double *)malloc(3 * n * sizeof(double));
+  if (!tmp) return P3MG_ERR_ALLOC;
+  cudaError_t e = cudaMemcpyAsync(tmp, src, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    free(tmp);
+    record_cuda_error(e);
+    return P3MG_ERR_CUDA;
+  }
+  for (int d = 0; d < 3; d++)
+    if (dst[d])
+      for (size_t i = 0; i < n; i++) dst[d][i] += tmp[d * n + i];
+  free(tmp);
+  return P3MG_OK;
+}
+
+int p3mg_kspace_forces(p3mg_ctx *h, double *fk_x, double *fk_y, double *fk_z, double *ft_x, double *ft_y,
+                       double *ft_z) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (c->n > 0 && (!fk_x || !fk_y || !fk_z)) return P3MG_ERR_ARG;
+  if (!c->have_G) return P3MG_ERR_STATE;
+  cudaSetDevice(c->device);
+  P3MG_TRY(zero_forces(c));
+  if (c->n > 0) {
+    P3MG_TRY(kspace_prepare(c));
+    P3MG_TRY(kspace_run(c));
+  }
+  collect_stage_times(c);
+  P3MG_TRY(copy_out3(c, c->fk, fk_x, fk_y, fk_z, true));
+  if (method_self_force(c->method) && (ft_x || ft_y || ft_z)) P3MG_TRY(copy_out3(c, c->f, ft_x, ft_y, ft_z, true));
+  return P3MG_OK;
+}
+
+int p3mg_real_forces(p3mg_ctx *h, double rcut, double alpha, double *fr_x, double *fr_y, double *fr_z,
+                     double *energy) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (c->n > 0 && (!fr_x || !fr_y || !fr_z)) return P3MG_ERR_ARG;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!(rcut >= 0.0) || !(alpha >= 0.0)) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  P3MG_TRY(zero_forces(c));
+  P3MG_TRY(pairs_run(c, rcut, alpha));
+  P3MG_TRY(copy_out3(c, c->fr, fr_x, fr_y, fr_z, true));
+  if (energy) {
+    double e;
+    P3MG_CUDA_TRY(cudaMemcpy(&e, c->energy, sizeof(double), cudaMemcpyDeviceToHost));
+    *energy += e;
+  }
+  return P3MG_OK;
+}
+
+int p3mg_compute(p3mg_ctx *h, double rcut) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!c->have_G) return P3MG_ERR_STATE;
+  if (!(rcut >= 0.0)) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  return step_device(c, rcut);
+}
+
+int p3mg_get_forces(p3mg_ctx *h, double *f_x, double *f_y, double *f_z, double *fk_x, double *fk_y, double *fk_z,
+                    double *fr_x, double *fr_y, double *fr_z, double *energy) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  cudaSetDevice(c->device);
+  collect_stage_times(c);
+  P3MG_TRY(copy_out3(c, c->f, f_x, f_y, f_z, false));
+  P3MG_TRY(copy_out3(c, c->fk, fk_x, fk_y, fk_z, false));
+  P3MG_TRY(copy_out3(c, c->fr, fr_x, fr_y, fr_z, false));
+  if (energy) P3MG_CUDA_TRY(cudaMemcpy(energy, c->energy, sizeof(double), cudaMemcpyDeviceToHost));
+  return P3MG_OK;
+}
+
+int p3mg_calculate_forces(p3mg_ctx *h, double rcut, double *f_x, double *f_y, double *f_z, double *fk_x, double *fk_y,
+                          double *fk_z, double *fr_x, double *fr_y, double *fr_z, double *energy) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (c->n > 0 && (!f_x || !f_y || !f_z)) return P3MG_ERR_ARG;
+  P3MG_TRY(p3mg_compute(h, rcut));
+  return p3mg_get_forces(h, f_x, f_y, f_z, fk_x, fk_y, fk_z, fr_x, fr_y, fr_z, energy);
+}
+
+int p3mg_get_forces_device(p3mg_ctx *h, const double **f, const double **fk, const double **fr) {
+  if (!h) return P3MG_ERR_ARG;
+  if (f) *f = h->c.f;
+  if (fk) *fk = h->c.fk;
+  if (fr) *fr = h->c.fr;
+  return P3MG_OK;
+}
+
+int p3mg_enable_timing(p3mg_ctx *h, int on) {
+  if (!h) return P3MG_ERR_ARG;
+  h->c.timing = on != 0;
+  return P3MG_OK;
+}
+
+int p3mg_stage_times(p3mg_ctx *h, double t[4]) {
+  if (!h || !t) return P3MG_ERR_ARG;
+  collect_stage_times(&h->c);
+  for (int i = 0; i < 4; i++) t[i] = h->c.stage_ms[i];
+  return P3MG_OK;
+}
+
+int p3mg_get_influence(p3mg_ctx *h, double *G, double *self81) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!c->have_G) return P3MG_ERR_STATE;
+  cudaSetDevice(c->device);
+  if (G) P3MG_CUDA_TRY(cudaMemcpy(G, c->G, c->M * sizeof(double), cudaMemcpyDeviceToHost));
+  if (self81) memcpy(self81, c->self_b_host, sizeof(c->self_b_host));
+  return P3MG_OK;
+}
+
+void *p3mg_stream(p3mg_ctx *h) { return h ? (void *)h->c.stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,313 @@
+// Hand-written 3D FFT for the P3M meshes (radix 2/3/4/5/7, complex, in
+// place, unnormalised): forward sign -1, backward +1, row-major m^3 with the
+// last index fastest -- the transform the reference plans with FFTW
+// (types.h:61-69, p3m-ik.c:84-88, p3m-ad.c:62-64, ...).
+//
+// One launch per axis.  Each CTA stages a tile of W pencils of length m
+// from HBM/L2 into shared memory (coalesced along the contiguous index),
+// runs the Stockham autosort passes of the mixed-radix decomposition in
+// shared memory (ping-pong buffers, no bit reversal), and writes the tile
+// back.  Tile layout is [element][pencil] so that the butterflies of
+// neighbouring threads touch neighbouring pencils (bank-conflict free).
+#include <math.h>
+#include <stdio.h>
+
+#include "p3mg_internal.cuh"
+
+namespace p3mg {
+
+namespace {
+
+constexpr int FFT_THREADS = 256;
+
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) {
+  C r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) {
+  C r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+
+// multiply by -i (forward) or +i (backward): sign = -1 / +1
+template <typename C>
+__device__ __forceinline__ C mul_i(C a, int sign) {
+  C r;
+  if (sign < 0) {
+    r.x = a.y;
+    r.y = -a.x;
+  } else {
+    r.x = -a.y;
+    r.y = a.x;
+  }
+  return r;
+}
+
+// twiddle exp(sign * 2 pi i e / m) from the forward table
+template <typename C>
+__device__ __forceinline__ C twiddle(const C *tw, int e, int m, int sign) {
+  C t = tw[e % m];
+  if (sign > 0) t.y = -t.y;
+  return t;
+}
+
+// One Stockham pass of radix P over W pencils of length m held in
+// src[e*LD + c]; writes dst.  Ns = size of the sub-transforms already done.
+template <typename C, int P>
+__device__ __forceinline__ void stockham_pass(const C *__restrict__ src, C *__restrict__ dst, const C *tw, int m, int W,
+                                              int LD, int Ns, int sign) {
+  const int nb = m / P;  // butterflies per pencil
+  const int total = nb * W;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int c = t % W;
+    const int j = t / W;
+    const int k = j % Ns;
+    C v[P];
+#pragma unroll
+    for (int r = 0; r < P; r++) v[r] = src[(j + r * nb) * LD + c];
+    // twiddle by W_{Ns P}^{r k} = exp(sign 2 pi i r k m/(Ns P) / m)
+    if (Ns > 1) {
+      const int step = m / (Ns * P);
+#pragma unroll
+      for (int r = 1; r < P; r++) v[r] = cmul(v[r], twiddle(tw, r * k * step, m, sign));
+    }
+    C u[P];
+    if (P == 2) {
+      u[0] = cadd(v[0], v[1]);
+      u[1] = csub(v[0], v[1]);
+    } else if (P == 4) {
+      C a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+      C b0 = cadd(v[1], v[3]), b1 = mul_i(csub(v[1], v[3]), sign);
+      u[0] = cadd(a0, b0);
+      u[2] = csub(a0, b0);
+      u[1] = cadd(a1, b1);
+      u[3] = csub(a1, b1);
+    } else {
+      // generic P-point DFT with W_P^{s r} = tw[s r m / P]
+      const int stepP = m / P;
+#pragma unroll
+      for (int s = 0; s < P; s++) {
+        C acc = v[0];
+#pragma unroll
+        for (int r = 1; r < P; r++) acc = cadd(acc, cmul(v[r], twiddle(tw, ((s * r) % P) * stepP, m, sign)));
+        u[s] = acc;
+      }
+    }
+    const int base = (j / Ns) * Ns * P + k;
+#pragma unroll
+    for (int s = 0; s < P; s++) dst[(base + s * Ns) * LD + c] = u[s];
+  }
+}
+
+struct PassList {
+  int npass;
+  int radix[24];
+};
+
+// AXIS: 0 = x (stride m^2), 1 = y (stride m), 2 = z (contiguous)
+template <typename real, int AXIS>
+__global__ void __launch_bounds__(FFT_THREADS) fft_axis_kernel(typename cplx<real>::type *__restrict__ data,
+                                                               const typename cplx<real>::type *__restrict__ twg, int m,
+                                                               int W, PassList passes, int sign, size_t batch_stride) {
+  typedef typename cplx<real>::type C;
+  extern __shared__ unsigned char smem_raw[];
+  C *tw = reinterpret_cast<C *>(smem_raw);
+  const int LD = W + 1;
+  C *bufA = tw + m;
+  C *bufB = bufA + (size_t)m * LD;
+
+  C *mesh = data + (size_t)blockIdx.y * batch_stride;
+  for (int e = threadIdx.x; e < m; e += blockDim.x) tw[e] = twg[e];
+
+  // which pencils does this CTA own?
+  const int ngroups_inner = (m + W - 1) / W;  // column groups along z for axes 0/1, row groups for axis 2
+  const int g = blockIdx.x;
+  int outer = 0, c0 = 0;
+  if (AXIS == 2) {
+    c0 = g * W;  // first row index (rows are (i,j) pairs flattened, m*m rows)
+  } else {
+    outer = g / ngroups_inner;   // i (axis 1) or j (axis 0)
+    c0 = (g % ngroups_inner) * W;  // first z index
+  }
+  const size_t M2 = (size_t)m * m;
+  const int nrows = (AXIS == 2) ? (int)M2 : m;
+
+  // load
+  for (int t = threadIdx.x; t < W * m; t += blockDim.x) {
+    int e, c;
+    size_t addr;
+    if (AXIS == 2) {
+      c = t / m;
+      e = t % m;
+      addr = (size_t)(c0 + c) * m + e;
+      if (c0 + c >= nrows) continue;
+    } else {
+      e = t / W;
+      c = t % W;
+      if (c0 + c >= m) continue;
+      if (AXIS == 1)
+        addr = ((size_t)outer * m + e) * m + c0 + c;
+      else
+        addr = ((size_t)e * m + outer) * m + c0 + c;
+    }
+    bufA[e * LD + c] = mesh[addr];
+  }
+  __syncthreads();
+
+  C *src = bufA, *dst = bufB;
+  int Ns = 1;
+  for (int p = 0; p < passes.npass; p++) {
+    const int P = passes.radix[p];
+    switch (P) {
+      case 2: stockham_pass<C, 2>(src, dst, tw, m, W, LD, Ns, sign); break;
+      case 3: stockham_pass<C, 3>(src, dst, tw, m, W, LD, Ns, sign); break;
+      case 4: stockham_pass<C, 4>(src, dst, tw, m, W, LD, Ns, sign); break;
+      case 5: stockham_pass<C, 5>(src, dst, tw, m, W, LD, Ns, sign); break;
+      case 7: stockham_pass<C, 7>(src, dst, tw, m, W, LD, Ns, sign); break;
+    }
+    Ns *= P;
+    __syncthreads();
+    C *tmp = src;
+    src = dst;
+    dst = tmp;
+  }
+
+  // store
+  for (int t = threadIdx.x; t < W * m; t += blockDim.x) {
+    int e, c;
+    size_t addr;
+    if (AXIS == 2) {
+      c = t / m;
+      e = t % m;
+      if (c0 + c >= nrows) continue;
+      addr = (size_t)(c0 + c) * m + e;
+    } else {
+      e = t / W;
+      c = t % W;
+      if (c0 + c >= m) continue;
+      if (AXIS == 1)
+        addr = ((size_t)outer * m + e) * m + c0 + c;
+      else
+        addr = ((size_t)e * m + outer) * m + c0 + c;
+    }
+    mesh[addr] = src[e * LD + c];
+  }
+}
+
+template <typename real>
+int launch_fft3d(Ctx *c, void *data, int nbatch, int sign) {
+  typedef typename cplx<real>::type C;
+  const int m = c->mesh;
+  PassList pl;
+  pl.npass = c->plan.npass;
+  for (int i = 0; i < pl.npass; i++) pl.radix[i] = c->plan.radix[i];
+  // pencils per tile: 128 B of contiguous data per row segment at least
+  int W = (sizeof(real) == 8) ? 8 : 16;
+  if (m * W * 2 * (int)sizeof(C) > 160 * 1024) W = 4;
+  const size_t smem = (size_t)m * sizeof(C) + 2 * (size_t)m * (W + 1) * sizeof(C);
+  const size_t stride = c->M;
+  C *d = reinterpret_cast<C *>(data);
+  const C *tw = reinterpret_cast<const C *>(c->plan.tw);
+  // axis order: z (contiguous), y, x -- any order gives the same transform
+  {
+    dim3 grid((unsigned)((size_t)m * m / W + ((size_t)m * m % W ? 1 : 0)), nbatch);
+    fft_axis_kernel<real, 2><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
+  }
+  {
+    const int gi = (m + W - 1) / W;
+    dim3 grid((unsigned)(m * gi), nbatch);
+    fft_axis_kernel<real, 1><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
+    fft_axis_kernel<real, 0><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
+  }
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
+template <typename real>
+int set_smem_limits() {
+  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  return P3MG_OK;
+}
+
+}  // namespace
+
+// Factor m into radices 4, 2, 3, 5, 7 (largest supported first); 0 on
+// success, -1 when m has another prime factor.
+int fft_factor(int m, int *radix, int *npass) {
+  int k = 0;
+  int r = m;
+  while (r % 4 == 0) {
+    radix[k++] = 4;
+    r /= 4;
+  }
+  const int pr[4] = {2, 3, 5, 7};
+  for (int i = 0; i < 4; i++)
+    while (r % pr[i] == 0) {
+      radix[k++] = pr[i];
+      r /= pr[i];
+    }
+  *npass = k;
+  return r == 1 ? 0 : -1;
+}
+
+int fft_plan_init(Ctx *c) {
+  const int m = c->mesh;
+  if (fft_factor(m, c->plan.radix, &c->plan.npass)) return P3MG_ERR_MESH;
+  c->plan.m = m;
+  // twiddle table exp(-2 pi i e/m), computed in long double on the host
+  const bool dbl = (c->precision == P3MG_FP64);
+  const size_t bytes = (size_t)m * (dbl ? sizeof(double2) : sizeof(float2));
+  void *host = malloc(bytes);
+  for (int e = 0; e < m; e++) {
+    long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)m;
+    double cr = (double)cosl(a), ci = (double)(-sinl(a));
+    if (dbl) {
+      ((double2 *)host)[e] = make_double2(cr, ci);
+    } else {
+      ((float2 *)host)[e] = make_float2((float)cr, (float)ci);
+    }
+  }
+  cudaError_t e = cudaMalloc(&c->plan.tw, bytes);
+  if (e != cudaSuccess) {
+    free(host);
+    record_cuda_error(e);
+    return P3MG_ERR_ALLOC;
+  }
+  e = cudaMemcpy(c->plan.tw, host, bytes, cudaMemcpyHostToDevice);
+  free(host);
+  P3MG_CUDA_TRY(e);
+  if (dbl)
+    P3MG_TRY(set_smem_limits<double>());
+  else
+    P3MG_TRY(set_smem_limits<float>());
+  return P3MG_OK;
+}
+
+void fft_plan_free(Ctx *c) {
+  if (c->plan.tw) cudaFree(c->plan.tw);
+  c->plan.tw = nullptr;
+}
+
+int fft3d(Ctx *c, void *data, int nbatch, int sign) {
+  if (c->precision == P3MG_FP64) return launch_fft3d<double>(c, data, nbatch, sign);
+  return launch_fft3d<float>(c, data, nbatch, sign);
+}
+
+}  // namespace p3mg

@@ -1,0 +1,220 @@
+// Optimal influence function G_opt with its aliasing sums, and the ad
+// self-force coefficients, in FP64 on the GPU (one thread per k-vector).
+//
+// Formulas (all per mesh index (NX,NY,NZ), signed frequencies
+// n_d = i - round(i/m) m (p3m-common.c:133-143), aliases n_d + m M_d,
+// |M_d| <= mc):
+//   ik    p3m-ik.c:93-173     G = 2/pi * (D.Z/L) / (|D/L|^2 N1^2)
+//   ik-i  p3m-ik-i.c:78-166   G = 2/pi * (D.Z/L) / (|D/L|^2 1/2 (N1^2 + N2^2))
+//   ad    p3m-ad.c:69-158     G = Z / (pi N1 N2)
+//   ad-i  p3m-ad-i.c:70-150   G = Z / (1/2 pi (N1 N2 + N3 N4))
+// with the reference's zeroing: k = 0 always; for ik/ik-i every k whose
+// three indices are 0 mod m/2; ad returns all zeros when alpha == 0.
+// D is the differential operator Dn[i] = n_i with Dn[m/2] = 0
+// (p3m-common.c:110-131).
+#include <math.h>
+
+#include "p3mg_internal.cuh"
+
+namespace p3mg {
+
+namespace {
+
+__device__ __forceinline__ double ipow_d(double b, int e) {
+  double r = 1.0;
+  for (int i = 0; i < e; i++) r *= b;
+  return r;
+}
+
+__device__ __forceinline__ double sinc_pi(double d) {
+  const double a = P3MG_PI * d;
+  return d == 0.0 ? 1.0 : sin(a) / a;
+}
+
+__device__ __forceinline__ double signed_freq(int i, int m) {
+  return (double)i - round((double)i / (double)m) * (double)m;
+}
+
+__global__ void influence_kernel(double *__restrict__ G, int method, int m, int cao, int mc, double alpha, double L) {
+  const size_t M = (size_t)m * m * m;
+  const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ind >= M) return;
+  const int NZ = (int)(ind % m);
+  const int NY = (int)((ind / m) % m);
+  const int NX = (int)(ind / ((size_t)m * m));
+  const int half = m / 2;
+  if ((NX | NY | NZ) == 0) {
+    G[ind] = 0.0;
+    return;
+  }
+  const bool ad = method_ad(method);
+  if (ad && alpha == 0.0) {
+    G[ind] = 0.0;
+    return;
+  }
+  if (!ad && (NX % half == 0) && (NY % half == 0) && (NZ % half == 0)) {
+    G[ind] = 0.0;
+    return;
+  }
+  const double Leni = 1.0 / L, fak1 = 1.0 / (double)m;
+  const double pa = P3MG_PI / alpha;
+  const double fak2 = pa * pa;
+  const double nx = signed_freq(NX, m), ny = signed_freq(NY, m), nz = signed_freq(NZ, m);
+  double Zx = 0.0, Zy = 0.0, Zz = 0.0, Z = 0.0, N1 = 0.0, N2 = 0.0, N3 = 0.0, N4 = 0.0;
+  for (int MX = -mc; MX <= mc; MX++) {
+    const double NMX = nx + (double)(m * MX);
+    const double sx = sinc_pi(fak1 * NMX);
+    const double S1 = (method == 0 || method == 6) ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
+    for (int MY = -mc; MY <= mc; MY++) {
+      const double NMY = ny + (double)(m * MY);
+      const double sy = sinc_pi(fak1 * NMY);
+      const double S2 = S1 * ((method == 0 || method == 6) ? ipow_d(ipow_d(sy, cao), 2) : ipow_d(sy, 2 * cao));
+      for (int MZ = -mc; MZ <= mc; MZ++) {
+        const double NMZ = nz + (double)(m * MZ);
+        const double sz = sinc_pi(fak1 * NMZ);
+        const double S3 = S2 * ((method == 0 || method == 6) ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao));
+        const double a = NMX * Leni, b = NMY * Leni, cc = NMZ * Leni;
+        const double NM2 = a * a + b * b + cc * cc;
+        const double TE = exp(-fak2 * NM2);
+        const bool even = ((MX + MY + MZ) % 2) == 0;
+        N1 += S3;
+        if (ad) {
+          N2 += S3 * NM2;
+          N3 += even ? S3 : -S3;
+          N4 += even ? S3 * NM2 : -(S3 * NM2);
+          Z += S3 * TE;
+        } else {
+          const double zwi = S3 * TE / NM2;
+          Zx += NMX * zwi * Leni;
+          Zy += NMY * zwi * Leni;
+          Zz += NMZ * zwi * Leni;
+          N2 += even ? S3 : -S3;
+        }
+      }
+    }
+  }
+  double g;
+  if (ad) {
+    g = (method == 3) ? Z / (0.5 * P3MG_PI * (N1 * N2 + N3 * N4)) : Z / (P3MG_PI * N1 * N2);
+  } else {
+    const double Dx = (NX == half) ? 0.0 : nx, Dy = (NY == half) ? 0.0 : ny, Dz = (NZ == half) ? 0.0 : nz;
+    double num = Dx * Zx * Leni + Dy * Zy * Leni + Dz * Zz * Leni;
+    const double dxl = Dx * Leni, dyl = Dy * Leni, dzl = Dz * Leni;
+    const double d2 = dxl * dxl + dyl * dyl + dzl * dzl;
+    if (method == 1) {
+      num /= d2;
+      num /= 0.5 * (N1 * N1 + N2 * N2);
+    } else {
+      num /= d2 * (N1 * N1);
+    }
+    g = 2.0 * num / P3MG_PI;
+  }
+  G[ind] = g;
+}
+
+// ad self-force sums S(m') for the 26 non-zero m' in {-1,0,1}^3
+// (p3m-ad-self-forces.c:30-91):
+//   S(m') = sum_{k: G(k) != 0} sum_{a in {-1,0,1}^3} G(k) U(k + a m) U(k + (a + m') m),
+//   U(k) = (sinc(k_x/m) sinc(k_y/m) sinc(k_z/m))^cao, k the truncated signed frequency.
+// Each thread evaluates the 5^3 alias values U(k + c m), c in {-2..2}^3,
+// once and forms all 26 sums; block reduction then one FP64 atomic per sum.
+__global__ void self_force_sum_kernel(const double *__restrict__ G, int m, int cao, double *__restrict__ S26) {
+  __shared__ double red[26][8];
+  const size_t M = (size_t)m * m * m;
+  const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[26];
+#pragma unroll
+  for (int t = 0; t < 26; t++) acc[t] = 0.0;
+  if (ind < M) {
+    const double g = G[ind];
+    if (g != 0.0) {
+      const int nz = (int)(ind % m), ny = (int)((ind / m) % m), nx = (int)(ind / ((size_t)m * m));
+      const int tx = (int)signed_freq(nx, m), ty = (int)signed_freq(ny, m), tz = (int)signed_freq(nz, m);
+      const double mi = 1.0 / m;
+      double sx[5], sy[5], sz[5];
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        sx[c] = sinc_pi(mi * (double)(tx + (c - 2) * m));
+        sy[c] = sinc_pi(mi * (double)(ty + (c - 2) * m));
+        sz[c] = sinc_pi(mi * (double)(tz + (c - 2) * m));
+      }
+      // U over c in {-2..2}^3 is needed at a (|a|<=1) and a+m' (|.|<=2)
+      for (int ax = 0; ax < 3; ax++)
+        for (int ay = 0; ay < 3; ay++)
+          for (int az = 0; az < 3; az++) {
+            const double U = pow(sx[ax + 1] * sy[ay + 1] * sz[az + 1], (double)cao);
+            const double gU = g * U;
+            int t = 0;
+            for (int px = -1; px <= 1; px++)
+              for (int py = -1; py <= 1; py++)
+                for (int pz = -1; pz <= 1; pz++) {
+                  if (px == 0 && py == 0 && pz == 0) continue;
+                  const double Us = pow(sx[ax + 1 + px] * sy[ay + 1 + py] * sz[az + 1 + pz], (double)cao);
+                  acc[t++] += gU * Us;
+                }
+          }
+    }
+  }
+  // warp reduce then across the (up to 8) warps of the block
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < 26; t++) {
+    double v = acc[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[t][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 26) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[threadIdx.x][w];
+    atomicAdd(&S26[threadIdx.x], v);
+  }
+}
+
+}  // namespace
+
+int influence_compute(Ctx *c, double alpha) {
+  const int m = c->mesh;
+  const size_t M = c->M;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((M + threads - 1) / threads);
+  influence_kernel<<<blocks, threads, 0, c->stream>>>(c->G, c->method, m, c->cao, c->mc, alpha, c->L);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  if (c->precision != P3MG_FP64) {
+    // FP32 copy of G for the mixed-precision convolution
+    P3MG_TRY(g_to_f32(c));
+  }
+  memset(c->self_b_host, 0, sizeof(c->self_b_host));
+  // the ad influence function with alpha == 0 returns before the
+  // self-force initialisation (p3m-ad.c:120-123); keep zeros then
+  if (method_self_force(c->method) && alpha != 0.0) {
+    double *S26 = c->self_b;  // use the first 26 slots as the accumulator
+    P3MG_CUDA_TRY(cudaMemsetAsync(S26, 0, 26 * sizeof(double), c->stream));
+    self_force_sum_kernel<<<blocks, threads, 0, c->stream>>>(c->G, m, c->cao, S26);
+    P3MG_CUDA_TRY(cudaGetLastError());
+    double S[26];
+    P3MG_CUDA_TRY(cudaMemcpyAsync(S, S26, sizeof(S), cudaMemcpyDeviceToHost, c->stream));
+    P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    // b_d(m') = pi m'_d mesh / L^4 * S(m'), zero where m'_d == 0
+    // (p3m-ad-self-forces.c:79-88, layout of Init_self_forces :98-106)
+    const double L4 = (c->L * c->L) * (c->L * c->L);
+    int ind = 0, t = 0;
+    for (int a0 = -1; a0 <= 1; a0++)
+      for (int a1 = -1; a1 <= 1; a1++)
+        for (int a2 = -1; a2 <= 1; a2++) {
+          const int mm[3] = {a0, a1, a2};
+          const bool zero = (a0 == 0 && a1 == 0 && a2 == 0);
+          for (int d = 0; d < 3; d++)
+            c->self_b_host[ind++] = (zero || mm[d] == 0) ? 0.0 : (P3MG_PI * mm[d] * m) / L4 * S[t];
+          if (!zero) t++;
+        }
+  }
+  P3MG_CUDA_TRY(cudaMemcpyAsync(c->self_b, c->self_b_host, 81 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->alpha = alpha;
+  c->have_G = true;
+  return P3MG_OK;
+}
+
+}  // namespace p3mg

@@ -1,0 +1,209 @@
+// Internal declarations of the p3mg library: context, device helpers and
+// the kernel launchers shared by the translation units.  sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "../../include/p3mg.h"
+
+#define P3MG_PI 3.14159265358979323846264338327950288
+#define P3MG_MAX_MESH 512
+#define P3MG_MAX_CAO 7
+// tabulated in-cell offset resolution of the reference: 2*MaxInterpol
+// = 131072 bins per mesh spacing (interpol.h:149, charge-assign.c:156)
+#define P3MG_NINTERP 131072
+
+namespace p3mg {
+
+// ------------------------------------------------------------ error handling
+void record_cuda_error(cudaError_t e);
+
+#define P3MG_CUDA_TRY(expr)                       \
+  do {                                            \
+    cudaError_t e_ = (expr);                      \
+    if (e_ != cudaSuccess) {                      \
+      ::p3mg::record_cuda_error(e_);              \
+      return (e_ == cudaErrorMemoryAllocation) ? P3MG_ERR_ALLOC : P3MG_ERR_CUDA; \
+    }                                             \
+  } while (0)
+
+#define P3MG_TRY(expr)      \
+  do {                      \
+    int s_ = (expr);        \
+    if (s_ != P3MG_OK) return s_; \
+  } while (0)
+
+// ------------------------------------------------------------ method traits
+__host__ __device__ inline bool method_interlaced(int m) { return m == 1 || m == 3; }
+__host__ __device__ inline bool method_ad(int m) { return m == 2 || m == 3 || m == 7; }
+__host__ __device__ inline bool method_self_force(int m) { return m == 2 || m == 7; }
+
+template <typename real>
+struct cplx;
+template <>
+struct cplx<double> {
+  typedef double2 type;
+};
+template <>
+struct cplx<float> {
+  typedef float2 type;
+};
+
+// ------------------------------------------------------------ FFT plan
+struct FftPlan {
+  int m = 0;
+  int npass = 0;
+  int radix[24];
+  void *tw = nullptr;  // m complex entries exp(-2 pi i e / m), real type of the context
+};
+
+// ------------------------------------------------------------ context
+struct Ctx {
+  int method = 0, mesh = 0, cao = 0, mc = 1, precision = P3MG_FP64;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+
+  // particles
+  int n = 0, cap = 0;
+  double L = 0.0;
+  double *x = nullptr, *y = nullptr, *z = nullptr, *q = nullptr;  // inputs (device)
+  double *f = nullptr, *fk = nullptr, *fr = nullptr;              // outputs, 3n each (device)
+  double *energy = nullptr;                                        // device: [0] pair energy, [1] compensation
+
+  // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
+  int brick = 8;
+  int nbrick1 = 0;  // bricks per dimension
+  int *brick_count = nullptr, *brick_start = nullptr, *brick_fill = nullptr;
+  int *part_key = nullptr;     // brick id per particle (input order)
+  int *sorted_idx = nullptr;   // input index of each sorted particle
+  double4 *sorted_xyzq = nullptr;
+
+  // pair cell list
+  int ncell1 = 0, ncell_cap = 0;
+  double cell_rcut = -1.0;
+  int *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
+  int *cell_key = nullptr;
+  int *cell_idx = nullptr;
+  void *cell_pos = nullptr;  // double4 (FP64) or float4 (FP32: position relative to the cell origin, q)
+
+  // mesh data (real type = double for FP64, float for FP32_MIXED)
+  size_t M = 0;               // mesh^3
+  void *Q = nullptr;          // complex mesh
+  void *F = nullptr;          // 3 complex meshes (ik methods)
+  double *G = nullptr;        // FP64 influence function (full mesh)
+  float *G32 = nullptr;       // FP32 copy for the mixed path
+  double *self_b = nullptr;   // 81 self-force coefficients (device)
+  double self_b_host[81];
+  FftPlan plan;
+
+  double alpha = 0.0;
+  bool have_G = false;
+
+  // timing
+  bool timing = false;
+  cudaEvent_t ev[5];
+  bool ev_ok = false;
+  double stage_ms[4] = {0, 0, 0, 0};
+  bool stage_pending = false;
+
+  // scratch for a single-CTA scan
+  int *scan_tmp = nullptr;
+};
+
+int alloc_system(Ctx *c, int n);
+int free_all(Ctx *c);
+
+// ------------------------------------------------------------ launchers
+// FFT (p3mg_fft.cu)
+int fft_plan_init(Ctx *c);
+void fft_plan_free(Ctx *c);
+int fft3d(Ctx *c, void *data, int nbatch, int sign);
+
+// influence (p3mg_influence.cu)
+int influence_compute(Ctx *c, double alpha);
+
+// charge assignment / back-interpolation (p3mg_assign.cu)
+int kspace_prepare(Ctx *c);
+int kspace_run(Ctx *c);  // scatter, FFTs, convolution, gather, self-force into c->fk / c->f
+
+// real space (p3mg_pairs.cu)
+int pairs_run(Ctx *c, double rcut, double alpha);
+
+// misc kernels (p3mg_api.cu)
+int zero_forces(Ctx *c);
+int combine_forces(Ctx *c);
+
+// FP32 copy of the FP64 influence function (mixed precision)
+int g_to_f32(Ctx *c);
+
+// single-CTA exclusive scan of counts[0..nb) into start[0..nb] (start[nb] = total)
+int exclusive_scan(Ctx *c, const int *counts, int *start, int nb);
+
+// ------------------------------------------------------------ device helpers
+
+__host__ __device__ inline int wrap_full(int i, int m) {
+  int r = i % m;
+  return r < 0 ? r + m : r;
+}
+
+// Mesh geometry of one coordinate, with the reference's rounding
+// (charge-assign.c:148-157): pos = x*Hi - shift (+ 0.5 for the shifted mesh),
+// nmp = floor(pos + 0.5), arg = floor((pos - nmp + 0.5) * 131072).
+// __dmul_rn/__dadd_rn keep each operation separately rounded (no FMA),
+// so the tabulated bin `arg` is the one the reference selects.
+__device__ inline void mesh_geometry(double xc, double Hi, double shift, int ii, int m, int *base, int *arg) {
+  double pos = __dadd_rn(__dmul_rn(xc, Hi), -shift);
+  if (ii) pos = __dadd_rn(pos, 0.5);
+  double nf = floor(__dadd_rn(pos, 0.5));
+  int nmp = (int)nf;
+  double frac = __dadd_rn(__dadd_rn(pos, -nf), 0.5);
+  int a = (int)floor(__dmul_rn(frac, (double)P3MG_NINTERP));
+  a = a < 0 ? 0 : (a > P3MG_NINTERP - 1 ? P3MG_NINTERP - 1 : a);
+  *base = wrap_full(nmp, m);
+  *arg = a;
+}
+
+// Cardinal B-spline weights of order CAO at the tabulated offset of bin
+// `arg` (x = (arg - 65536)/131072 in [-0.5, 0.5)):  w[j] = M_CAO(u + CAO-1-j),
+// u = x + 1/2, with the recursion M_n(u) = [u M_{n-1}(u) + (n-u) M_{n-1}(u-1)]/(n-1)
+// (de Boor; Essmann et al. 1995) and dw[j] = M_{CAO-1}(u+k) - M_{CAO-1}(u+k-1),
+// k = CAO-1-j.  These are the charge-assignment polynomials of
+// window-functions.c:46-183.
+template <typename real, int CAO, bool DERIV>
+__device__ __forceinline__ void bspline_weights(int arg, real *w, real *dw) {
+  const real u = (real)(arg - P3MG_NINTERP / 2) * (real)(1.0 / P3MG_NINTERP) + (real)0.5;
+  real a[CAO];
+  real prev[CAO];
+  a[0] = (real)1;
+#pragma unroll
+  for (int k = 1; k < CAO; k++) a[k] = (real)0;
+#pragma unroll
+  for (int n = 2; n <= CAO; n++) {
+#pragma unroll
+    for (int k = 0; k < CAO; k++) prev[k] = a[k];
+    const real inv = (real)1 / (real)(n - 1);
+#pragma unroll
+    for (int k = 0; k < CAO; k++) {
+      if (k < n) {
+        real lo = (k < n - 1) ? prev[k] : (real)0;
+        real hi = (k > 0) ? prev[k - 1] : (real)0;
+        a[k] = ((u + (real)k) * lo + ((real)n - u - (real)k) * hi) * inv;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < CAO; j++) {
+    const int k = CAO - 1 - j;
+    w[j] = a[k];
+    if (DERIV) {
+      if (CAO == 1)
+        dw[j] = (real)0;
+      else
+        dw[j] = prev[k] - (k > 0 ? prev[k - 1] : (real)0);
+    }
+  }
+}
+
+}  // namespace p3mg

@@ -1,0 +1,400 @@
+"""Python host side of p3mg: ctypes bindings over the C ABI (include/p3mg.h)
+and a mirror of the reference's plugin interface for the P3M force path.
+
+The reference selects a ``method_t`` by numeric id (main.c:314-344) and
+drives it as Init -> Influence_function (per alpha) -> Calculate_forces
+(common.c:268-327).  ``Method`` below keeps those names, ids and the
+accumulate-into semantics; ``calculate_forces`` is Calculate_forces.  The
+compute runs in ``libp3mg.so`` (hand-written sm_100a kernels); there is no
+CPU fallback -- loading fails loudly when the library or a GPU is missing.
+
+Arrays: positions, charges and forces are numpy float64; forces are (3, n)
+arrays (the reference's SoA vector_array_t, types.h:126-132).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+OK = 0
+FP64 = 0
+FP32_MIXED = 1
+
+# method ids and names of the reference's method_t tables
+METHODS = {
+    0: ("P3M with ik differentiation, not intelaced.", "p3m-ik"),
+    1: ("P3M with ik differentiation, interlaced.", "p3m-ik-i"),
+    2: ("P3M with analytic differentiation, not intelaced.", "p3m-ad"),
+    3: ("P3M with analytic differentiation, intelaced.", "p3m-ad-i"),
+    6: ("P3M with ik differentiation, not intelaced, real input.", "p3m-ik-r"),
+    7: ("P3M with analytic differentiation, not intelaced, real input.", "p3m-ad-r"),
+}
+
+# method_t flags (types.h:290-303)
+FLAG_IK, FLAG_AD, FLAG_INTERLACED, FLAG_SELF_FORCE = 1, 2, 4, 128
+METHOD_FLAGS = {
+    0: FLAG_IK, 1: FLAG_IK | FLAG_INTERLACED, 2: FLAG_AD | FLAG_SELF_FORCE, 3: FLAG_AD | FLAG_INTERLACED,
+    6: FLAG_IK, 7: FLAG_AD | FLAG_SELF_FORCE,
+}
+
+
+class P3MGError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = _lib_or_none().p3mg_strerror(status).decode() if _lib_or_none() else str(status)
+        extra = ""
+        if status == -6 and _lib_or_none():
+            extra = " (%s)" % _lib_or_none().p3mg_last_cuda_error().decode()
+        super().__init__("%s: %s [status %d]%s" % (what, msg, status, extra))
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_LIB = None
+
+
+def _lib_or_none():
+    return _LIB
+
+
+def lib_path():
+    return os.path.join(HERE, "libp3mg.so")
+
+
+def load():
+    """Load libp3mg.so (built by p3m-standalone_b200/build.py).  Raises if absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = lib_path()
+    if not os.path.exists(path):
+        raise RuntimeError("libp3mg.so not found at %s: run python p3m-standalone_b200/build.py" % path)
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.p3mg_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_int]
+    L.p3mg_destroy.argtypes = [vp]
+    L.p3mg_destroy.restype = None
+    L.p3mg_set_system.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double]
+    L.p3mg_set_system_device.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_double]
+    L.p3mg_influence.argtypes = [vp, ctypes.c_double]
+    L.p3mg_kspace_forces.argtypes = [vp] + [_dp] * 6
+    L.p3mg_real_forces.argtypes = [vp, ctypes.c_double, ctypes.c_double] + [_dp] * 4
+    L.p3mg_calculate_forces.argtypes = [vp, ctypes.c_double] + [_dp] * 10
+    L.p3mg_compute.argtypes = [vp, ctypes.c_double]
+    L.p3mg_get_forces.argtypes = [vp] + [_dp] * 10
+    L.p3mg_get_forces_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)]
+    L.p3mg_enable_timing.argtypes = [vp, ctypes.c_int]
+    L.p3mg_stage_times.argtypes = [vp, _dp]
+    L.p3mg_get_influence.argtypes = [vp, _dp, _dp]
+    L.p3mg_stream.argtypes = [vp]
+    L.p3mg_stream.restype = vp
+    L.p3mg_strerror.argtypes = [ctypes.c_int]
+    L.p3mg_strerror.restype = ctypes.c_char_p
+    L.p3mg_last_cuda_error.argtypes = []
+    L.p3mg_last_cuda_error.restype = ctypes.c_char_p
+    _LIB = L
+    return L
+
+
+def _check(status, what):
+    if status != OK:
+        raise P3MGError(status, what)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One p3mg context: a method on one mesh, owning its device memory."""
+
+    def __init__(self, method, mesh, cao, mc=1, precision=FP64):
+        self._lib = load()
+        self._h = ctypes.c_void_p()
+        _check(self._lib.p3mg_create(ctypes.byref(self._h), int(method), int(mesh), int(cao), int(mc),
+                                     int(precision)), "p3mg_create")
+        self.method, self.mesh, self.cao, self.mc, self.precision = method, mesh, cao, mc, precision
+        self.n = 0
+        self.L = None
+
+    def close(self):
+        if self._h:
+            self._lib.p3mg_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_system(self, x, y, z, q, L):
+        x, y, z, q = map(_f64, (x, y, z, q))
+        self._keep = (x, y, z, q)
+        _check(self._lib.p3mg_set_system(self._h, len(x), _p(x), _p(y), _p(z), _p(q), float(L)), "p3mg_set_system")
+        self.n, self.L = len(x), float(L)
+
+    def set_system_device(self, n, px, py, pz, pq, L):
+        """Device pointers (ints) to n doubles each."""
+        _check(self._lib.p3mg_set_system_device(self._h, int(n), ctypes.c_void_p(px), ctypes.c_void_p(py),
+                                                ctypes.c_void_p(pz), ctypes.c_void_p(pq), float(L)),
+               "p3mg_set_system_device")
+        self.n, self.L = int(n), float(L)
+
+    def influence(self, alpha):
+        _check(self._lib.p3mg_influence(self._h, float(alpha)), "p3mg_influence")
+
+    def kspace_forces(self, fk=None, ftot=None):
+        n = self.n
+        fk = np.zeros((3, n)) if fk is None else fk
+        args = [_p(fk[0]), _p(fk[1]), _p(fk[2])]
+        args += [None] * 3 if ftot is None else [_p(ftot[0]), _p(ftot[1]), _p(ftot[2])]
+        _check(self._lib.p3mg_kspace_forces(self._h, *args), "p3mg_kspace_forces")
+        return fk
+
+    def real_forces(self, rcut, alpha, fr=None):
+        n = self.n
+        fr = np.zeros((3, n)) if fr is None else fr
+        e = ctypes.c_double(0.0)
+        _check(self._lib.p3mg_real_forces(self._h, float(rcut), float(alpha), _p(fr[0]), _p(fr[1]), _p(fr[2]),
+                                          ctypes.byref(e)), "p3mg_real_forces")
+        return fr, e.value
+
+    def calculate_forces(self, rcut):
+        """Calculate_forces (common.c:268-327): dict f, f_k, f_r, energy."""
+        n = self.n
+        f, fk, fr = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+        e = ctypes.c_double(0.0)
+        _check(self._lib.p3mg_calculate_forces(self._h, float(rcut), _p(f[0]), _p(f[1]), _p(f[2]), _p(fk[0]),
+                                               _p(fk[1]), _p(fk[2]), _p(fr[0]), _p(fr[1]), _p(fr[2]),
+                                               ctypes.byref(e)), "p3mg_calculate_forces")
+        return dict(f=f, f_k=fk, f_r=fr, energy=e.value)
+
+    def compute(self, rcut):
+        _check(self._lib.p3mg_compute(self._h, float(rcut)), "p3mg_compute")
+
+    def get_forces(self):
+        n = self.n
+        f, fk, fr = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+        e = ctypes.c_double(0.0)
+        _check(self._lib.p3mg_get_forces(self._h, _p(f[0]), _p(f[1]), _p(f[2]), _p(fk[0]), _p(fk[1]), _p(fk[2]),
+                                         _p(fr[0]), _p(fr[1]), _p(fr[2]), ctypes.byref(e)), "p3mg_get_forces")
+        return dict(f=f, f_k=fk, f_r=fr, energy=e.value)
+
+    def forces_device(self):
+        """Device pointers (ints) to the f, f_k, f_r arrays (3n doubles each)."""
+        a, b, c = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _check(self._lib.p3mg_get_forces_device(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+               "p3mg_get_forces_device")
+        return a.value, b.value, c.value
+
+    def enable_timing(self, on=True):
+        _check(self._lib.p3mg_enable_timing(self._h, int(bool(on))), "p3mg_enable_timing")
+
+    def stage_times(self):
+        t = np.zeros(4)
+        _check(self._lib.p3mg_stage_times(self._h, _p(t)), "p3mg_stage_times")
+        return dict(t_c=t[0], t_g=t[1], t_f=t[2], t_r=t[3])
+
+    def get_influence(self):
+        G = np.zeros(self.mesh ** 3)
+        b = np.zeros(81)
+        _check(self._lib.p3mg_get_influence(self._h, _p(G), _p(b)), "p3mg_get_influence")
+        return G.reshape(self.mesh, self.mesh, self.mesh), b
+
+    def stream(self):
+        return self._lib.p3mg_stream(self._h)
+
+
+class Method:
+    """Mirror of the reference's method_t (types.h:306-316) for one id.
+
+    Init -> Context; Influence_function(alpha); Kspace_force accumulates into
+    forces['f_k'] (and subtracts the ad self-force from forces['f']).
+    """
+
+    def __init__(self, method_id):
+        if method_id not in METHODS:
+            raise P3MGError(-2, "method %r" % (method_id,)) if _LIB else ValueError("method %r not known" % method_id)
+        self.method_id = method_id
+        self.method_name, self.method_name_short = METHODS[method_id]
+        self.flags = METHOD_FLAGS[method_id]
+
+    def Init(self, x, y, z, q, L, mesh, cao, mc=1, precision=FP64):
+        ctx = Context(self.method_id, mesh, cao, mc, precision)
+        ctx.set_system(x, y, z, q, L)
+        return ctx
+
+    @staticmethod
+    def Influence_function(ctx, alpha):
+        ctx.influence(alpha)
+
+    @staticmethod
+    def Kspace_force(ctx, forces):
+        ctx.kspace_forces(forces["f_k"], forces["f"])
+
+
+def calculate_forces(ctx, rcut):
+    """Calculate_forces (common.c:268-327) on a context with G computed."""
+    return ctx.calculate_forces(rcut)
+
+
+# ------------------------------------------------------------------ systems
+
+SYSTEM_RANDOM, SYSTEM_INNER_BOX, SYSTEM_MADELUNG, SYSTEM_SEPARATED_DIPOLE, SYSTEM_GAUSSIAN, SYSTEM_SLAB = range(6)
+
+
+def generate_system(system_type, n, L, charge=1.0, seed=12345, sigma=None):
+    """Seeded synthetic systems of the reference's types (generate_system.c,
+    README 'system_type'): returns x, y, z, q (float64) with positions in
+    [0, L).  The generator is numpy's PCG64, not GSL's stream; inputs are
+    shared with the reference through the position-file format.
+
+    0 uniform; 1 inner box [0.25L, 0.75L)^3; 2 Madelung crystal; 3 separated
+    dipoles (pairs at distance 1, isotropic); 4 Gaussian about the centre
+    (sigma default L/6, rejection to [0, L)); 5 slab x in [0.25L, 0.75L)
+    (README:57 geometry)."""
+    rng = np.random.default_rng(seed)
+    alt = 1.0 - 2.0 * (np.arange(n) % 2)
+    if system_type == SYSTEM_RANDOM:
+        p = rng.uniform(0.0, L, size=(3, n))
+        q = alt * charge
+    elif system_type == SYSTEM_INNER_BOX:
+        p = 0.25 * L + 0.5 * L * rng.uniform(0.0, 1.0, size=(3, n))
+        q = alt.copy()
+    elif system_type == SYSTEM_MADELUNG:
+        per_row = int(np.ceil(n ** (1.0 / 3.0) - 1e-9))
+        a = L / per_row
+        i, j, k = np.meshgrid(np.arange(per_row), np.arange(per_row), np.arange(per_row), indexing="ij")
+        p = np.stack([a * i.ravel() + 0.5 * a, a * j.ravel() + 0.5 * a, a * k.ravel() + 0.5 * a])
+        q = 1.0 - 2.0 * ((i + j + k).ravel() % 2)
+    elif system_type == SYSTEM_SEPARATED_DIPOLE:
+        nd = n // 2
+        c = L * rng.uniform(0.0, 1.0, size=(3, nd))
+        u = rng.uniform(-1.0, 1.0, size=nd)
+        th = 2.0 * np.pi * rng.uniform(0.0, 1.0, size=nd)
+        s = np.sqrt(1.0 - u * u)
+        d = np.stack([s * np.cos(th), s * np.sin(th), u])
+        p = np.empty((3, 2 * nd))
+        p[:, 0::2] = c
+        p[:, 1::2] = np.mod(c + d, L)
+        q = np.empty(2 * nd)
+        q[0::2] = 1.0
+        q[1::2] = -1.0
+    elif system_type == SYSTEM_GAUSSIAN:
+        sig = L / 6.0 if sigma is None else sigma
+        p = np.empty((3, n))
+        for dim in range(3):
+            v = rng.normal(L / 2.0, sig, size=n)
+            bad = (v < 0.0) | (v >= L)
+            while bad.any():
+                v[bad] = rng.normal(L / 2.0, sig, size=int(bad.sum()))
+                bad = (v < 0.0) | (v >= L)
+            p[dim] = v
+        q = alt * charge
+    elif system_type == SYSTEM_SLAB:
+        p = rng.uniform(0.0, L, size=(3, n))
+        p[0] = 0.25 * L + 0.5 * L * rng.uniform(0.0, 1.0, size=n)
+        q = alt.copy()
+    else:
+        raise ValueError("system_type %r not known" % (system_type,))
+    p = np.where(p >= L, p - L, p)
+    return p[0].copy(), p[1].copy(), p[2].copy(), np.asarray(q, dtype=np.float64)
+
+
+# --------------------------------------------------------------- file formats
+
+def read_system(path):
+    """Read_system (io.c:100-157): '# Teilchenzahl: N', '# Len: L', then
+    N lines 'x y z q'.  Extra '#' header lines (as in the Data/ fixtures'
+    '# Mesh:') are skipped."""
+    n = L = None
+    rows = []
+    with open(path) as fh:
+        for line in fh:
+            s = line.strip()
+            if not s:
+                continue
+            if s.startswith("#"):
+                if "Teilchenzahl" in s:
+                    n = int(s.split(":")[1])
+                elif "Len" in s:
+                    L = float(s.split(":")[1])
+                continue
+            rows.append([float(v) for v in s.split()[:4]])
+            if n is not None and len(rows) == n:
+                break
+    if n is None or L is None:
+        raise ValueError("Error while reading file '%s'" % path)
+    a = np.array(rows, dtype=np.float64).reshape(-1, 4)
+    if a.shape[0] != n:
+        raise ValueError("Error while reading file '%s': %d of %d particles" % (path, a.shape[0], n))
+    return a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy(), a[:, 3].copy(), L
+
+
+def write_system(path, x, y, z, q, L):
+    """Write_system (io.c:199-225), same '%lf' text format."""
+    with open(path, "w") as fh:
+        fh.write("# Teilchenzahl: %d\n" % len(x))
+        fh.write("# Len: %f\n" % L)
+        for i in range(len(x)):
+            fh.write("%f\t%f\t%f\t%f\n" % (x[i], y[i], z[i], q[i]))
+
+
+def read_exact_forces(path, n):
+    """Read_exact_forces (io.c:70-98): lines 'id fx fy fz'.  Also accepts the
+    7-column 'id F(3) F_k(3)' layout Write_exact_forces writes (io.c:171-173),
+    taking the total force columns."""
+    f = np.zeros((3, n))
+    i = 0
+    with open(path) as fh:
+        for line in fh:
+            s = line.split()
+            if len(s) < 4:
+                continue
+            f[:, i] = [float(s[1]), float(s[2]), float(s[3])]
+            i += 1
+            if i == n:
+                break
+    if i != n:
+        raise ValueError("Error while reading file '%s' (%d)" % (path, i))
+    return f
+
+
+def write_exact_forces(path, f, fk):
+    """Write_exact_forces (io.c:159-177): 'id F(3) F_k(3)' with %lf."""
+    with open(path, "w") as fh:
+        for i in range(f.shape[1]):
+            fh.write("%d\t%f\t%f\t%f\t%f\t%f\t%f\n" % (i, f[0, i], f[1, i], f[2, i], fk[0, i], fk[1, i], fk[2, i]))
+
+
+def rms_error(f, ref):
+    """DeltaF = sqrt(sum |F - F_ref|^2) / sqrt(N) (error.c:21-34, main.c:446)."""
+    f = np.asarray(f)
+    return float(np.sqrt(np.sum((f - ref) ** 2)) / np.sqrt(f.shape[-1]))
+
+
+def alpha_sweep(alphamin, alphamax, alphastep):
+    """The reference's alpha loop values (main.c:375): double accumulation."""
+    out = []
+    a = float(alphamin)
+    while a <= alphamax:
+        out.append(a)
+        a += alphastep
+    return out
