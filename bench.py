@@ -1,0 +1,433 @@
+"""P3M steps/s on one B200 (or N replicas): FP32-mixed vs FP64 plain.
+
+Workload (the headline configuration): method 1 (P3M ik, c2c, interlaced),
+1,000,000 particles uniform in a box of side 100 (density 1), +-1 charges
+alternating, mesh 128^3, cao 7, rcut 3.5, alpha 0.9, mc 1.  One step = one
+force evaluation (Calculate_forces, common.c:268-327): real-space pairs,
+charge assignment, FFTs, convolution, back-interpolation, f = f_k + f_r.
+The influence function is computed once per alpha outside the timed region,
+as the reference's own timer does (main.c:382-386).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one process per GPU): independent replicas of the
+workload, no collective on the data path ("replicas only"); the timed region
+is bracketed by barriers and the time is the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "p3m-standalone_b200"))
+
+WORKLOAD = dict(workload="p3m-ik-i 1M particles, box 100, mesh 128^3, cao 7, rcut 3.5, alpha 0.9",
+                method=1, n=1_000_000, box=100.0, mesh=128, cao=7, mc=1, rcut=3.5, alpha=0.9,
+                system_type=0, seed=12345)
+METRIC = "P3M steps/s at 1e-4 RMS force error: FP32-mixed vs FP64 plain, same B200"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [v.strip() for v in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return dict(sm_mhz=statistics.median(sm), sm_max_mhz=smax, reasons=sorted(reasons), samples=len(sm))
+
+
+# --------------------------------------------------------------- helpers
+
+def algorithmic_bytes(method, n, mesh, s):
+    """Algorithmic HBM bytes of one step: each stage reads its inputs once
+    and writes its outputs once.  R = mesh bytes (2M s interlaced, M s
+    otherwise), G = M s; particles 7 n s (x, y, z, q in, f out).
+    ik: 7ns + 16R + G ; ad: 7ns + 8R + G."""
+    M = mesh ** 3
+    interlaced = method in (1, 3)
+    R = (2 * M if interlaced else M) * s
+    G = M * s
+    if method in (0, 1, 6):
+        return 7 * n * s + 16 * R + G
+    return 7 * n * s + 8 * R + G
+
+
+def gather_bytes(method, n, mesh, s):
+    """Algorithmic bytes of the back-interpolation kernel: the ik fields
+    (3R) or the ad potential (R) read once, n (x, y, z, q) in, n f out."""
+    M = mesh ** 3
+    R = (2 * M if method in (1, 3) else M) * s
+    return (3 * R if method in (0, 1, 6) else R) + 7 * n * s
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch of `kernel` at this workload from a committed
+    ncu summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            d = json.load(fh)
+        v = d.get(kernel)
+        return None if v is None else float(v["bytes_per_launch"])
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- our arm
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import p3mg
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    W = WORKLOAD
+    n = args.n or W["n"]
+    L = W["box"] * (n / W["n"]) ** (1.0 / 3.0)
+    x, y, z, q = p3mg.generate_system(W["system_type"], n, L, seed=W["seed"] + rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    results = {}
+    clocks = None
+    for prec in (p3mg.FP32_MIXED, p3mg.FP64):
+        ctx = p3mg.Context(W["method"], W["mesh"], W["cao"], W["mc"], prec)
+        ctx.set_system(x, y, z, q, L)
+        ctx.influence(W["alpha"])
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+        ctx.enable_timing(True)
+        for _ in range(args.warmup):
+            ctx.compute(W["rcut"])
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local_rank) if prec == p3mg.FP32_MIXED else None
+        barrier()
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        l0 = ctx.launch_count()
+        dev_ms = 0.0
+        kms = {"pairs": 0.0, "scatter": 0.0, "gather": 0.0}
+        sms = {"t_c": 0.0, "t_g": 0.0, "t_f": 0.0, "t_r": 0.0}
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # evict the previous step from L2 (untimed)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.compute(W["rcut"])
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms += e0.elapsed_time(e1)
+            for k, v in ctx.kernel_times().items():
+                kms[k] += v
+            for k, v in ctx.stage_times().items():
+                sms[k] += v
+        launches = ctx.launch_count() - l0
+        barrier()
+        if sampler:
+            clocks = sampler.stop()
+        ms = max_over_ranks(dev_ms) / args.steps
+        results[prec] = dict(ms=ms, kernels={k: v / args.steps for k, v in kms.items()},
+                             stages={k: v / args.steps for k, v in sms.items()}, launches=launches)
+        ctx.enable_timing(False)
+
+        # end to end through the public C ABI with pinned host buffers
+        hx = [torch.from_numpy(a).pin_memory() for a in (x, y, z, q)]
+        hf = [torch.empty(n, dtype=torch.float64).pin_memory() for _ in range(3)]
+        for _ in range(max(1, args.warmup // 2)):
+            ctx.set_system_ptr(n, *[t.data_ptr() for t in hx], L)
+            ctx.compute(W["rcut"])
+            ctx.get_total_forces_ptr(*[t.data_ptr() for t in hf])
+        barrier()
+        e2e_ms = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.set_system_ptr(n, *[t.data_ptr() for t in hx], L)
+            ctx.compute(W["rcut"])
+            ctx.get_total_forces_ptr(*[t.data_ptr() for t in hf])
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms += e0.elapsed_time(e1)
+        barrier()
+        results[prec]["e2e_ms"] = max_over_ranks(e2e_ms) / args.steps
+        if prec == p3mg.FP32_MIXED:
+            results["fp32_forces"] = np.stack([t.numpy().copy() for t in hf])
+        ctx.close()
+
+    r32, r64 = results[p3mg.FP32_MIXED], results[p3mg.FP64]
+    value = world * 1000.0 / r32["ms"]
+    e2e = world * 1000.0 / r32["e2e_ms"]
+
+    out = None
+    if rank == 0:
+        # dominant kernel of the FP32 step and its HBM roofline
+        k = r32["kernels"]
+        dom = max(k, key=k.get)
+        peak, peak_kind = measured_peaks()
+        s = 4
+        if dom == "gather":
+            abytes = gather_bytes(W["method"], n, W["mesh"], s)
+        elif dom == "scatter":
+            R = 2 * W["mesh"] ** 3 * s
+            abytes = R + 4 * n * s
+        else:
+            abytes = 16 * n + 7 * n * s  # float4 cell-sorted particles in, forces out
+        achieved = abytes / (k[dom] * 1e-3) / 1e9
+        kernel_names = {"gather": "gather_kernel", "scatter": "scatter_kernel", "pairs": "pairs_fp32_kernel"}
+        traffic = profile_traffic(kernel_names[dom])
+        out = {
+            "metric": METRIC,
+            "value": round(value, 3),
+            "unit": "steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(r32["ms"], 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (mesh, FFT, pairs; f64 G_opt and geometry)",
+            "data": "synthetic: seeded uniform system (system_type 0), +-1 charges alternating",
+            "config": {"workload": W["workload"], "method": W["method"], "particles": n, "box": L,
+                       "mesh": W["mesh"], "cao": W["cao"], "rcut": W["rcut"], "alpha": W["alpha"], "mc": W["mc"],
+                       "parallelism": "replicas%d" % world if world > 1 else "single-gpu",
+                       "l2": "flushed between timed steps (256 MB write, untimed)"},
+            "fp64": {"value": round(world * 1000.0 / r64["ms"], 3), "unit": "steps/s",
+                     "ms_per_step": round(r64["ms"], 4), "e2e_steps_per_s": round(world * 1000.0 / r64["e2e_ms"], 3)},
+            "fp32_over_fp64": round(r64["ms"] / r32["ms"], 3),
+            "stages_ms": {"fp32": {k2: round(v, 4) for k2, v in r32["stages"].items()},
+                          "fp64": {k2: round(v, 4) for k2, v in r64["stages"].items()}},
+            "kernels_ms": {"fp32": {k2: round(v, 4) for k2, v in r32["kernels"].items()},
+                           "fp64": {k2: round(v, 4) for k2, v in r64["kernels"].items()}},
+            "e2e": {"value": round(e2e, 3), "unit": "steps/s", "h2d_bytes_per_step": 4 * 8 * n,
+                    "d2h_bytes_per_step": 3 * 8 * n},
+            "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": round(achieved, 2),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_source": peak_kind, "algorithmic_bytes": int(abytes),
+                         "traffic": traffic},
+            "step_roofline": {"algorithmic_bytes": int(algorithmic_bytes(W["method"], n, W["mesh"], 4)),
+                              "achieved_gbs": round(algorithmic_bytes(W["method"], n, W["mesh"], 4)
+                                                    / (r32["ms"] * 1e-3) / 1e9, 2)},
+            "gpu_launches": int(r32["launches"]),
+            "clocks": clocks,
+        }
+    return out, results
+
+
+# ----------------------------------------------------------- CPU baseline
+
+def reference_sample(n_k=20000, n_r=5000):
+    """One bounded sample of the reference's own CPU code (oracle/_ref, the
+    reference compiled from its sources, single-threaded) scaled to a full
+    step of the workload:
+      k-space: Kspace_force in the reference's timing mode (tuning=1, stage
+        timers t_c/t_g/t_f, p3m-common.h:48-57) on n_k particles at the
+        workload's mesh; charge and force assignment scale with N, the
+        FFT/convolution stage does not;
+      real space: Realteil (O(N^2) loop) on n_r particles at density 1,
+        scaled by (N/n_r)^2.
+    Returns (seconds per full step, description, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import p3mg
+    W = WORKLOAD
+    N = W["n"]
+    kind = "reference" if O.ref_available() else "port"
+    rng = np.random.default_rng(7)
+    x, y, z, q = p3mg.generate_system(0, N, W["box"], seed=W["seed"])
+    sel = np.sort(rng.choice(N, n_k, replace=False))
+    qq = 1.0 - 2.0 * (np.arange(n_k) % 2)
+    if kind == "reference":
+        r = O.ref_forces(W["method"], W["mesh"], W["cao"], W["mc"], W["alpha"], 0.0, x[sel], y[sel], z[sel], qq,
+                         W["box"], tuning=True)
+        tc, tg, tf = r["times"]
+    else:
+        t0 = time.perf_counter()
+        O.kspace(W["method"], W["mesh"], W["cao"], W["mc"], W["alpha"], x[sel], y[sel], z[sel], qq, W["box"],
+                 G=np.ones(W["mesh"] ** 3))
+        tc, tg, tf = 0.0, 0.0, time.perf_counter() - t0
+    t_k = (tc + tf) * (N / n_k) + tg
+    Lr = W["box"] * (n_r / N) ** (1.0 / 3.0)
+    xr, yr, zr, qr = p3mg.generate_system(0, n_r, Lr, seed=3)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        O.ref_realteil(xr, yr, zr, qr, Lr, W["rcut"], W["alpha"])
+    else:
+        O.realspace(xr, yr, zr, qr, Lr, W["rcut"], W["alpha"], cells=False)
+    t_r = (time.perf_counter() - t0) * (N / n_r) ** 2
+    desc = ("k-space on %d of the 1M particles (stage times t_c+t_f scaled x%d, t_g as is) + real-space "
+            "N^2 loop on %d particles at density 1 scaled x%d; FFT is the oracle's DFT standing in for FFTW"
+            % (n_k, N // n_k, n_r, (N // n_r) ** 2))
+    return t_k + t_r, desc, kind, dict(t_c=tc, t_g=tg, t_f=tf, t_real_sample=t_r / (N / n_r) ** 2)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    times = []
+    for i in range(args.warmup + args.steps):
+        t, desc, kind, parts = reference_sample()
+        if i >= args.warmup:
+            times.append(t)
+    v = 1.0 / statistics.mean(times)
+    try:
+        import scipy.fft
+        a = np.random.default_rng(0).standard_normal((128, 128, 128)) + 0j
+        t0 = time.perf_counter()
+        scipy.fft.fftn(a, workers=1)
+        fft_proxy = time.perf_counter() - t0
+    except Exception:
+        fft_proxy = None
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": v,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 / v,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded uniform system (system_type 0), +-1 charges alternating",
+        "config": {"workload": WORKLOAD["workload"], "parallelism": "cpu, 1 thread"},
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": kind, "sample": desc,
+                         "last_sample_parts_s": parts, "scipy_fft_128cube_1thread_s": fft_proxy,
+                         "cpu": _cpu_model()},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip() + " (nproc %d)" % os.cpu_count()
+    except Exception:
+        pass
+    return "nproc %d" % os.cpu_count()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=0, help="particles (default: the workload's 1,000,000)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out))
+        return
+    out, _ = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            t, desc, kind, parts = reference_sample()
+            out["cpu_baseline"] = {"value": 1.0 / t, "unit": "steps/s", "cores": 1, "kind": kind, "sample": desc,
+                                   "cpu": _cpu_model()}
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -129,6 +129,20 @@ int p3mg_stage_times(p3mg_ctx *ctx, double t[4]);
  * coefficients (zeros for other methods) to host memory; either may be NULL. */
 int p3mg_get_influence(p3mg_ctx *ctx, double *G, double *self_coeffs81);
 
+/* Times in milliseconds of single kernels in the last timed step:
+ * t[0] real-space pair kernel, t[1] charge-assignment (scatter) kernel,
+ * t[2] back-interpolation (gather) kernel.  Needs p3mg_enable_timing. */
+int p3mg_kernel_times(p3mg_ctx *ctx, double t[3]);
+
+/* Replay p3mg_compute as a CUDA graph: the first step for a given particle
+ * count and rcut runs eagerly, the next is captured, later ones replay the
+ * graph (one launch instead of ~20).  Off by default; stage timing
+ * disables it.  No reference counterpart (the reference is single-threaded C). */
+int p3mg_set_graph(p3mg_ctx *ctx, int on);
+
+/* Number of CUDA kernels this context has launched so far. */
+int p3mg_launch_count(p3mg_ctx *ctx, long long *count);
+
 /* The context's CUDA stream (cudaStream_t) as an opaque pointer. */
 void *p3mg_stream(p3mg_ctx *ctx);
 

@@ -49,6 +49,7 @@ int combine_forces(Ctx *c) {
   const size_t n3 = 3 * (size_t)c->n;
   if (n3 == 0) return P3MG_OK;
   combine_kernel<<<(unsigned)((n3 + 255) / 256), 256, 0, c->stream>>>(c->f, c->fk, c->fr, n3);
+  c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -118,43 +119,100 @@ int free_all(Ctx *c) {
   dfree(c->self_b);
   dfree(c->scan_tmp);
   fft_plan_free(c);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
   if (c->ev_ok)
-    for (int i = 0; i < 5; i++) cudaEventDestroy(c->ev[i]);
+    for (int i = 0; i < 12; i++) cudaEventDestroy(c->ev[i]);
   c->ev_ok = false;
   if (c->stream) cudaStreamDestroy(c->stream);
   c->stream = nullptr;
   return P3MG_OK;
 }
 
-static int step_device(Ctx *c, double rcut) {
+// Enqueue one force evaluation on the context stream (Calculate_forces,
+// common.c:268-327): zero, real space (rcut != 0, common.c:290-294),
+// k-space with self-force, f += f_k + f_r.
+static int enqueue_step(Ctx *c, double rcut) {
   P3MG_TRY(zero_forces(c));
-  if (c->timing && c->ev_ok) cudaEventRecord(c->ev[4], c->stream);
-  // real space when rcut != 0 (common.c:290-294)
+  const bool timed = c->timing && c->ev_ok && c->n > 0;
+  if (timed) {
+    // brackets of stages that may not run this step must still be recorded
+    for (int s = EV_K0; s <= EV_K5; s++) cudaEventRecord(c->ev[s], c->stream);
+  }
+  mark(c, EV_S0);
   if (rcut != 0.0) P3MG_TRY(pairs_run(c, rcut, c->alpha));
+  mark(c, EV_S1);
   if (c->n > 0) {
     P3MG_TRY(kspace_prepare(c));
     P3MG_TRY(kspace_run(c));
   }
   P3MG_TRY(combine_forces(c));
-  c->stage_pending = c->timing && c->ev_ok;
+  c->stage_pending = timed;
   return P3MG_OK;
 }
 
 static void collect_stage_times(Ctx *c) {
   if (!c->stage_pending) return;
-  cudaEventSynchronize(c->ev[3]);
+  cudaEventSynchronize(c->ev[EV_S4]);
   float t;
-  // ev[4] start of pairs, ev[0] start of scatter (after binning), ev[1] end
-  // of scatter, ev[2] end of FFT/convolution, ev[3] end of gather
-  if (cudaEventElapsedTime(&t, c->ev[4], c->ev[0]) == cudaSuccess) c->stage_ms[3] = t;
-  if (cudaEventElapsedTime(&t, c->ev[0], c->ev[1]) == cudaSuccess) c->stage_ms[0] = t;
-  if (cudaEventElapsedTime(&t, c->ev[1], c->ev[2]) == cudaSuccess) c->stage_ms[1] = t;
-  if (cudaEventElapsedTime(&t, c->ev[2], c->ev[3]) == cudaSuccess) c->stage_ms[2] = t;
+  const int st[4][2] = {{EV_S1, EV_S2}, {EV_S2, EV_S3}, {EV_S3, EV_S4}, {EV_S0, EV_S1}};
+  for (int i = 0; i < 4; i++)
+    if (cudaEventElapsedTime(&t, c->ev[st[i][0]], c->ev[st[i][1]]) == cudaSuccess) c->stage_ms[i] = t;
+  const int kt[3][2] = {{EV_K0, EV_K1}, {EV_K2, EV_K3}, {EV_K4, EV_K5}};
+  for (int i = 0; i < 3; i++)
+    if (cudaEventElapsedTime(&t, c->ev[kt[i][0]], c->ev[kt[i][1]]) == cudaSuccess) c->kernel_ms[i] = t;
   c->stage_pending = false;
 }
 
-static int check_ctx(Ctx *c) {
-  if (!c) return P3MG_ERR_ARG;
+static void drop_graph(Ctx *c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
+  c->graph_rcut = -1.0;
+  c->graph_n = -1;
+}
+
+// One step: eager, or replay of a captured CUDA graph when graphs are on.
+// The first step for a given (n, rcut) runs eagerly (allocations, function
+// attributes), the second captures and replays, later ones replay.
+static int step_device(Ctx *c, double rcut) {
+  if (!c->use_graph || c->timing) return enqueue_step(c, rcut);
+  if (c->gexec && c->graph_rcut == rcut && c->graph_n == c->n) {
+    P3MG_CUDA_TRY(cudaGraphLaunch(c->gexec, c->stream));
+    c->launches += c->graph_launches;
+    return P3MG_OK;
+  }
+  if (c->graph_rcut != rcut || c->graph_n != c->n) {
+    // eager warm-up for this shape; capture on the next call
+    drop_graph(c);
+    P3MG_TRY(pairs_reserve(c, rcut));
+    c->graph_rcut = rcut;
+    c->graph_n = c->n;
+    return enqueue_step(c, rcut);
+  }
+  cudaGraph_t g = nullptr;
+  P3MG_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  const long long before = c->launches;
+  int st = enqueue_step(c, rcut);
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (st != P3MG_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  if (e != cudaSuccess) {
+    record_cuda_error(e);
+    return P3MG_ERR_CUDA;
+  }
+  c->graph_launches = c->launches - before;
+  c->launches = before;
+  e = cudaGraphInstantiate(&c->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->gexec = nullptr;
+    record_cuda_error(e);
+    return P3MG_ERR_CUDA;
+  }
+  P3MG_CUDA_TRY(cudaGraphLaunch(c->gexec, c->stream));
+  c->launches += c->graph_launches;
   return P3MG_OK;
 }
 
@@ -252,7 +310,7 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     st = fft_plan_init(c);
     if (st != P3MG_OK) break;
     c->ev_ok = true;
-    for (int i = 0; i < 5; i++)
+    for (int i = 0; i < 12; i++)
       if (cudaEventCreate(&c->ev[i]) != cudaSuccess) c->ev_ok = false;
   } while (0);
   if (st != P3MG_OK) {
@@ -277,7 +335,10 @@ static int set_system_common(Ctx *c, int n, const double *x, const double *y, co
   if (n < 0 || !(L > 0.0) || !isfinite(L)) return P3MG_ERR_ARG;
   if (n > 0 && (!x || !y || !z || !q)) return P3MG_ERR_ARG;
   cudaSetDevice(c->device);
+  const bool same_shape = (n == c->n) && c->x != nullptr;
+  if (!same_shape) drop_graph(c);  // a captured step holds the old buffers and sizes
   P3MG_TRY(alloc_system(c, n));
+  if (L != c->L) c->have_G = false;  // G_opt and the self-force depend on L
   c->L = L;
   const size_t b = (size_t)n * sizeof(double);
   if (n > 0) {
@@ -286,7 +347,6 @@ static int set_system_common(Ctx *c, int n, const double *x, const double *y, co
     P3MG_CUDA_TRY(cudaMemcpyAsync(c->z, z, b, kind, c->stream));
     P3MG_CUDA_TRY(cudaMemcpyAsync(c->q, q, b, kind, c->stream));
   }
-  c->have_G = false;  // G depends on L
   return P3MG_OK;
 }
 
@@ -437,5 +497,25 @@ int p3mg_get_influence(p3mg_ctx *h, double *G, double *self81) {
 }
 
 void *p3mg_stream(p3mg_ctx *h) { return h ? (void *)h->c.stream : nullptr; }
+
+int p3mg_set_graph(p3mg_ctx *h, int on) {
+  if (!h) return P3MG_ERR_ARG;
+  h->c.use_graph = on != 0;
+  if (!h->c.use_graph) drop_graph(&h->c);
+  return P3MG_OK;
+}
+
+int p3mg_launch_count(p3mg_ctx *h, long long *count) {
+  if (!h || !count) return P3MG_ERR_ARG;
+  *count = h->c.launches;
+  return P3MG_OK;
+}
+
+int p3mg_kernel_times(p3mg_ctx *h, double t[3]) {
+  if (!h || !t) return P3MG_ERR_ARG;
+  collect_stage_times(&h->c);
+  for (int i = 0; i < 3; i++) t[i] = h->c.kernel_ms[i];
+  return P3MG_OK;
+}
 
 }  // extern "C"

@@ -100,12 +100,14 @@ __global__ void g_to_f32_kernel(const double *__restrict__ G, float *__restrict_
 int g_to_f32(Ctx *c) {
   const int threads = 256;
   g_to_f32_kernel<<<(unsigned)((c->M + threads - 1) / threads), threads, 0, c->stream>>>(c->G, c->G32, c->M);
+  c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
 
 int exclusive_scan(Ctx *c, const int *counts, int *start, int nb) {
   scan_kernel<<<1, 1024, 0, c->stream>>>(counts, start, nb);
+  c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -123,12 +125,14 @@ int kspace_prepare(Ctx *c) {
   if (c->n > 0) {
     bin_bricks_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->n, Hi, shift, c->mesh, c->brick, nb,
                                                          c->part_key, c->brick_count);
+    c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
   }
   P3MG_TRY(exclusive_scan(c, c->brick_count, c->brick_start, nbr));
   if (c->n > 0) {
     place_bricks_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, c->part_key, c->brick_start,
                                                            c->brick_fill, c->sorted_idx, c->sorted_xyzq);
+    c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
   }
   return P3MG_OK;

@@ -231,12 +231,21 @@ template <typename real, int CAO, int NMESH>
 int launch_scatter(Ctx *c, size_t smem) {
   typedef typename cplx<real>::type C;
   auto kern = scatter_kernel<real, CAO, NMESH>;
-  P3MG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // raise the dynamic shared-memory limit once per instantiation (outside
+  // any graph capture: the first step of a shape always runs eagerly)
+  static size_t smem_set = 0;
+  if (smem > smem_set) {
+    P3MG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    smem_set = 200 * 1024;
+  }
   const double Hi = (double)c->mesh / c->L;
   const double shift = (double)((c->cao - 1) / 2);
   const int nbr = c->nbrick1 * c->nbrick1 * c->nbrick1;
+  mark(c, EV_K2);
   kern<<<nbr, ASSIGN_THREADS, smem, c->stream>>>(c->sorted_xyzq, c->brick_start, c->mesh, c->brick, c->nbrick1, Hi,
                                                 shift, reinterpret_cast<C *>(c->Q));
+  c->launches++;
+  mark(c, EV_K3);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -260,6 +269,7 @@ int dispatch_gather(Ctx *c) {
   const int blocks = (c->n + ASSIGN_THREADS - 1) / ASSIGN_THREADS;
   const bool il = method_interlaced(c->method);
   const C *F = reinterpret_cast<const C *>(method_ad(c->method) ? c->Q : c->F);
+  mark(c, EV_K4);
   if (method_ad(c->method)) {
     // prefactor Mesh * Leni^3 (p3m-ad.c:202, p3m-ad-i.c:199, p3m-ad-real.c:110)
     const double pref = (double)c->mesh * Leni * Leni * Leni;
@@ -279,6 +289,8 @@ int dispatch_gather(Ctx *c) {
       gather_kernel<real, CAO, 1, false><<<blocks, ASSIGN_THREADS, 0, c->stream>>>(
           c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, F, c->M, c->fk, c->n);
   }
+  c->launches++;
+  mark(c, EV_K5);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -289,8 +301,7 @@ int run_kspace(Ctx *c) {
   const size_t M = c->M;
   const int threads = 256;
   const unsigned mblocks = (unsigned)((M + threads - 1) / threads);
-  // charge assignment
-  if (c->timing) cudaEventRecord(c->ev[0], c->stream);
+  // charge assignment (the brick binning ran in kspace_prepare)
   P3MG_CUDA_TRY(cudaMemsetAsync(c->Q, 0, M * sizeof(C), c->stream));
   switch (c->cao) {
     case 1: P3MG_TRY((dispatch_scatter<real, 1>(c))); break;
@@ -301,7 +312,7 @@ int run_kspace(Ctx *c) {
     case 6: P3MG_TRY((dispatch_scatter<real, 6>(c))); break;
     case 7: P3MG_TRY((dispatch_scatter<real, 7>(c))); break;
   }
-  if (c->timing) cudaEventRecord(c->ev[1], c->stream);
+  mark(c, EV_S2);
   // forward FFT, convolution, backward FFT(s)
   P3MG_TRY(fft3d(c, c->Q, 1, -1));
   if (method_ad(c->method)) {
@@ -309,6 +320,7 @@ int run_kspace(Ctx *c) {
       conv_ad_kernel<real, double><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<C *>(c->Q), c->G, M);
     else
       conv_ad_kernel<real, float><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<C *>(c->Q), c->G32, M);
+    c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
     P3MG_TRY(fft3d(c, c->Q, 1, +1));
   } else {
@@ -319,10 +331,11 @@ int run_kspace(Ctx *c) {
     else
       conv_ik_kernel<real, float><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), c->G32,
                                                                       c->mesh, s, M, reinterpret_cast<C *>(c->F));
+    c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
     P3MG_TRY(fft3d(c, c->F, 3, +1));
   }
-  if (c->timing) cudaEventRecord(c->ev[2], c->stream);
+  mark(c, EV_S3);
   // back-interpolation
   switch (c->cao) {
     case 1: P3MG_TRY((dispatch_gather<real, 1>(c))); break;
@@ -337,9 +350,10 @@ int run_kspace(Ctx *c) {
     const int blocks = (c->n + threads - 1) / threads;
     self_force_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, c->L / c->mesh, c->self_b,
                                                           c->f);
+    c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
   }
-  if (c->timing) cudaEventRecord(c->ev[3], c->stream);
+  mark(c, EV_S4);
   return P3MG_OK;
 }
 

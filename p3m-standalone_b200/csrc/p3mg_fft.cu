@@ -234,6 +234,7 @@ int launch_fft3d(Ctx *c, void *data, int nbatch, int sign) {
     fft_axis_kernel<real, 1><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
     fft_axis_kernel<real, 0><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
   }
+  c->launches += 3;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }

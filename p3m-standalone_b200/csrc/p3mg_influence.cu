@@ -180,6 +180,7 @@ int influence_compute(Ctx *c, double alpha) {
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
   influence_kernel<<<blocks, threads, 0, c->stream>>>(c->G, c->method, m, c->cao, c->mc, alpha, c->L);
+  c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   if (c->precision != P3MG_FP64) {
     // FP32 copy of G for the mixed-precision convolution
@@ -192,6 +193,7 @@ int influence_compute(Ctx *c, double alpha) {
     double *S26 = c->self_b;  // use the first 26 slots as the accumulator
     P3MG_CUDA_TRY(cudaMemsetAsync(S26, 0, 26 * sizeof(double), c->stream));
     self_force_sum_kernel<<<blocks, threads, 0, c->stream>>>(c->G, m, c->cao, S26);
+    c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
     double S[26];
     P3MG_CUDA_TRY(cudaMemcpyAsync(S, S26, sizeof(S), cudaMemcpyDeviceToHost, c->stream));

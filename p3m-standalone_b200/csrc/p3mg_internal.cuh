@@ -101,16 +101,46 @@ struct Ctx {
   double alpha = 0.0;
   bool have_G = false;
 
-  // timing
+  // timing: CUDA events on the context stream (see EV_* below)
   bool timing = false;
-  cudaEvent_t ev[5];
+  cudaEvent_t ev[12];
   bool ev_ok = false;
-  double stage_ms[4] = {0, 0, 0, 0};
+  double stage_ms[4] = {0, 0, 0, 0};   // t_c, t_g, t_f, t_r
+  double kernel_ms[3] = {0, 0, 0};     // pair kernel, scatter kernel, gather kernel
   bool stage_pending = false;
+
+  // kernels launched by this context (host-side count)
+  long long launches = 0;
+
+  // CUDA graph of one p3mg_compute step (replayed when the same rcut/n repeat)
+  bool use_graph = false;
+  cudaGraphExec_t gexec = nullptr;
+  double graph_rcut = -1.0;
+  int graph_n = -1;
+  long long graph_launches = 0;  // kernels per replay
 
   // scratch for a single-CTA scan
   int *scan_tmp = nullptr;
 };
+
+// event slots: stage markers and kernel brackets
+enum {
+  EV_S0 = 0,   // step start
+  EV_S1 = 1,   // after real space
+  EV_S2 = 2,   // after binning + charge assignment
+  EV_S3 = 3,   // after FFTs + convolution
+  EV_S4 = 4,   // after back-interpolation + self-force
+  EV_K0 = 5,   // pair kernel start / end
+  EV_K1 = 6,
+  EV_K2 = 7,   // scatter kernel start / end
+  EV_K3 = 8,
+  EV_K4 = 9,   // gather kernel start / end
+  EV_K5 = 10,
+};
+
+inline void mark(Ctx *c, int slot) {
+  if (c->timing && c->ev_ok) cudaEventRecord(c->ev[slot], c->stream);
+}
 
 int alloc_system(Ctx *c, int n);
 int free_all(Ctx *c);
@@ -129,6 +159,7 @@ int kspace_prepare(Ctx *c);
 int kspace_run(Ctx *c);  // scatter, FFTs, convolution, gather, self-force into c->fk / c->f
 
 // real space (p3mg_pairs.cu)
+int pairs_reserve(Ctx *c, double rcut);
 int pairs_run(Ctx *c, double rcut, double alpha);
 
 // misc kernels (p3mg_api.cu)

@@ -268,34 +268,54 @@ __global__ void __launch_bounds__(BRUTE_THREADS) pairs_brute_kernel(const double
 
 }  // namespace
 
-int pairs_run(Ctx *c, double rcut, double alpha) {
-  const int n = c->n;
-  if (n == 0 || rcut <= 0.0) return P3MG_OK;
-  int nc = (int)floor(c->L / rcut);
-  if (nc > 256) nc = 256;
-  const int threads = 256;
-  const int blocks = (n + threads - 1) / threads;
-  if (nc < 3) {
-    pairs_brute_kernel<<<blocks, BRUTE_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, rcut, alpha, c->fr,
-                                                                 c->energy);
-    P3MG_CUDA_TRY(cudaGetLastError());
-    return P3MG_OK;
-  }
+static int cells_per_side(double L, double rcut) {
+  int nc = (int)floor(L / rcut);
+  return nc > 256 ? 256 : nc;
+}
+
+// Allocate the cell-list arrays for this rcut (host-side; called before a
+// step is captured into a CUDA graph).
+int pairs_reserve(Ctx *c, double rcut) {
+  if (c->n == 0 || rcut <= 0.0) return P3MG_OK;
+  const int nc = cells_per_side(c->L, rcut);
+  if (nc < 3) return P3MG_OK;
   const int ncell = nc * nc * nc;
   if (ncell > c->ncell_cap) {
     if (c->cell_count) cudaFree(c->cell_count);
     if (c->cell_start) cudaFree(c->cell_start);
     if (c->cell_fill) cudaFree(c->cell_fill);
     c->cell_count = c->cell_start = c->cell_fill = nullptr;
+    c->ncell_cap = 0;
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_count, sizeof(int) * ncell));
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_start, sizeof(int) * (ncell + 1)));
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_fill, sizeof(int) * ncell));
     c->ncell_cap = ncell;
   }
+  return P3MG_OK;
+}
+
+int pairs_run(Ctx *c, double rcut, double alpha) {
+  const int n = c->n;
+  if (n == 0 || rcut <= 0.0) return P3MG_OK;
+  const int nc = cells_per_side(c->L, rcut);
+  const int threads = 256;
+  const int blocks = (n + threads - 1) / threads;
+  if (nc < 3) {
+    mark(c, EV_K0);
+    pairs_brute_kernel<<<blocks, BRUTE_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, rcut, alpha, c->fr,
+                                                                 c->energy);
+    c->launches++;
+    mark(c, EV_K1);
+    P3MG_CUDA_TRY(cudaGetLastError());
+    return P3MG_OK;
+  }
+  const int ncell = nc * nc * nc;
+  P3MG_TRY(pairs_reserve(c, rcut));
   c->ncell1 = nc;
   P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_count, 0, sizeof(int) * ncell, c->stream));
   P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_fill, 0, sizeof(int) * ncell, c->stream));
   bin_cells_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, n, c->L, nc, c->cell_key, c->cell_count);
+  c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   P3MG_TRY(exclusive_scan(c, c->cell_count, c->cell_start, ncell));
   if (c->precision == P3MG_FP64) {
@@ -303,6 +323,7 @@ int pairs_run(Ctx *c, double rcut, double alpha) {
                                                                    c->cell_start, c->cell_fill, c->cell_idx,
                                                                    reinterpret_cast<double4 *>(c->cell_pos));
     P3MG_CUDA_TRY(cudaGetLastError());
+    mark(c, EV_K0);
     pairs_fp64_kernel<<<ncell, PAIR_THREADS, 0, c->stream>>>(reinterpret_cast<const double4 *>(c->cell_pos),
                                                              c->cell_idx, c->cell_start, nc, c->L, rcut, alpha, c->fr,
                                                              n, c->energy);
@@ -311,10 +332,13 @@ int pairs_run(Ctx *c, double rcut, double alpha) {
                                                                   c->cell_start, c->cell_fill, c->cell_idx,
                                                                   reinterpret_cast<float4 *>(c->cell_pos));
     P3MG_CUDA_TRY(cudaGetLastError());
+    mark(c, EV_K0);
     pairs_fp32_kernel<<<ncell, PAIR_THREADS, 0, c->stream>>>(reinterpret_cast<const float4 *>(c->cell_pos),
                                                              c->cell_idx, c->cell_start, nc, (float)(c->L / nc),
                                                              (float)rcut, (float)alpha, c->fr, n, c->energy);
   }
+  c->launches += 2;
+  mark(c, EV_K1);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }

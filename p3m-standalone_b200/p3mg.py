@@ -88,6 +88,9 @@ def load():
     L.p3mg_enable_timing.argtypes = [vp, ctypes.c_int]
     L.p3mg_stage_times.argtypes = [vp, _dp]
     L.p3mg_get_influence.argtypes = [vp, _dp, _dp]
+    L.p3mg_kernel_times.argtypes = [vp, _dp]
+    L.p3mg_set_graph.argtypes = [vp, ctypes.c_int]
+    L.p3mg_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.p3mg_stream.argtypes = [vp]
     L.p3mg_stream.restype = vp
     L.p3mg_strerror.argtypes = [ctypes.c_int]
@@ -211,6 +214,31 @@ class Context:
         t = np.zeros(4)
         _check(self._lib.p3mg_stage_times(self._h, _p(t)), "p3mg_stage_times")
         return dict(t_c=t[0], t_g=t[1], t_f=t[2], t_r=t[3])
+
+    def kernel_times(self):
+        t = np.zeros(3)
+        _check(self._lib.p3mg_kernel_times(self._h, _p(t)), "p3mg_kernel_times")
+        return dict(pairs=t[0], scatter=t[1], gather=t[2])
+
+    def set_graph(self, on=True):
+        _check(self._lib.p3mg_set_graph(self._h, int(bool(on))), "p3mg_set_graph")
+
+    def launch_count(self):
+        c = ctypes.c_longlong(0)
+        _check(self._lib.p3mg_launch_count(self._h, ctypes.byref(c)), "p3mg_launch_count")
+        return int(c.value)
+
+    def set_system_ptr(self, n, px, py, pz, pq, L):
+        """Host pointers (ints, e.g. pinned torch tensors) to n doubles each."""
+        P = lambda v: ctypes.cast(ctypes.c_void_p(v), _dp)  # noqa: E731
+        _check(self._lib.p3mg_set_system(self._h, int(n), P(px), P(py), P(pz), P(pq), float(L)), "p3mg_set_system")
+        self.n, self.L = int(n), float(L)
+
+    def get_total_forces_ptr(self, px, py, pz):
+        """Copy the total force of the last compute to host pointers (ints)."""
+        P = lambda v: ctypes.cast(ctypes.c_void_p(v), _dp)  # noqa: E731
+        _check(self._lib.p3mg_get_forces(self._h, P(px), P(py), P(pz), None, None, None, None, None, None, None),
+               "p3mg_get_forces")
 
     def get_influence(self):
         G = np.zeros(self.mesh ** 3)
