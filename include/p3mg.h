@@ -140,6 +140,29 @@ int p3mg_kernel_times(p3mg_ctx *ctx, double t[3]);
  * disables it.  No reference counterpart (the reference is single-threaded C). */
 int p3mg_set_graph(p3mg_ctx *ctx, int on);
 
+/* Real-space erfc pair forces that allocate no device memory.
+ * No counterpart in the reference (its Realteil, realpart.c:124-167, is the
+ * computation; this entry point only changes who owns the memory).
+ * For callers that cannot let a library allocate GPU memory: an engine
+ * whose allocator owns all device memory (a library cudaMalloc would
+ * synchronise the device and fragment its pool), or a stepping loop that
+ * must not allocate after start-up.  The caller passes device-accessible
+ * inputs x, y, z, q (n doubles each), the output fr (3n doubles: x block,
+ * y block, z block; forces are ADDED, like Realteil) and energy (one double,
+ * the pair energy is ADDED), and a cudaStream_t (NULL = default stream).
+ * The cell list lives in one static device array of
+ * P3MG_NOALLOC_SCRATCH_BYTES in the library, held by every GPU that loads
+ * it until the process exits; n above P3MG_NOALLOC_MAX_PARTICLES returns
+ * P3MG_ERR_NOBUF.  The first call on a device looks up that array's device
+ * address (make it before any stream capture).  Calls share the array:
+ * calls that overlap on the GPU race and corrupt each other's results.
+ * The call is asynchronous on the given stream. */
+#define P3MG_NOALLOC_MAX_PARTICLES 131072
+#define P3MG_NOALLOC_MAX_CELLS 32768
+#define P3MG_NOALLOC_SCRATCH_BYTES (6u << 20)
+int p3mg_real_forces_noalloc(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                             double rcut, double alpha, int precision, double *fr, double *energy, void *stream);
+
 /* Number of CUDA kernels this context has launched so far. */
 int p3mg_launch_count(p3mg_ctx *ctx, long long *count);
 

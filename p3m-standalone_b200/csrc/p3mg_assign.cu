@@ -105,6 +105,12 @@ int g_to_f32(Ctx *c) {
   return P3MG_OK;
 }
 
+int scan_counts(const int *counts, int *start, int nb, cudaStream_t stream) {
+  scan_kernel<<<1, 1024, 0, stream>>>(counts, start, nb);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
 int exclusive_scan(Ctx *c, const int *counts, int *start, int nb) {
   scan_kernel<<<1, 1024, 0, c->stream>>>(counts, start, nb);
   c->launches++;

@@ -171,6 +171,7 @@ int g_to_f32(Ctx *c);
 
 // single-CTA exclusive scan of counts[0..nb) into start[0..nb] (start[nb] = total)
 int exclusive_scan(Ctx *c, const int *counts, int *start, int nb);
+int scan_counts(const int *counts, int *start, int nb, cudaStream_t stream);
 
 // ------------------------------------------------------------ device helpers
 

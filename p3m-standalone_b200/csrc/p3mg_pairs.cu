@@ -343,4 +343,116 @@ int pairs_run(Ctx *c, double rcut, double alpha) {
   return P3MG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Real-space pair forces without any device allocation.
+//
+// Some callers cannot let a library allocate device memory: an MD engine or
+// framework that owns all device memory through its own pool (a cudaMalloc
+// from the library would synchronise the device and fragment that pool),
+// or a time-stepping loop that fixes its memory at start-up and must not
+// allocate afterwards.  p3mg_real_forces_noalloc serves them: the caller
+// passes device-accessible inputs and outputs and a stream, and the cell
+// list lives in the file-scope array below, which is part of the loaded
+// module (every GPU that loads the library holds it until the process
+// exits).  Its capacity bounds the particle count; the cell grid is capped
+// so that it fits as well (cells stay at least rcut wide, so the pairs found
+// are the same).  All calls on a device share the one array and it keeps
+// the previous call's contents: the per-call counters are cleared on the
+// caller's stream before use, and calls that overlap on the GPU (different
+// streams, or host threads racing) corrupt each other's cell lists.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr size_t NA_CELL_BYTES = sizeof(int) * (size_t)P3MG_NOALLOC_MAX_CELLS;
+constexpr size_t NA_PART_INT_BYTES = sizeof(int) * (size_t)P3MG_NOALLOC_MAX_PARTICLES;
+constexpr size_t na_round(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t NA_OFF_COUNT = 0;
+constexpr size_t NA_OFF_START = NA_OFF_COUNT + na_round(NA_CELL_BYTES);
+constexpr size_t NA_OFF_FILL = NA_OFF_START + na_round(NA_CELL_BYTES + sizeof(int));
+constexpr size_t NA_OFF_KEY = NA_OFF_FILL + na_round(NA_CELL_BYTES);
+constexpr size_t NA_OFF_IDX = NA_OFF_KEY + na_round(NA_PART_INT_BYTES);
+constexpr size_t NA_OFF_POS = NA_OFF_IDX + na_round(NA_PART_INT_BYTES);
+constexpr size_t NA_BYTES = NA_OFF_POS + na_round(sizeof(double4) * (size_t)P3MG_NOALLOC_MAX_PARTICLES);
+static_assert(NA_BYTES <= (size_t)P3MG_NOALLOC_SCRATCH_BYTES, "no-alloc scratch layout exceeds its array");
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[P3MG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int NA_MAX_DEVICES = 64;
+unsigned char *g_na_ptr[NA_MAX_DEVICES] = {nullptr};
+
+// Device address of the scratch array for the current device.  In host
+// code the symbol name only stands for the array, it is not an address the
+// GPU can use, so the address is looked up once per device (with that
+// device current) and cached.
+int noalloc_scratch(unsigned char **out) {
+  int dev = 0;
+  P3MG_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NA_MAX_DEVICES) return P3MG_ERR_ARG;
+  if (!g_na_ptr[dev]) {
+    void *p = nullptr;
+    P3MG_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_na_ptr[dev] = (unsigned char *)p;
+  }
+  *out = g_na_ptr[dev];
+  return P3MG_OK;
+}
+
+}  // namespace
+
 }  // namespace p3mg
+
+extern "C" int p3mg_real_forces_noalloc(int n, const double *x, const double *y, const double *z, const double *q,
+                                        double L, double rcut, double alpha, int precision, double *fr, double *energy,
+                                        void *stream) {
+  using namespace p3mg;
+  if (n < 0 || !(L > 0.0) || !(rcut >= 0.0) || !(alpha >= 0.0)) return P3MG_ERR_ARG;
+  if (precision != P3MG_FP64 && precision != P3MG_FP32_MIXED) return P3MG_ERR_PRECISION;
+  if (n > P3MG_NOALLOC_MAX_PARTICLES) return P3MG_ERR_NOBUF;
+  if (n == 0 || rcut == 0.0) return P3MG_OK;
+  if (!x || !y || !z || !q || !fr || !energy) return P3MG_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char *base = nullptr;
+  P3MG_TRY(noalloc_scratch(&base));
+  const int threads = 256;
+  const int blocks = (n + threads - 1) / threads;
+  int nc = cells_per_side(L, rcut);
+  if (nc < 3) {
+    pairs_brute_kernel<<<blocks, BRUTE_THREADS, 0, s>>>(x, y, z, q, n, L, rcut, alpha, fr, energy);
+    P3MG_CUDA_TRY(cudaGetLastError());
+    return P3MG_OK;
+  }
+  while (nc > 3 && nc * nc * nc > P3MG_NOALLOC_MAX_CELLS) nc--;
+  const int ncell = nc * nc * nc;
+  int *count = (int *)(base + NA_OFF_COUNT);
+  int *start = (int *)(base + NA_OFF_START);
+  int *fill = (int *)(base + NA_OFF_FILL);
+  int *key = (int *)(base + NA_OFF_KEY);
+  int *idx = (int *)(base + NA_OFF_IDX);
+  void *pos = (void *)(base + NA_OFF_POS);
+  // the array keeps the previous call's counters: clear them first
+  P3MG_CUDA_TRY(cudaMemsetAsync(count, 0, sizeof(int) * ncell, s));
+  P3MG_CUDA_TRY(cudaMemsetAsync(fill, 0, sizeof(int) * ncell, s));
+  bin_cells_kernel<<<blocks, threads, 0, s>>>(x, y, z, n, L, nc, key, count);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  P3MG_TRY(scan_counts(count, start, ncell, s));
+  if (precision == P3MG_FP64) {
+    place_cells_kernel<double4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
+                                                           reinterpret_cast<double4 *>(pos));
+    P3MG_CUDA_TRY(cudaGetLastError());
+    pairs_fp64_kernel<<<ncell, PAIR_THREADS, 0, s>>>(reinterpret_cast<const double4 *>(pos), idx, start, nc, L, rcut,
+                                                     alpha, fr, n, energy);
+  } else {
+    place_cells_kernel<float4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
+                                                          reinterpret_cast<float4 *>(pos));
+    P3MG_CUDA_TRY(cudaGetLastError());
+    pairs_fp32_kernel<<<ncell, PAIR_THREADS, 0, s>>>(reinterpret_cast<const float4 *>(pos), idx, start, nc,
+                                                     (float)(L / nc), (float)rcut, (float)alpha, fr, n, energy);
+  }
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
