@@ -262,7 +262,7 @@ def run_ours(args, rank, world, local_rank):
         else:
             abytes = 16 * n + 7 * n * s  # float4 cell-sorted particles in, forces out
         achieved = abytes / (k[dom] * 1e-3) / 1e9
-        kernel_names = {"gather": "gather_kernel", "scatter": "scatter_kernel", "pairs": "pairs_fp32_kernel"}
+        kernel_names = {"gather": "gather_kernel", "scatter": "scatter_kernel", "pairs": "pairs_cell_kernel"}
         traffic = profile_traffic(kernel_names[dom])
         out = {
             "metric": METRIC,

@@ -114,10 +114,12 @@ int free_all(Ctx *c) {
   dfree(c->cell_pos);
   dfree(c->Q);
   dfree(c->F);
+  dfree(c->P);
   dfree(c->G);
   dfree(c->G32);
   dfree(c->self_b);
   dfree(c->scan_tmp);
+  dfree(c->scatter_tab);
   fft_plan_free(c);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   c->gexec = nullptr;
@@ -294,6 +296,7 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     ALLOC(c->Q, c->M * csz);
     if (!method_ad(method_id)) {
       ALLOC(c->F, 3 * c->M * csz);
+      ALLOC(c->P, (method_interlaced(method_id) ? 2 : 1) * c->M * 2 * csz);
     }
     ALLOC(c->G, c->M * sizeof(double));
     if (precision != P3MG_FP64) {

@@ -15,57 +15,103 @@ __host__ __device__ inline int brick_tile(int B, int cao, int nmesh) { return B 
 
 // ---------------------------------------------------------------- scatter
 
+// particles staged per round of the scatter (weights and tile offsets)
+constexpr int SCATTER_CHUNK = 128;
+
+template <typename real, int CAO, int NMESH>
+__host__ __device__ constexpr size_t scatter_stage_bytes() {
+  return (size_t)NMESH * SCATTER_CHUNK * (3 * CAO * sizeof(real) + sizeof(int));
+}
+
+// One CTA per mesh brick.  Round by round, SCATTER_CHUNK particles of the
+// brick are staged: one thread per particle computes its stencil origin in
+// the tile and its B-spline weights (charge folded into the x weights) for
+// each mesh.  Then each warp deposits whole particles: its 32 lanes take
+// distinct stencil points (a, b, c) of the same particle, so the shared-
+// memory atomics of one instruction never hit the same address.  The tile
+// is added to the global mesh at the end (periodic wrap, one global atomic
+// per non-zero tile point).
 template <typename real, int CAO, int NMESH>
 __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *__restrict__ sxyzq,
                                                                   const int *__restrict__ start, int m, int B, int nb,
-                                                                  double Hi, double shift,
+                                                                  double Hi, double shift, int SR, int SP,
+                                                                  const int2 *__restrict__ lanetab,
                                                                   typename cplx<real>::type *__restrict__ Q) {
-  extern __shared__ unsigned char smem_raw[];
-  real *tile0 = reinterpret_cast<real *>(smem_raw);
+  constexpr int S = CAO * CAO * CAO;
+  constexpr int IT = (S + 31) / 32;  // points per lane: the host picks pitches with even bank classes
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int T = brick_tile(B, CAO, NMESH);
-  const int T3 = T * T * T;
+  const int T3 = T * SP;  // tile elements: T planes of pitch SP, rows of pitch SR
+  real *tile0 = reinterpret_cast<real *>(smem_raw);
   real *tile1 = tile0 + T3;
+  real *sw = tile0 + NMESH * T3;                                   // [NMESH*CHUNK][3][CAO]
+  int *soff = reinterpret_cast<int *>(sw + NMESH * SCATTER_CHUNK * 3 * CAO);  // tile offset of the stencil origin
   const int bid = blockIdx.x;
   const int p0 = start[bid], p1 = start[bid + 1];
   if (p0 == p1) return;
   for (int t = threadIdx.x; t < NMESH * T3; t += blockDim.x) tile0[t] = (real)0;
-  __syncthreads();
   const int bz = bid % nb, by = (bid / nb) % nb, bx = bid / (nb * nb);
   const int o0 = bx * B, o1 = by * B, o2 = bz * B;
-  for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-    const double4 r = sxyzq[p];
-    const real qp = (real)r.w;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  // This lane's stencil points (tile offset, packed a/b/c), from the host
+  // table that assigns each lane the points of one shared-memory bank class
+  // (scatter_lane_table): the 32 atomics of one instruction hit 32 banks.
+  int loff[IT], labc[IT];
 #pragma unroll
-    for (int ii = 0; ii < NMESH; ii++) {
-      int base[3], arg[3];
-      mesh_geometry(r.x, Hi, shift, ii, m, &base[0], &arg[0]);
-      mesh_geometry(r.y, Hi, shift, ii, m, &base[1], &arg[1]);
-      mesh_geometry(r.z, Hi, shift, ii, m, &base[2], &arg[2]);
-      int rel0 = base[0] - o0, rel1 = base[1] - o1, rel2 = base[2] - o2;
-      rel0 += (rel0 < 0) ? m : 0;
-      rel1 += (rel1 < 0) ? m : 0;
-      rel2 += (rel2 < 0) ? m : 0;
-      real wx[CAO], wy[CAO], wz[CAO];
-      bspline_weights<real, CAO, false>(arg[0], wx, nullptr);
-      bspline_weights<real, CAO, false>(arg[1], wy, nullptr);
-      bspline_weights<real, CAO, false>(arg[2], wz, nullptr);
-      real *tile = ii ? tile1 : tile0;
+  for (int it = 0; it < IT; it++) {
+    const int2 e = lanetab[it * 32 + lane];
+    loff[it] = e.x;
+    labc[it] = e.y;
+  }
+  for (int pc = p0; pc < p1; pc += SCATTER_CHUNK) {
+    const int cnt = min(SCATTER_CHUNK, p1 - pc);
+    __syncthreads();
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      const double4 r = sxyzq[pc + t];
 #pragma unroll
-      for (int a = 0; a < CAO; a++) {
-        const real qa = qp * wx[a];
+      for (int ii = 0; ii < NMESH; ii++) {
+        int base[3], arg[3];
+        mesh_geometry(r.x, Hi, shift, ii, m, &base[0], &arg[0]);
+        mesh_geometry(r.y, Hi, shift, ii, m, &base[1], &arg[1]);
+        mesh_geometry(r.z, Hi, shift, ii, m, &base[2], &arg[2]);
+        int rel0 = base[0] - o0, rel1 = base[1] - o1, rel2 = base[2] - o2;
+        rel0 += (rel0 < 0) ? m : 0;
+        rel1 += (rel1 < 0) ? m : 0;
+        rel2 += (rel2 < 0) ? m : 0;
+        real w[3][CAO];
+        bspline_weights<real, CAO, false>(arg[0], w[0], nullptr);
+        bspline_weights<real, CAO, false>(arg[1], w[1], nullptr);
+        bspline_weights<real, CAO, false>(arg[2], w[2], nullptr);
+        const int v = t * NMESH + ii;
+        real *dst = sw + (size_t)v * 3 * CAO;
 #pragma unroll
-        for (int b = 0; b < CAO; b++) {
-          const real qab = qa * wy[b];
-          real *row = tile + ((rel0 + a) * T + (rel1 + b)) * T + rel2;
+        for (int j = 0; j < CAO; j++) {
+          dst[j] = (real)r.w * w[0][j];  // q * W_x, the reference's first product
+          dst[CAO + j] = w[1][j];
+          dst[2 * CAO + j] = w[2][j];
+        }
+        soff[v] = rel0 * SP + rel1 * SR + rel2;
+      }
+    }
+    __syncthreads();
+    for (int v = warp; v < cnt * NMESH; v += nwarp) {
+      const real *wv = sw + (size_t)v * 3 * CAO;
+      real *tile = (NMESH == 2 && (v & 1)) ? tile1 : tile0;
+      real *org = tile + soff[v];
 #pragma unroll
-          for (int c = 0; c < CAO; c++) atomicAdd(row + c, qab * wz[c]);
+      for (int it = 0; it < IT; it++) {
+        if (labc[it] >= 0) {
+          const int abc = labc[it];
+          const real val = (wv[abc >> 16] * wv[CAO + ((abc >> 8) & 0xff)]) * wv[2 * CAO + (abc & 0xff)];
+          atomicAdd(org + loff[it], val);
         }
       }
     }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < T3; t += blockDim.x) {
+  for (int t = threadIdx.x; t < T * T * T; t += blockDim.x) {
     const int c = t % T, b = (t / T) % T, a = t / (T * T);
+    const int e = a * SP + b * SR + c;
     int gi = o0 + a, gj = o1 + b, gk = o2 + c;
     gi -= (gi >= m) ? m : 0;
     gj -= (gj >= m) ? m : 0;
@@ -74,11 +120,13 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
     if (gj >= m) gj %= m;
     if (gk >= m) gk %= m;
     const size_t g = ((size_t)gi * m + gj) * m + gk;
-    const real v0 = tile0[t];
-    if (v0 != (real)0) atomicAdd(&Q[g].x, v0);
+    const real v0 = tile0[e];
     if (NMESH == 2) {
-      const real v1 = tile1[t];
+      const real v1 = tile1[e];
+      if (v0 != (real)0) atomicAdd(&Q[g].x, v0);
       if (v1 != (real)0) atomicAdd(&Q[g].y, v1);
+    } else {
+      if (v0 != (real)0) atomicAdd(&Q[g].x, v0);
     }
   }
 }
@@ -127,15 +175,45 @@ __global__ void conv_ad_kernel(typename cplx<real>::type *__restrict__ Q, const 
 
 // ---------------------------------------------------------------- gather
 
+// Pack the three ik field meshes for the back-interpolation: per mesh point
+// one vector (F_x, F_y, F_z, 0) of the unshifted mesh (real parts) and, for
+// interlaced methods, one of the shifted mesh (imaginary parts), so the
+// gather reads one 16-byte (FP32) / 32-byte (FP64) vector per stencil point.
+template <typename real, int NMESH>
+__global__ void pack_ik_kernel(const typename cplx<real>::type *__restrict__ F, size_t M,
+                               typename cplx<real>::vec4 *__restrict__ P) {
+  typedef typename cplx<real>::vec4 V;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= M) return;
+  const typename cplx<real>::type f0 = F[t], f1 = F[M + t], f2 = F[2 * M + t];
+  V v;
+  v.x = f0.x;
+  v.y = f1.x;
+  v.z = f2.x;
+  v.w = (real)0;
+  P[t] = v;
+  if (NMESH == 2) {
+    v.x = f0.y;
+    v.y = f1.y;
+    v.z = f2.y;
+    P[M + t] = v;
+  }
+}
+
 // ik: f_d -= scale * q W F_d ; ad: f -= scale * phi * q/L * grad W.
 // scale = pref (one mesh) or pref/2 (interlaced, charge-assign.c:646-806).
+// One thread per brick-sorted particle; ik reads the packed fields (Fv =
+// P), ad the potential in the complex mesh (Fv = Q).
 template <typename real, int CAO, int NMESH, bool AD>
 __global__ void __launch_bounds__(ASSIGN_THREADS) gather_kernel(const double4 *__restrict__ sxyzq,
                                                                  const int *__restrict__ sidx, int np, int m,
                                                                  double Hi, double shift, double pref, double Leni,
-                                                                 const typename cplx<real>::type *__restrict__ F,
-                                                                 size_t M, double *__restrict__ fk, int n) {
+                                                                 const void *__restrict__ Fv, size_t M,
+                                                                 double *__restrict__ fk, int n) {
   typedef typename cplx<real>::type C;
+  typedef typename cplx<real>::vec4 V;
+  const C *__restrict__ F = reinterpret_cast<const C *>(Fv);
+  const V *__restrict__ P = reinterpret_cast<const V *>(Fv);
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
   const double4 r = sxyzq[p];
@@ -164,16 +242,16 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_kernel(const double4 *_
         const size_t rowb = ((size_t)gi * m + gj) * m;
         if (!AD) {
           const real qab = qp * wx[a] * wy[b];
+          const V *__restrict__ Pm = P + (ii ? M : 0) + rowb;
 #pragma unroll
           for (int c = 0; c < CAO; c++) {
             int gk = base[2] + c;
             gk -= (gk >= m) ? m : 0;
-            const size_t g = rowb + gk;
             const real Bw = scale * (qab * wz[c]);
-            const C f0 = F[g], f1 = F[M + g], f2 = F[2 * M + g];
-            acc0 -= (ii ? f0.y : f0.x) * Bw;
-            acc1 -= (ii ? f1.y : f1.x) * Bw;
-            acc2 -= (ii ? f2.y : f2.x) * Bw;
+            const V f = Pm[gk];
+            acc0 -= f.x * Bw;
+            acc1 -= f.y * Bw;
+            acc2 -= f.z * Bw;
           }
         } else {
 #pragma unroll
@@ -227,8 +305,68 @@ __global__ void self_force_kernel(const double *__restrict__ x, const double *__
 
 // ---------------------------------------------------------------- launch
 
+// Row and plane pitches of the scatter tile (in elements) such that the
+// CAO^3 stencil offsets split evenly over the shared-memory bank classes
+// (32 for 4-byte, 16 for 8-byte elements): searched once per shape.
+inline void scatter_pitch(int cao, int T, int word_bytes, int *SRo, int *SPo) {
+  static int cache[8][32][2][2];
+  static bool have[8][32][2];
+  const int wi = word_bytes == 8 ? 1 : 0;
+  if (cao < 8 && T < 32 && have[cao][T][wi]) {
+    *SRo = cache[cao][T][wi][0];
+    *SPo = cache[cao][T][wi][1];
+    return;
+  }
+  const int R = 32 / (word_bytes / 4), nsplit = 32 / R, S = cao * cao * cao;
+  int best_m = 1 << 30, best_mem = 1 << 30, bSR = T, bSP = T * T;
+  for (int SR = T; SR <= T + 8; SR++)
+    for (int SP = T * SR; SP <= T * SR + 32; SP++) {
+      int counts[32] = {0}, seen[32] = {0};
+      for (int sp = 0; sp < S; sp++) {
+        const int a = sp / (cao * cao), b = (sp / cao) % cao, cc = sp % cao;
+        const int cls = (a * SP + b * SR + cc) % R;
+        counts[cls + R * (seen[cls] % nsplit)]++;
+        seen[cls]++;
+      }
+      int mx = 0;
+      for (int l = 0; l < 32; l++) mx = counts[l] > mx ? counts[l] : mx;
+      if (mx < best_m || (mx == best_m && SP * T < best_mem)) {
+        best_m = mx;
+        best_mem = SP * T;
+        bSR = SR;
+        bSP = SP;
+      }
+    }
+  if (cao < 8 && T < 32) {
+    cache[cao][T][wi][0] = bSR;
+    cache[cao][T][wi][1] = bSP;
+    have[cao][T][wi] = true;
+  }
+  *SRo = bSR;
+  *SPo = bSP;
+}
+
+// Lane table of the scatter: entry it*32 + lane = (tile offset a*SP + b*SR
+// + c, (a << 16) | (b << 8) | c) of the it-th stencil point of that lane,
+// or (0, -1).  Lane l takes the points whose offset is congruent to l modulo
+// the number of bank classes R (32 for 4-byte, 16 for 8-byte elements;
+// with 8-byte elements lanes l and l + 16 alternate over one class).
+inline void scatter_lane_table(int cao, int SR, int SP, int word_bytes, int2 *tab) {
+  const int R = 32 / (word_bytes / 4), nsplit = 32 / R, S = cao * cao * cao, IT = (S + 31) / 32;
+  int fill[32] = {0}, seen[32] = {0};
+  for (int e = 0; e < 32 * IT; e++) tab[e] = make_int2(0, -1);
+  for (int sp = 0; sp < S; sp++) {
+    const int a = sp / (cao * cao), b = (sp / cao) % cao, cc = sp % cao;
+    const int off = a * SP + b * SR + cc;
+    const int cls = off % R;
+    const int lane = cls + R * (seen[cls] % nsplit);
+    seen[cls]++;
+    if (fill[lane] < IT) tab[fill[lane]++ * 32 + lane] = make_int2(off, (a << 16) | (b << 8) | cc);
+  }
+}
+
 template <typename real, int CAO, int NMESH>
-int launch_scatter(Ctx *c, size_t smem) {
+int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
   typedef typename cplx<real>::type C;
   auto kern = scatter_kernel<real, CAO, NMESH>;
   // raise the dynamic shared-memory limit once per instantiation (outside
@@ -242,8 +380,17 @@ int launch_scatter(Ctx *c, size_t smem) {
   const double shift = (double)((c->cao - 1) / 2);
   const int nbr = c->nbrick1 * c->nbrick1 * c->nbrick1;
   mark(c, EV_K2);
+  if (!c->scatter_tab) {
+    // built once per context, on its first (eager, uncaptured) step
+    const int IT = (CAO * CAO * CAO + 31) / 32;
+    int2 host[32 * 16];
+    scatter_lane_table(CAO, SR, SP, (int)sizeof(real), host);
+    P3MG_CUDA_TRY(cudaMalloc(&c->scatter_tab, sizeof(int2) * 32 * IT));
+    P3MG_CUDA_TRY(cudaMemcpy(c->scatter_tab, host, sizeof(int2) * 32 * IT, cudaMemcpyHostToDevice));
+  }
   kern<<<nbr, ASSIGN_THREADS, smem, c->stream>>>(c->sorted_xyzq, c->brick_start, c->mesh, c->brick, c->nbrick1, Hi,
-                                                shift, reinterpret_cast<C *>(c->Q));
+                                                shift, SR, SP, reinterpret_cast<const int2 *>(c->scatter_tab),
+                                                reinterpret_cast<C *>(c->Q));
   c->launches++;
   mark(c, EV_K3);
   P3MG_CUDA_TRY(cudaGetLastError());
@@ -254,9 +401,11 @@ template <typename real, int CAO>
 int dispatch_scatter(Ctx *c) {
   const int nmesh = method_interlaced(c->method) ? 2 : 1;
   const int T = brick_tile(c->brick, CAO, nmesh);
-  const size_t smem = (size_t)nmesh * T * T * T * sizeof(real);
-  if (nmesh == 2) return launch_scatter<real, CAO, 2>(c, smem);
-  return launch_scatter<real, CAO, 1>(c, smem);
+  int SR, SP;
+  scatter_pitch(CAO, T, (int)sizeof(real), &SR, &SP);
+  const size_t tile = (size_t)nmesh * T * SP * sizeof(real);
+  if (nmesh == 2) return launch_scatter<real, CAO, 2>(c, tile + scatter_stage_bytes<real, CAO, 2>(), SR, SP);
+  return launch_scatter<real, CAO, 1>(c, tile + scatter_stage_bytes<real, CAO, 1>(), SR, SP);
 }
 
 template <typename real, int CAO>
@@ -268,7 +417,7 @@ int dispatch_gather(Ctx *c) {
   const double Leni = 1.0 / c->L;
   const int blocks = (c->n + ASSIGN_THREADS - 1) / ASSIGN_THREADS;
   const bool il = method_interlaced(c->method);
-  const C *F = reinterpret_cast<const C *>(method_ad(c->method) ? c->Q : c->F);
+  const void *F = method_ad(c->method) ? c->Q : c->P;
   mark(c, EV_K4);
   if (method_ad(c->method)) {
     // prefactor Mesh * Leni^3 (p3m-ad.c:202, p3m-ad-i.c:199, p3m-ad-real.c:110)
@@ -334,6 +483,15 @@ int run_kspace(Ctx *c) {
     c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
     P3MG_TRY(fft3d(c, c->F, 3, +1));
+    typedef typename cplx<real>::vec4 V;
+    if (method_interlaced(c->method))
+      pack_ik_kernel<real, 2><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->F), M,
+                                                                  reinterpret_cast<V *>(c->P));
+    else
+      pack_ik_kernel<real, 1><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->F), M,
+                                                                  reinterpret_cast<V *>(c->P));
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
   }
   mark(c, EV_S3);
   // back-interpolation

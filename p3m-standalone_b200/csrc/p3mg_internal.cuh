@@ -45,10 +45,12 @@ struct cplx;
 template <>
 struct cplx<double> {
   typedef double2 type;
+  typedef double4 vec4;
 };
 template <>
 struct cplx<float> {
   typedef float2 type;
+  typedef float4 vec4;
 };
 
 // ------------------------------------------------------------ FFT plan
@@ -72,6 +74,9 @@ struct Ctx {
   double *f = nullptr, *fk = nullptr, *fr = nullptr;              // outputs, 3n each (device)
   double *energy = nullptr;                                        // device: [0] pair energy, [1] compensation
 
+  // scatter lane table (int2 per lane and iteration, built on the first step)
+  void *scatter_tab = nullptr;
+
   // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
   int brick = 8;
   int nbrick1 = 0;  // bricks per dimension
@@ -92,6 +97,7 @@ struct Ctx {
   size_t M = 0;               // mesh^3
   void *Q = nullptr;          // complex mesh
   void *F = nullptr;          // 3 complex meshes (ik methods)
+  void *P = nullptr;          // ik: packed fields per mesh point (Fx, Fy, Fz, 0), unshifted then shifted mesh
   double *G = nullptr;        // FP64 influence function (full mesh)
   float *G32 = nullptr;       // FP32 copy for the mixed path
   double *self_b = nullptr;   // 81 self-force coefficients (device)

@@ -2,19 +2,25 @@
 // for every ordered pair i != j with minimum-image distance r <= rcut
 //   f_i += q_i q_j (erfc(alpha r)/r + 2 alpha/sqrt(pi) exp(-alpha^2 r^2)) / r^2 * d
 //   E   += 1/2 q_i q_j erfc(alpha r)/r
-// The reference loops over all N^2 pairs; here particles are counting-sorted
+// The reference loops over all N^2 pairs.  Here particles are counting-sorted
 // into a cell list of side >= rcut (nc = floor(L/rcut) >= 3 cells per side),
-// which visits exactly the same pair set.  One CTA per cell: its particles
-// are the i's (one per thread), the 27 neighbour cells are staged through
-// shared memory and every thread reads them as broadcasts.
+// each cell split into 2x2x2 half-cells, which visits exactly the same pair
+// set.  One CTA per cell stages the 6x6x6 half-cells around it through
+// shared memory; a particle in half-cell u only tests the 5x5x5 half-cells
+// whose distance from u can be <= rcut (about 58 % of the 27-cell
+// candidates).  Within a CTA each warp takes one i at a time: its lanes test
+// 32 candidates per step, the accepted ones are compacted (ballot + prefix
+// count) into a circular per-warp queue, and 32 interactions are evaluated
+// at once whenever the queue holds 32 -- the erfc branch runs on full warps
+// although only ~15 % of the 27-cell candidates are within rcut.
 //
-// FP64: absolute positions and the reference's minimum-image rounding
-// (dx -= round(dx/L) L) with separately rounded products, so the r <= rcut
-// decisions are the reference's.  FP32 (mixed): positions relative to the
-// origin of their cell (exact in FP32 to ~1e-7 of a cell), neighbour image
-// offsets added as integer multiples of the cell side; energy summed with
-// compensated (Kahan) FP32 per thread and FP64 across threads.
-// With fewer than 3 cells per side the all-pairs kernel runs instead.
+// FP64: a conservative FP32 filter, then every queued pair is evaluated
+// exactly like the reference (dx -= round(dx/L) L with separately rounded
+// products, r <= rcut), so the pair set and the forces are the reference's.
+// FP32 (mixed): positions relative to the origin of their cell, neighbour
+// offsets added as multiples of the cell side; erfc from a fitted rational
+// form; energy summed with compensated (Kahan) FP32 per lane and FP64 across
+// lanes.  With fewer than 3 cells per side the all-pairs kernel runs.
 #include <math.h>
 
 #include "p3mg_internal.cuh"
@@ -23,19 +29,19 @@ namespace p3mg {
 
 namespace {
 
-constexpr int PAIR_THREADS = 64;
 constexpr int BRUTE_THREADS = 256;
 
+// half-cell key of a particle: cell-major, then the 2x2x2 sub-cell
 __global__ void bin_cells_kernel(const double *__restrict__ x, const double *__restrict__ y,
                                  const double *__restrict__ z, int n, double L, int nc, int *__restrict__ key,
                                  int *__restrict__ count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double s = (double)nc / L;
-  int c0 = wrap_full((int)floor(x[i] * s), nc);
-  int c1 = wrap_full((int)floor(y[i] * s), nc);
-  int c2 = wrap_full((int)floor(z[i] * s), nc);
-  const int k = (c0 * nc + c1) * nc + c2;
+  const double s = (double)(2 * nc) / L;
+  const int h0 = wrap_full((int)floor(x[i] * s), 2 * nc);
+  const int h1 = wrap_full((int)floor(y[i] * s), 2 * nc);
+  const int h2 = wrap_full((int)floor(z[i] * s), 2 * nc);
+  const int k = (((h0 >> 1) * nc + (h1 >> 1)) * nc + (h2 >> 1)) * 8 + ((h0 & 1) << 2) + ((h1 & 1) << 1) + (h2 & 1);
   key[i] = k;
   atomicAdd(&count[k], 1);
 }
@@ -55,7 +61,8 @@ __global__ void place_cells_kernel(const double *__restrict__ x, const double *_
   } else {
     // position relative to the cell origin, folded into the box
     const double cs = L / nc;
-    const int c2 = k % nc, c1 = (k / nc) % nc, c0 = k / (nc * nc);
+    const int cell = k >> 3;
+    const int c2 = cell % nc, c1 = (cell / nc) % nc, c0 = cell / (nc * nc);
     double xr = x[i] - L * floor(x[i] / L) - c0 * cs;
     double yr = y[i] - L * floor(y[i] / L) - c1 * cs;
     double zr = z[i] - L * floor(z[i] / L) - c2 * cs;
@@ -68,146 +75,310 @@ __device__ __forceinline__ double min_image(double d, double Li, double L) {
   return __dadd_rn(d, -__dmul_rn(round(__dmul_rn(d, Li)), L));
 }
 
-__global__ void __launch_bounds__(PAIR_THREADS) pairs_fp64_kernel(const double4 *__restrict__ pos,
-                                                                   const int *__restrict__ sidx,
-                                                                   const int *__restrict__ start, int nc, double L,
-                                                                   double rcut, double alpha, double *__restrict__ fr,
-                                                                   int n, double *__restrict__ energy) {
-  __shared__ double4 sj[PAIR_THREADS];
-  __shared__ double ered[PAIR_THREADS / 32];
-  const int cell = blockIdx.x;
-  const int c2 = cell % nc, c1 = (cell / nc) % nc, c0 = cell / (nc * nc);
-  const int i0 = start[cell], i1 = start[cell + 1];
-  const double Li = 1.0 / L;
-  const double wupi = 1.77245385090551602729816748334;
-  const double pref = 2.0 * alpha / wupi;
-  double e_loc = 0.0;
-  for (int ib = i0; ib < i1; ib += PAIR_THREADS) {
-    const int i = ib + threadIdx.x;
-    const bool act = i < i1;
-    double4 pi = act ? pos[i] : make_double4(0, 0, 0, 0);
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int nb = 0; nb < 27; nb++) {
-      const int d0 = nb / 9 - 1, d1 = (nb / 3) % 3 - 1, d2 = nb % 3 - 1;
-      const int nc0 = wrap_full(c0 + d0, nc), nc1 = wrap_full(c1 + d1, nc), nc2 = wrap_full(c2 + d2, nc);
-      const int ncell = (nc0 * nc + nc1) * nc + nc2;
-      const int j0 = start[ncell], j1 = start[ncell + 1];
-      for (int jb = j0; jb < j1; jb += PAIR_THREADS) {
-        __syncthreads();
-        if (jb + threadIdx.x < j1) sj[threadIdx.x] = pos[jb + threadIdx.x];
-        __syncthreads();
-        const int cnt = min(PAIR_THREADS, j1 - jb);
-        if (act) {
-          for (int t = 0; t < cnt; t++) {
-            if (jb + t == i) continue;
-            const double4 pj = sj[t];
-            const double dx = min_image(__dadd_rn(pi.x, -pj.x), Li, L);
-            const double dy = min_image(__dadd_rn(pi.y, -pj.y), Li, L);
-            const double dz = min_image(__dadd_rn(pi.z, -pj.z), Li, L);
-            const double r2s = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            const double r = sqrt(r2s);
-            if (r <= rcut) {
-              const double ar = alpha * r;
-              const double ec = erfc(ar);
-              const double r2 = r * r;
-              const double fak = pi.w * pj.w * (ec / r + pref * exp(-ar * ar)) / r2;
-              fx += fak * dx;
-              fy += fak * dy;
-              fz += fak * dz;
-              e_loc += 0.5 * pi.w * pj.w * ec / r;
-            }
-          }
-        }
-      }
-    }
-    if (act) {
-      const int o = sidx[i];
-      fr[o] += fx;
-      fr[(size_t)n + o] += fy;
-      fr[2 * (size_t)n + o] += fz;
-    }
-  }
-  // energy: warp then block reduction, one atomic per CTA
-  for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
-  if ((threadIdx.x & 31) == 0) ered[threadIdx.x >> 5] = e_loc;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < PAIR_THREADS / 32; w++) s += ered[w];
-    if (s != 0.0) atomicAdd(energy, s);
-  }
+// erfc(x) for x >= 0 given ex = exp(-x^2):  erfc(x) = t P(t) ex,
+// t = 1/(1 + 0.415 x), P a degree-7 polynomial -- the form of Abramowitz &
+// Stegun 7.1.26 with coefficients from a least-squares fit of the relative
+// error of erfc(x) e^{x^2} / t on [0, 6] (max relative error 8e-8 in exact
+// arithmetic, 2e-6 evaluated in FP32 with a fast exp).
+__device__ __forceinline__ float erfc_fit(float x, float ex) {
+  const float t = __fdividef(1.0f, fmaf(0.415f, x, 1.0f));
+  float P = 0.0763478258f;
+  P = fmaf(P, t, -0.360062487f);
+  P = fmaf(P, t, 0.535669094f);
+  P = fmaf(P, t, -0.220555614f);
+  P = fmaf(P, t, 0.318725078f);
+  P = fmaf(P, t, 0.176562497f);
+  P = fmaf(P, t, 0.23950376f);
+  P = fmaf(P, t, 0.233809829f);
+  return t * P * ex;
 }
 
-__global__ void __launch_bounds__(PAIR_THREADS) pairs_fp32_kernel(const float4 *__restrict__ pos,
-                                                                   const int *__restrict__ sidx,
-                                                                   const int *__restrict__ start, int nc, float cs,
-                                                                   float rcut, float alpha, double *__restrict__ fr,
-                                                                   int n, double *__restrict__ energy) {
-  __shared__ float4 sj[PAIR_THREADS];
-  __shared__ double ered[PAIR_THREADS / 32];
+// CTA shape and shared-memory budget of the cell kernel.
+constexpr int PAIR_CTA = 128;
+constexpr int PAIR_WARPS = PAIR_CTA / 32;
+constexpr int PAIR_JCH = 1536;   // staged candidates (the whole neighbourhood when it fits)
+constexpr int PAIR_MAXI = 128;   // i particles per batch
+constexpr int PAIR_QCAP = 64;    // circular queue per warp (power of two)
+constexpr int PAIR_NSEG = 216;   // 6x6x6 half-cells around the cell
+
+__host__ __device__ constexpr size_t pair_smem_bytes(bool dbl) {
+  return (size_t)PAIR_JCH * sizeof(float4) + (dbl ? (size_t)PAIR_JCH * sizeof(int) : 0) +
+         (size_t)PAIR_MAXI * sizeof(float4) + (size_t)PAIR_MAXI * 3 * (dbl ? sizeof(double) : sizeof(float)) +
+         (size_t)PAIR_WARPS * PAIR_QCAP * sizeof(unsigned short);
+}
+
+template <bool DBL>
+struct PairAcc {
+  typedef float type;
+};
+template <>
+struct PairAcc<true> {
+  typedef double type;
+};
+
+template <bool DBL>
+__global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__restrict__ posv,
+                                                               const int *__restrict__ sidx,
+                                                               const int *__restrict__ start, int nc, double L,
+                                                               double rcut, double alpha, int cull,
+                                                               double *__restrict__ fr, int n,
+                                                               double *__restrict__ energy) {
+  typedef typename PairAcc<DBL>::type acc_t;
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  float4 *cf = reinterpret_cast<float4 *>(pair_smem);
+  int *csrc = reinterpret_cast<int *>(cf + PAIR_JCH);  // FP64: sorted slot of each staged candidate
+  float4 *spi = reinterpret_cast<float4 *>(DBL ? reinterpret_cast<unsigned char *>(csrc + PAIR_JCH)
+                                               : reinterpret_cast<unsigned char *>(cf + PAIR_JCH));
+  acc_t *sfi = reinterpret_cast<acc_t *>(spi + PAIR_MAXI);
+  unsigned short *queue = reinterpret_cast<unsigned short *>(sfi + 3 * PAIR_MAXI);
+  __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
+  __shared__ double cell_off[27][3];
+  __shared__ unsigned short runs[8][36][2];
+  __shared__ double ered[PAIR_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned short *q = queue + warp * PAIR_QCAP;
   const int cell = blockIdx.x;
   const int c2 = cell % nc, c1 = (cell / nc) % nc, c0 = cell / (nc * nc);
-  const int i0 = start[cell], i1 = start[cell + 1];
-  const float pref = 2.0f * alpha / 1.7724538509055160273f;
-  const float rc2 = rcut * rcut;
-  float e_sum = 0.0f, e_comp = 0.0f;  // Kahan
-  for (int ib = i0; ib < i1; ib += PAIR_THREADS) {
-    const int i = ib + threadIdx.x;
-    const bool act = i < i1;
-    float4 pi = act ? pos[i] : make_float4(0, 0, 0, 0);
-    float fx = 0.f, fy = 0.f, fz = 0.f;
-    for (int nb = 0; nb < 27; nb++) {
-      const int d0 = nb / 9 - 1, d1 = (nb / 3) % 3 - 1, d2 = nb % 3 - 1;
-      const int nc0 = wrap_full(c0 + d0, nc), nc1 = wrap_full(c1 + d1, nc), nc2 = wrap_full(c2 + d2, nc);
-      const int ncell = (nc0 * nc + nc1) * nc + nc2;
-      const int j0 = start[ncell], j1 = start[ncell + 1];
-      // i relative to the neighbour cell's origin: pi - d*cs
-      const float ox = pi.x - d0 * cs, oy = pi.y - d1 * cs, oz = pi.z - d2 * cs;
-      for (int jb = j0; jb < j1; jb += PAIR_THREADS) {
-        __syncthreads();
-        if (jb + threadIdx.x < j1) sj[threadIdx.x] = pos[jb + threadIdx.x];
-        __syncthreads();
-        const int cnt = min(PAIR_THREADS, j1 - jb);
-        if (act) {
-          for (int t = 0; t < cnt; t++) {
-            const float4 pj = sj[t];
-            const float dx = ox - pj.x, dy = oy - pj.y, dz = oz - pj.z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 <= rc2 && (jb + t) != i) {
-              const float rinv = rsqrtf(r2);
-              const float r = r2 * rinv;
-              const float ar = alpha * r;
-              const float ec = erfcf(ar);
-              const float qq = pi.w * pj.w;
-              const float fak = qq * (ec * rinv + pref * __expf(-ar * ar)) * (rinv * rinv);
-              fx += fak * dx;
-              fy += fak * dy;
-              fz += fak * dz;
+  const double cs = L / nc;
+  if (tid < 27) {
+    const int d0 = tid / 9 - 1, d1 = (tid / 3) % 3 - 1, d2 = tid % 3 - 1;
+    const int u0 = c0 + d0, u1 = c1 + d1, u2 = c2 + d2;
+    const int w0 = wrap_full(u0, nc), w1 = wrap_full(u1, nc), w2 = wrap_full(u2, nc);
+    if (DBL) {
+      cell_off[tid][0] = (double)((u0 - w0) / nc) * L;  // periodic image: 0 or +-L
+      cell_off[tid][1] = (double)((u1 - w1) / nc) * L;
+      cell_off[tid][2] = (double)((u2 - w2) / nc) * L;
+    } else {
+      cell_off[tid][0] = d0 * cs;  // neighbour cell origin relative to this one
+      cell_off[tid][1] = d1 * cs;
+      cell_off[tid][2] = d2 * cs;
+    }
+  }
+  // half-cell segments in grid order: J = 2 d + v in -2..3 per axis, J2 fastest
+  for (int sg = tid; sg < PAIR_NSEG; sg += PAIR_CTA) {
+    const int J0 = sg / 36 - 2, J1 = (sg / 6) % 6 - 2, J2 = sg % 6 - 2;
+    const int d0 = (J0 + 2) / 2 - 1, d1 = (J1 + 2) / 2 - 1, d2 = (J2 + 2) / 2 - 1;
+    const int v0 = (J0 + 2) & 1, v1 = (J1 + 2) & 1, v2 = (J2 + 2) & 1;
+    const int w0 = wrap_full(c0 + d0, nc), w1 = wrap_full(c1 + d1, nc), w2 = wrap_full(c2 + d2, nc);
+    const int key = ((w0 * nc + w1) * nc + w2) * 8 + (v0 << 2) + (v1 << 1) + v2;
+    seg_src[sg] = start[key];
+    seg_pre[sg + 1] = start[key + 1] - start[key];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    seg_pre[0] = 0;
+    for (int sg = 0; sg < PAIR_NSEG; sg++) seg_pre[sg + 1] += seg_pre[sg];
+  }
+  __syncthreads();
+  // candidate runs of each sub-cell u: for every (J0, J1) in range one
+  // contiguous J2 range.  With cull, half-cells two steps away along an axis
+  // (at least 2h > rcut apart) are skipped: |J - U| <= 2.
+  for (int e = tid; e < 8 * 36; e += PAIR_CTA) {
+    const int u = e / 36, r = e % 36;
+    const int U0 = (u >> 2) & 1, U1 = (u >> 1) & 1, U2 = u & 1;
+    int lo0 = -2, hi0 = 3, lo1 = -2, hi1 = 3, lo2 = -2, hi2 = 3;
+    if (cull) {
+      lo0 = max(-2, U0 - 2); hi0 = min(3, U0 + 2);
+      lo1 = max(-2, U1 - 2); hi1 = min(3, U1 + 2);
+      lo2 = max(-2, U2 - 2); hi2 = min(3, U2 + 2);
+    }
+    const int n0 = hi0 - lo0 + 1, n1 = hi1 - lo1 + 1;
+    unsigned short a = 0, b = 0;
+    if (r < n0 * n1) {
+      const int J0 = lo0 + r / n1, J1 = lo1 + r % n1;
+      const int base = (J0 + 2) * 36 + (J1 + 2) * 6;
+      a = (unsigned short)seg_pre[base + (lo2 + 2)];
+      b = (unsigned short)seg_pre[base + (hi2 + 2) + 1];
+    }
+    runs[u][r][0] = a;
+    runs[u][r][1] = b;
+  }
+  const int total = seg_pre[PAIR_NSEG];
+  const bool fits = total <= PAIR_JCH;
+  const int i0 = start[cell * 8], i1 = start[cell * 8 + 8];
+  // this cell's 8 half-cells: sorted-order starts and staged segment starts
+  __shared__ int own_start[9], own_seg[8];
+  if (tid < 9) own_start[tid] = start[cell * 8 + tid];
+  if (tid < 8) own_seg[tid] = seg_pre[(2 + ((tid >> 2) & 1)) * 36 + (2 + ((tid >> 1) & 1)) * 6 + 2 + (tid & 1)];
+  __syncthreads();
+  const double ox = c0 * cs, oy = c1 * cs, oz = c2 * cs;
+  const double Li = 1.0 / L;
+  const double wupi = 1.77245385090551602729816748334;
+  const float rc2f = DBL ? (float)(rcut * rcut * (1.0 + 1e-4)) : (float)rcut * (float)rcut;
+  const float alphaf = (float)alpha, preff = (float)(2.0 * alpha / wupi);
+  const double prefd = 2.0 * alpha / wupi;
+  const float4 *pos32 = reinterpret_cast<const float4 *>(posv);
+  const double4 *pos64 = reinterpret_cast<const double4 *>(posv);
+  double e_d = 0.0;
+  float e_sum = 0.0f, e_comp = 0.0f;  // compensated FP32 energy sum (Kahan)
+
+  for (int ib = i0; ib < i1; ib += PAIR_MAXI) {
+    const int ni = min(PAIR_MAXI, i1 - ib);
+    __syncthreads();
+    for (int t = tid; t < ni; t += PAIR_CTA) {
+      if (DBL) {
+        const double4 p = pos64[ib + t];
+        spi[t] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz), (float)p.w);
+      } else {
+        spi[t] = pos32[ib + t];
+      }
+      sfi[3 * t] = sfi[3 * t + 1] = sfi[3 * t + 2] = (acc_t)0;
+    }
+    // all candidates in one chunk when they fit (sub-cell runs), else chunks
+    // of the flat candidate order without culling
+    for (int k0 = 0; k0 < total; k0 += PAIR_JCH) {
+      const int kn = min(PAIR_JCH, total - k0);
+      __syncthreads();
+#pragma unroll 4
+      for (int kk = tid; kk < kn; kk += PAIR_CTA) {
+        const int k = k0 + kk;
+        int sg = 0;
+#pragma unroll
+        for (int step = 128; step > 0; step >>= 1)
+          if (sg + step < PAIR_NSEG && seg_pre[sg + step] <= k) sg += step;
+        const int src = seg_src[sg] + (k - seg_pre[sg]);
+        const int J0 = sg / 36, J1 = (sg / 6) % 6, J2 = sg % 6;
+        const int cidx = ((J0 / 2) * 3 + J1 / 2) * 3 + J2 / 2;
+        if (DBL) {
+          const double4 p = pos64[src];
+          csrc[kk] = src;
+          cf[kk] = make_float4((float)(p.x + cell_off[cidx][0] - ox), (float)(p.y + cell_off[cidx][1] - oy),
+                               (float)(p.z + cell_off[cidx][2] - oz), (float)p.w);
+        } else {
+          const float4 p = pos32[src];
+          cf[kk] = make_float4(p.x + (float)cell_off[cidx][0], p.y + (float)cell_off[cidx][1],
+                               p.z + (float)cell_off[cidx][2], p.w);
+        }
+      }
+      __syncthreads();
+      for (int il = warp; il < ni; il += PAIR_WARPS) {
+        const float4 pif = spi[il];
+        double4 pid = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (DBL) pid = pos64[ib + il];
+        // half-cell u of i and its own staged slot (excluded from its pairs)
+        const int isorted = ib + il;
+        int u = 0;
+#pragma unroll
+        for (int v = 1; v < 8; v++)
+          if (isorted >= own_start[v]) u = v;
+        const int kself = own_seg[u] + (isorted - own_start[u]) - k0;
+        acc_t fx = 0, fy = 0, fz = 0;
+        unsigned head = 0, tail = 0;
+        // evaluate `take` queued interactions (one per lane) and pop them
+        auto process = [&](int take) {
+          __syncwarp();
+          if (lane < take) {
+            const int sl = q[(head + lane) & (PAIR_QCAP - 1)];
+            if (DBL) {
+              const double4 pj = pos64[csrc[sl]];
+              const double ddx = min_image(__dadd_rn(pid.x, -pj.x), Li, L);
+              const double ddy = min_image(__dadd_rn(pid.y, -pj.y), Li, L);
+              const double ddz = min_image(__dadd_rn(pid.z, -pj.z), Li, L);
+              const double rr = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)));
+              if (rr <= rcut) {
+                const double ar = alpha * rr;
+                const double ec = erfc(ar);
+                const double fak = pid.w * pj.w * (ec / rr + prefd * exp(-ar * ar)) / (rr * rr);
+                fx += fak * ddx;
+                fy += fak * ddy;
+                fz += fak * ddz;
+                e_d += 0.5 * pid.w * pj.w * ec / rr;
+              }
+            } else {
+              const float4 pj = cf[sl];
+              const float ex = pif.x - pj.x, ey = pif.y - pj.y, ez = pif.z - pj.z;
+              const float rr2 = ex * ex + ey * ey + ez * ez;
+              const float rinv = rsqrtf(rr2);
+              const float ar = alphaf * (rr2 * rinv);
+              const float gs = __expf(-ar * ar);
+              const float ec = erfc_fit(ar, gs);
+              const float qq = pif.w * pj.w;
+              const float fak = qq * (ec * rinv + preff * gs) * (rinv * rinv);
+              fx += fak * ex;
+              fy += fak * ey;
+              fz += fak * ez;
               const float term = 0.5f * qq * ec * rinv - e_comp;
               const float tsum = e_sum + term;
               e_comp = (tsum - e_sum) - term;
               e_sum = tsum;
             }
           }
+          head += take;
+          __syncwarp();
+        };
+        const int nrun = fits ? (cull ? 25 : 36) : 1;
+        for (int r = 0; r < nrun; r++) {
+          const int a = fits ? runs[u][r][0] : 0;
+          const int b = fits ? runs[u][r][1] : kn;
+          for (int jb = a; jb < b; jb += 32) {
+            const int kk = jb + lane;
+            // branch-free test: the load index is clamped into the staged range
+            const float4 pj = cf[min(kk, PAIR_JCH - 1)];
+            const float dx = pif.x - pj.x, dy = pif.y - pj.y, dz = pif.z - pj.z;
+            const bool ok = (kk < b) & (dx * dx + dy * dy + dz * dz <= rc2f) & (kk != kself);
+            const unsigned mask = __ballot_sync(0xffffffffu, ok);
+            if (ok) q[(tail + __popc(mask & ((1u << lane) - 1u))) & (PAIR_QCAP - 1)] = (unsigned short)kk;
+            tail += __popc(mask);
+            // at most 63 queued: one full round drains it below 32
+            if (tail - head >= 32) process(32);
+          }
+        }
+        if (tail != head) process((int)(tail - head));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          fx += __shfl_xor_sync(0xffffffffu, fx, o);
+          fy += __shfl_xor_sync(0xffffffffu, fy, o);
+          fz += __shfl_xor_sync(0xffffffffu, fz, o);
+        }
+        if (lane == 0) {
+          sfi[3 * il] += fx;
+          sfi[3 * il + 1] += fy;
+          sfi[3 * il + 2] += fz;
         }
       }
     }
-    if (act) {
-      const int o = sidx[i];
-      fr[o] += (double)fx;
-      fr[(size_t)n + o] += (double)fy;
-      fr[2 * (size_t)n + o] += (double)fz;
+    __syncthreads();
+    for (int t = tid; t < ni; t += PAIR_CTA) {
+      const int o = sidx[ib + t];
+      fr[o] += (double)sfi[3 * t];
+      fr[(size_t)n + o] += (double)sfi[3 * t + 1];
+      fr[2 * (size_t)n + o] += (double)sfi[3 * t + 2];
     }
   }
-  double e_loc = (double)e_sum - (double)e_comp;
+  double e_loc = DBL ? e_d : ((double)e_sum - (double)e_comp);
   for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
-  if ((threadIdx.x & 31) == 0) ered[threadIdx.x >> 5] = e_loc;
+  if (lane == 0) ered[warp] = e_loc;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     double s = 0.0;
-    for (int w = 0; w < PAIR_THREADS / 32; w++) s += ered[w];
+    for (int w = 0; w < PAIR_WARPS; w++) s += ered[w];
     if (s != 0.0) atomicAdd(energy, s);
   }
+}
+
+// Launch the cell kernel (FP64 or FP32 positions, already half-cell sorted).
+int launch_pairs_cells(bool dbl, const void *pos, const int *sidx, const int *start, int nc, double L, double rcut,
+                       double alpha, double *fr, int n, double *energy, cudaStream_t s) {
+  static bool attr_set[2] = {false, false};
+  const size_t smem = pair_smem_bytes(dbl);
+  if (!attr_set[dbl]) {
+    if (dbl)
+      P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+      P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dbl] = true;
+  }
+  // half-cells two steps apart along one axis are >= 2h > rcut apart when
+  // the half-cell side h exceeds rcut/2 (kept when they are exactly equal)
+  const double h = 0.5 * L / nc;
+  const int cull = (4.0 * h * h > rcut * rcut * (1.0 + 1e-9)) ? 1 : 0;
+  const int ncell = nc * nc * nc;
+  if (dbl)
+    pairs_cell_kernel<true><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, cull, fr, n, energy);
+  else
+    pairs_cell_kernel<false><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, cull, fr, n, energy);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
 }
 
 // All-pairs fallback (fewer than 3 cells per side): the reference's loop
@@ -274,22 +445,22 @@ static int cells_per_side(double L, double rcut) {
 }
 
 // Allocate the cell-list arrays for this rcut (host-side; called before a
-// step is captured into a CUDA graph).
+// step is captured into a CUDA graph).  Keys: 8 half-cells per cell.
 int pairs_reserve(Ctx *c, double rcut) {
   if (c->n == 0 || rcut <= 0.0) return P3MG_OK;
   const int nc = cells_per_side(c->L, rcut);
   if (nc < 3) return P3MG_OK;
-  const int ncell = nc * nc * nc;
-  if (ncell > c->ncell_cap) {
+  const int nkey = 8 * nc * nc * nc;
+  if (nkey > c->ncell_cap) {
     if (c->cell_count) cudaFree(c->cell_count);
     if (c->cell_start) cudaFree(c->cell_start);
     if (c->cell_fill) cudaFree(c->cell_fill);
     c->cell_count = c->cell_start = c->cell_fill = nullptr;
     c->ncell_cap = 0;
-    P3MG_CUDA_TRY(cudaMalloc(&c->cell_count, sizeof(int) * ncell));
-    P3MG_CUDA_TRY(cudaMalloc(&c->cell_start, sizeof(int) * (ncell + 1)));
-    P3MG_CUDA_TRY(cudaMalloc(&c->cell_fill, sizeof(int) * ncell));
-    c->ncell_cap = ncell;
+    P3MG_CUDA_TRY(cudaMalloc(&c->cell_count, sizeof(int) * nkey));
+    P3MG_CUDA_TRY(cudaMalloc(&c->cell_start, sizeof(int) * (nkey + 1)));
+    P3MG_CUDA_TRY(cudaMalloc(&c->cell_fill, sizeof(int) * nkey));
+    c->ncell_cap = nkey;
   }
   return P3MG_OK;
 }
@@ -309,37 +480,30 @@ int pairs_run(Ctx *c, double rcut, double alpha) {
     P3MG_CUDA_TRY(cudaGetLastError());
     return P3MG_OK;
   }
-  const int ncell = nc * nc * nc;
+  const int nkey = 8 * nc * nc * nc;
   P3MG_TRY(pairs_reserve(c, rcut));
   c->ncell1 = nc;
-  P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_count, 0, sizeof(int) * ncell, c->stream));
-  P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_fill, 0, sizeof(int) * ncell, c->stream));
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_count, 0, sizeof(int) * nkey, c->stream));
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_fill, 0, sizeof(int) * nkey, c->stream));
   bin_cells_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, n, c->L, nc, c->cell_key, c->cell_count);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
-  P3MG_TRY(exclusive_scan(c, c->cell_count, c->cell_start, ncell));
-  if (c->precision == P3MG_FP64) {
+  P3MG_TRY(exclusive_scan(c, c->cell_count, c->cell_start, nkey));
+  const bool dbl = (c->precision == P3MG_FP64);
+  if (dbl)
     place_cells_kernel<double4><<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, nc, c->cell_key,
                                                                    c->cell_start, c->cell_fill, c->cell_idx,
                                                                    reinterpret_cast<double4 *>(c->cell_pos));
-    P3MG_CUDA_TRY(cudaGetLastError());
-    mark(c, EV_K0);
-    pairs_fp64_kernel<<<ncell, PAIR_THREADS, 0, c->stream>>>(reinterpret_cast<const double4 *>(c->cell_pos),
-                                                             c->cell_idx, c->cell_start, nc, c->L, rcut, alpha, c->fr,
-                                                             n, c->energy);
-  } else {
+  else
     place_cells_kernel<float4><<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, nc, c->cell_key,
                                                                   c->cell_start, c->cell_fill, c->cell_idx,
                                                                   reinterpret_cast<float4 *>(c->cell_pos));
-    P3MG_CUDA_TRY(cudaGetLastError());
-    mark(c, EV_K0);
-    pairs_fp32_kernel<<<ncell, PAIR_THREADS, 0, c->stream>>>(reinterpret_cast<const float4 *>(c->cell_pos),
-                                                             c->cell_idx, c->cell_start, nc, (float)(c->L / nc),
-                                                             (float)rcut, (float)alpha, c->fr, n, c->energy);
-  }
+  P3MG_CUDA_TRY(cudaGetLastError());
+  mark(c, EV_K0);
+  P3MG_TRY(launch_pairs_cells(dbl, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut, alpha, c->fr, n,
+                              c->energy, c->stream));
   c->launches += 2;
   mark(c, EV_K1);
-  P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
 
@@ -356,7 +520,7 @@ int pairs_run(Ctx *c, double rcut, double alpha) {
 // module (every GPU that loads the library holds it until the process
 // exits).  Its capacity bounds the particle count; the cell grid is capped
 // so that it fits as well (cells stay at least rcut wide, so the pairs found
-// are the same).  All calls on a device share the one array and it keeps
+// are the same).  The cell list has 8 half-cell keys per cell.  All calls on a device share the one array and it keeps
 // the previous call's contents: the per-call counters are cleared on the
 // caller's stream before use, and calls that overlap on the GPU (different
 // streams, or host threads racing) corrupt each other's cell lists.
@@ -426,8 +590,8 @@ extern "C" int p3mg_real_forces_noalloc(int n, const double *x, const double *y,
     P3MG_CUDA_TRY(cudaGetLastError());
     return P3MG_OK;
   }
-  while (nc > 3 && nc * nc * nc > P3MG_NOALLOC_MAX_CELLS) nc--;
-  const int ncell = nc * nc * nc;
+  while (nc > 3 && 8 * nc * nc * nc > P3MG_NOALLOC_MAX_CELLS) nc--;
+  const int ncell = 8 * nc * nc * nc;  // half-cell keys
   int *count = (int *)(base + NA_OFF_COUNT);
   int *start = (int *)(base + NA_OFF_START);
   int *fill = (int *)(base + NA_OFF_FILL);
@@ -444,14 +608,12 @@ extern "C" int p3mg_real_forces_noalloc(int n, const double *x, const double *y,
     place_cells_kernel<double4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
                                                            reinterpret_cast<double4 *>(pos));
     P3MG_CUDA_TRY(cudaGetLastError());
-    pairs_fp64_kernel<<<ncell, PAIR_THREADS, 0, s>>>(reinterpret_cast<const double4 *>(pos), idx, start, nc, L, rcut,
-                                                     alpha, fr, n, energy);
+    P3MG_TRY(launch_pairs_cells(true, pos, idx, start, nc, L, rcut, alpha, fr, n, energy, s));
   } else {
     place_cells_kernel<float4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
                                                           reinterpret_cast<float4 *>(pos));
     P3MG_CUDA_TRY(cudaGetLastError());
-    pairs_fp32_kernel<<<ncell, PAIR_THREADS, 0, s>>>(reinterpret_cast<const float4 *>(pos), idx, start, nc,
-                                                     (float)(L / nc), (float)rcut, (float)alpha, fr, n, energy);
+    P3MG_TRY(launch_pairs_cells(false, pos, idx, start, nc, L, rcut, alpha, fr, n, energy, s));
   }
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
