@@ -239,11 +239,30 @@ def run_ours(args, rank, world, local_rank):
             e2e_ms += e0.elapsed_time(e1)
         barrier()
         results[prec]["e2e_ms"] = max_over_ranks(e2e_ms) / args.steps
-        if prec == p3mg.FP32_MIXED:
-            results["fp32_forces"] = np.stack([t.numpy().copy() for t in hf])
+        results[prec]["forces"] = np.stack([t.numpy().copy() for t in hf])
         ctx.close()
 
     r32, r64 = results[p3mg.FP32_MIXED], results[p3mg.FP64]
+    # accuracy (untimed): DeltaF of both paths against the FP64 Ewald reference
+    # forces on a seeded subset of 2000 targets (Calculate_errors, error.c:21-34)
+    accuracy = None
+    if rank == 0 and not args.no_accuracy:
+        tg = np.sort(np.random.default_rng(2024).choice(n, min(2000, n), replace=False))
+        with p3mg.Context(W["method"], W["mesh"], W["cao"], W["mc"], p3mg.FP64) as ectx:
+            ectx.set_system(x, y, z, q, L)
+            t0 = time.perf_counter()
+            ew = ectx.ewald_forces(tg)
+            t_ew = time.perf_counter() - t0
+        fe = ew["f"]
+        def _rms(f):
+            d = f[:, tg] - fe
+            return float(np.sqrt(np.sum(d * d) / len(tg)))
+        fr = float(np.sqrt(np.sum(fe * fe) / len(tg)))
+        accuracy = {"targets": int(len(tg)), "ewald_alpha": ew["alpha"], "ewald_kmax": ew["kmax"],
+                    "ewald_seconds": round(t_ew, 3), "rms_force": fr,
+                    "rms_error_fp32": _rms(r32["forces"]), "rms_error_fp64": _rms(r64["forces"]),
+                    "rms_fp32_vs_fp64": float(np.sqrt(np.sum((r32["forces"][:, tg] - r64["forces"][:, tg]) ** 2)
+                                                     / len(tg)))}
     value = world * 1000.0 / r32["ms"]
     e2e = world * 1000.0 / r32["e2e_ms"]
 
@@ -297,6 +316,7 @@ def run_ours(args, rank, world, local_rank):
             "step_roofline": {"algorithmic_bytes": int(algorithmic_bytes(W["method"], n, W["mesh"], 4)),
                               "achieved_gbs": round(algorithmic_bytes(W["method"], n, W["mesh"], 4)
                                                     / (r32["ms"] * 1e-3) / 1e9, 2)},
+            "accuracy": accuracy,
             "gpu_launches": int(r32["launches"]),
             "clocks": clocks,
         }
@@ -408,6 +428,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=0, help="particles (default: the workload's 1,000,000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the Ewald error report")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)

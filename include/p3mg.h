@@ -124,6 +124,18 @@ int p3mg_get_forces_device(p3mg_ctx *ctx, const double **f, const double **fk, c
 int p3mg_enable_timing(p3mg_ctx *ctx, int on);
 int p3mg_stage_times(p3mg_ctx *ctx, double t[4]);
 
+/* FP64 Ewald reference forces for the context's particles, evaluated on nt
+ * target particles (targets: host array of particle indices, or NULL with
+ * nt == n for all), written (not accumulated) to the host arrays f_x/f_y/f_z
+ * (nt each): real space with rcut = 0.49 L plus the Ewald k-space sum, alpha
+ * and kmax chosen like the reference (alpha by bisection with the context's
+ * mesh as kmax, then kmax = 2, 4, ... until the estimate <= 1e-8).
+ * alpha_out / kmax_out may be NULL.  Replaces Calculate_reference_forces
+ * (common.c:329-363) with Ewald_k_space (ewald.c:122-173); the reference's
+ * Ewald energy is not reproduced (ewald.c:169 accumulates only the last k). */
+int p3mg_ewald_forces(p3mg_ctx *ctx, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
+                      double *alpha_out, int *kmax_out);
+
 /* Copy the FP64 influence function (mesh^3 doubles, full mesh, index
  * (i*mesh + j)*mesh + k as r_ind, p3m-common.h:25) and the 81 ad self-force
  * coefficients (zeros for other methods) to host memory; either may be NULL. */

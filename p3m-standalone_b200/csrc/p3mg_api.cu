@@ -522,3 +522,63 @@ int p3mg_kernel_times(p3mg_ctx *h, double t[3]) {
 }
 
 }  // extern "C"
+
+extern "C" int p3mg_ewald_forces(p3mg_ctx *h, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
+                                 double *alpha_out, int *kmax_out) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (nt < 0 || (nt > 0 && (!f_x || !f_y || !f_z))) return P3MG_ERR_ARG;
+  if (!targets && nt != c->n) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->n;
+  if (targets)
+    for (int t = 0; t < nt; t++)
+      if (targets[t] < 0 || (size_t)targets[t] >= n) return P3MG_ERR_ARG;
+  // sum of q^2 (system_t.q2) from the device copy
+  double q2 = 0.0;
+  if (n > 0) {
+    double *hq = (double *)malloc(n * sizeof(double));
+    if (!hq) return P3MG_ERR_ALLOC;
+    cudaError_t e = cudaMemcpy(hq, c->q, n * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      free(hq);
+      record_cuda_error(e);
+      return P3MG_ERR_CUDA;
+    }
+    for (size_t i = 0; i < n; i++) q2 += hq[i] * hq[i];
+    free(hq);
+  }
+  double alpha = 0.0;
+  int kmax = 0;
+  P3MG_TRY(ewald_parameters(c->n, q2, c->L, c->mesh, &alpha, &kmax));
+  if (alpha_out) *alpha_out = alpha;
+  if (kmax_out) *kmax_out = kmax;
+  if (nt == 0) return P3MG_OK;
+  int *d_tgt = nullptr;
+  double *d_out = nullptr;
+  int st = P3MG_OK;
+  cudaError_t e = cudaMalloc(&d_out, 3 * (size_t)nt * sizeof(double));
+  if (e == cudaSuccess && targets) {
+    e = cudaMalloc(&d_tgt, (size_t)nt * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(d_tgt, targets, (size_t)nt * sizeof(int), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    record_cuda_error(e);
+    st = (e == cudaErrorMemoryAllocation) ? P3MG_ERR_ALLOC : P3MG_ERR_CUDA;
+  } else {
+    st = ewald_forces(c, nt, d_tgt, alpha, kmax, d_out);
+    if (st == P3MG_OK) {
+      double *dst[3] = {f_x, f_y, f_z};
+      for (int d = 0; d < 3 && e == cudaSuccess; d++)
+        e = cudaMemcpy(dst[d], d_out + (size_t)d * nt, (size_t)nt * sizeof(double), cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) {
+        record_cuda_error(e);
+        st = P3MG_ERR_CUDA;
+      }
+    }
+  }
+  if (d_tgt) cudaFree(d_tgt);
+  if (d_out) cudaFree(d_out);
+  return st;
+}

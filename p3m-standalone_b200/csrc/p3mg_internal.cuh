@@ -164,6 +164,10 @@ int influence_compute(Ctx *c, double alpha);
 int kspace_prepare(Ctx *c);
 int kspace_run(Ctx *c);  // scatter, FFTs, convolution, gather, self-force into c->fk / c->f
 
+// FP64 Ewald reference (p3mg_ewald.cu)
+int ewald_parameters(int n, double q2, double L, int mesh_param, double *alpha, int *kmax);
+int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, double *d_out);
+
 // real space (p3mg_pairs.cu)
 int pairs_reserve(Ctx *c, double rcut);
 int pairs_run(Ctx *c, double rcut, double alpha);

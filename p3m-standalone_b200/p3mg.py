@@ -88,6 +88,8 @@ def load():
     L.p3mg_enable_timing.argtypes = [vp, ctypes.c_int]
     L.p3mg_stage_times.argtypes = [vp, _dp]
     L.p3mg_get_influence.argtypes = [vp, _dp, _dp]
+    L.p3mg_ewald_forces.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp, _dp,
+                                    ctypes.POINTER(ctypes.c_int)]
     L.p3mg_kernel_times.argtypes = [vp, _dp]
     L.p3mg_set_graph.argtypes = [vp, ctypes.c_int]
     L.p3mg_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -214,6 +216,22 @@ class Context:
         t = np.zeros(4)
         _check(self._lib.p3mg_stage_times(self._h, _p(t)), "p3mg_stage_times")
         return dict(t_c=t[0], t_g=t[1], t_f=t[2], t_r=t[3])
+
+    def ewald_forces(self, targets=None):
+        """FP64 Ewald reference forces on the targets (indices; None = all):
+        dict f (3, nt), alpha, kmax (Calculate_reference_forces, common.c:329-363)."""
+        if targets is None:
+            nt, tp = self.n, None
+        else:
+            tg = np.ascontiguousarray(targets, dtype=np.int32)
+            self._tg = tg
+            nt, tp = len(tg), tg.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        f = np.zeros((3, nt))
+        a = ctypes.c_double(0.0)
+        k = ctypes.c_int(0)
+        _check(self._lib.p3mg_ewald_forces(self._h, nt, tp, _p(f[0]), _p(f[1]), _p(f[2]), ctypes.byref(a),
+                                           ctypes.byref(k)), "p3mg_ewald_forces")
+        return dict(f=f, alpha=a.value, kmax=k.value)
 
     def kernel_times(self):
         t = np.zeros(3)

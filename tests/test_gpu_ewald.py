@@ -1,0 +1,66 @@
+"""FP64 Ewald reference forces on the GPU (p3mg_ewald_forces) against the
+oracle's Ewald, the reference's own Ewald outputs (golden fixtures) and
+the reference fixture tests-wall.for."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import p3mg
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_ewald_matches_oracle_all_targets(gpu):
+    x, y, z, q = p3mg.generate_system(0, 300, 9.0, seed=31)
+    ref = O.ewald(x, y, z, q, 9.0, 16)
+    with p3mg.Context(1, 16, 5, 1) as ctx:
+        ctx.set_system(x, y, z, q, 9.0)
+        out = ctx.ewald_forces()
+    assert (out["alpha"], out["kmax"]) == (ref["alpha"], ref["kmax"])
+    assert O.rel_rms(out["f"], ref["f"]) <= 1e-10
+
+
+def test_ewald_target_subset(gpu):
+    x, y, z, q = p3mg.generate_system(4, 500, 11.0, seed=32)
+    tg = np.array([3, 77, 12, 499, 250])
+    ref = O.ewald(x, y, z, q, 11.0, 24, targets=tg)
+    with p3mg.Context(3, 24, 5, 1) as ctx:
+        ctx.set_system(x, y, z, q, 11.0)
+        out = ctx.ewald_forces(tg)
+    assert O.rel_rms(out["f"], ref["f"]) <= 1e-10
+
+
+def test_ewald_matches_reference_golden(gpu):
+    s = dict(np.load(os.path.join(GOLD, "sweep.npz")))
+    with p3mg.Context(7, 16, 7, 2) as ctx:
+        ctx.set_system(s["x"], s["y"], s["z"], s["q"], float(s["L"]))
+        out = ctx.ewald_forces()
+    assert out["kmax"] == int(s["ewald_kmax"]) and out["alpha"] == float(s["ewald_alpha"])
+    assert O.rel_rms(out["f"], s["ewald_f"]) <= 1e-10
+
+
+def test_ewald_matches_tests_wall_for(gpu):
+    w = dict(np.load(os.path.join(GOLD, "wall.npz")))
+    with p3mg.Context(0, 16, 7, 1) as ctx:
+        ctx.set_system(w["x"], w["y"], w["z"], w["q"], float(w["L"]))
+        out = ctx.ewald_forces()
+    assert O.rel_rms(out["f"], w["for_total"]) <= 1e-6
+
+
+def test_p3m_error_close_to_reference_estimate(gpu):
+    """DeltaF of the GPU P3M against the GPU Ewald is of the size of the
+    reference's analytic error estimate (main.c:428-434 prints both)."""
+    n, L = 3000, 14.4
+    x, y, z, q = p3mg.generate_system(0, n, L, seed=33)
+    with p3mg.Context(2, 24, 5, 1) as ctx:
+        ctx.set_system(x, y, z, q, L)
+        ctx.influence(1.0)
+        f = ctx.calculate_forces(3.5)["f"]
+        ew = ctx.ewald_forces()["f"]
+    err = p3mg.rms_error(f, ew)
+    est = np.hypot(O.kspace_error(2, 24, 5, 1, 1.0, n, float(np.sum(q * q)), L),
+                   O.realspace_error(n, float(np.sum(q * q)), L, 3.5, 1.0))
+    assert 0.3 * est <= err <= 3.0 * est, (err, est)
