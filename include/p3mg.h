@@ -124,6 +124,16 @@ int p3mg_get_forces_device(p3mg_ctx *ctx, const double **f, const double **fk, c
 int p3mg_enable_timing(p3mg_ctx *ctx, int on);
 int p3mg_stage_times(p3mg_ctx *ctx, double t[4]);
 
+/* The method's analytic RMS force error estimates for the context's system
+ * at (alpha, rcut), computed on the GPU: est[0] total = sqrt(est[1]^2 +
+ * est[2]^2), est[1] k-space, est[2] real space.  mc_est is the aliasing
+ * range P3M_BRILLOUIN_TUNING (CLI "mc_est", default 1).  Replaces
+ * method.Error / method.Error_k (p3m-ik.c:249-336, p3m-ik-i.c:249-320,
+ * p3m-ad.c:436-505, p3m-ad-i.c:205-294) and Realspace_error
+ * (realpart.c:343-346); for ik/ik-i at meshes the reference tabulates
+ * (find_error.c:84-107) it interpolates stored values of these sums instead. */
+int p3mg_error_estimate(p3mg_ctx *ctx, double alpha, double rcut, int mc_est, double est[3]);
+
 /* FP64 Ewald reference forces for the context's particles, evaluated on nt
  * target particles (targets: host array of particle indices, or NULL with
  * nt == n for all), written (not accumulated) to the host arrays f_x/f_y/f_z

@@ -523,6 +523,37 @@ int p3mg_kernel_times(p3mg_ctx *h, double t[3]) {
 
 }  // extern "C"
 
+// sum of q^2 (system_t.q2, io.c:150) from the context's device copy
+static int host_q2(Ctx *c, double *q2) {
+  *q2 = 0.0;
+  const size_t n = (size_t)c->n;
+  if (n == 0) return P3MG_OK;
+  double *hq = (double *)malloc(n * sizeof(double));
+  if (!hq) return P3MG_ERR_ALLOC;
+  cudaError_t e = cudaMemcpy(hq, c->q, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    free(hq);
+    record_cuda_error(e);
+    return P3MG_ERR_CUDA;
+  }
+  double s = 0.0;
+  for (size_t i = 0; i < n; i++) s += hq[i] * hq[i];
+  free(hq);
+  *q2 = s;
+  return P3MG_OK;
+}
+
+extern "C" int p3mg_error_estimate(p3mg_ctx *h, double alpha, double rcut, int mc_est, double est[3]) {
+  if (!h || !est) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!(alpha > 0.0) || !(rcut >= 0.0) || mc_est < 0) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  double q2 = 0.0;
+  P3MG_TRY(host_q2(c, &q2));
+  return error_estimates(c, alpha, rcut, mc_est, q2, est);
+}
+
 extern "C" int p3mg_ewald_forces(p3mg_ctx *h, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
                                  double *alpha_out, int *kmax_out) {
   if (!h) return P3MG_ERR_ARG;
@@ -535,20 +566,8 @@ extern "C" int p3mg_ewald_forces(p3mg_ctx *h, int nt, const int *targets, double
   if (targets)
     for (int t = 0; t < nt; t++)
       if (targets[t] < 0 || (size_t)targets[t] >= n) return P3MG_ERR_ARG;
-  // sum of q^2 (system_t.q2) from the device copy
   double q2 = 0.0;
-  if (n > 0) {
-    double *hq = (double *)malloc(n * sizeof(double));
-    if (!hq) return P3MG_ERR_ALLOC;
-    cudaError_t e = cudaMemcpy(hq, c->q, n * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) {
-      free(hq);
-      record_cuda_error(e);
-      return P3MG_ERR_CUDA;
-    }
-    for (size_t i = 0; i < n; i++) q2 += hq[i] * hq[i];
-    free(hq);
-  }
+  P3MG_TRY(host_q2(c, &q2));
   double alpha = 0.0;
   int kmax = 0;
   P3MG_TRY(ewald_parameters(c->n, q2, c->L, c->mesh, &alpha, &kmax));

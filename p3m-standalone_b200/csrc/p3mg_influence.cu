@@ -220,3 +220,137 @@ int influence_compute(Ctx *c, double alpha) {
 }
 
 }  // namespace p3mg
+
+// ---------------------------------------------------------------------------
+// Analytic error estimates (the reference's method.Error / method.Error_k):
+//   k space  2 q2 sqrt(he / N) / L^2 with he a sum over the mesh vectors
+//            n in [-m/2, m/2)^3 of aliasing sums over |m'| <= mc_est:
+//     ik, ik-r  p3m-ik.c:264-336     he = |-1 + sum_{n!=0} a1 - (a2/cs)^2/n^2|
+//     ik-i      p3m-ik-i.c:249-318   he = |sum_{n!=0} a1 - a2^2/(n^2/2 (a3^2 + a4^2))|
+//     ad, ad-r  p3m-ad.c:436-497     he =  sum_{all n_d!=0} a1 - a2^2/(a3 a4)
+//     ad-i      p3m-ad-i.c:205-284   he = |sum_{all n_d!=0} a1 - a2^2/(a3 a4/2 + a5 a6/2)|
+//   (the ik estimate starts from the table-miss value -1, and the ad sums
+//   skip every vector with a zero component, as the reference does);
+//   real space  2 q2 exp(-(rcut alpha)^2) / sqrt(N rcut L^3)  (realpart.c:343-346).
+// The reference substitutes interpolated tables (find_error.c:84-107) for
+// ik/ik-i at tabulated (mesh, cao); these are the sums the tables hold.
+// ---------------------------------------------------------------------------
+
+namespace p3mg {
+namespace {
+
+__device__ __forceinline__ double cot_sum(int nn, double mi, int cao) {
+  // closed form of sum over aliases of sinc^(2 cao) (p3m-common.c:77-107)
+  const double c0 = cos(P3MG_PI * mi * (double)nn);
+  const double c = c0 * c0;
+  switch (cao) {
+    case 1: return 1.0;
+    case 2: return (1.0 + c * 2.0) / 3.0;
+    case 3: return (2.0 + c * (11.0 + c * 2.0)) / 15.0;
+    case 4: return (17.0 + c * (180.0 + c * (114.0 + c * 4.0))) / 315.0;
+    case 5: return (62.0 + c * (1072.0 + c * (1452.0 + c * (247.0 + c * 2.0)))) / 2835.0;
+    case 6: return (1382.0 + c * (35396.0 + c * (83021.0 + c * (34096.0 + c * (2026.0 + c * 4.0))))) / 155925.0;
+    case 7:
+      return (21844.0 + c * (776661.0 + c * (2801040.0 + c * (2123860.0 + c * (349500.0 + c * (8166.0 + c * 4.0)))))) /
+             6081075.0;
+  }
+  return 0.0;
+}
+
+__global__ void kspace_error_kernel(int method, int m, int cao, int mc, double alpha, double L, double *__restrict__ he) {
+  __shared__ double red[8];
+  const size_t M = (size_t)m * m * m;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double contrib = 0.0;
+  if (t < M) {
+    const int h = m / 2;
+    const int nx = (int)(t / ((size_t)m * m)) - h, ny = (int)((t / m) % m) - h, nz = (int)(t % m) - h;
+    const bool ad = method_ad(method);
+    const bool any = (nx != 0) || (ny != 0) || (nz != 0);
+    const bool all = (nx != 0) && (ny != 0) && (nz != 0);
+    if (ad ? all : any) {
+      const double mi = 1.0 / m;
+      const double f1 = (P3MG_PI / (alpha * L)) * (P3MG_PI / (alpha * L));
+      double a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0, a6 = 0;
+      for (int mx = -mc; mx <= mc; mx++)
+        for (int my = -mc; my <= mc; my++)
+          for (int mz = -mc; mz <= mc; mz++) {
+            const double nmx = nx + mx * m, nmy = ny + my * m, nmz = nz + mz * m;
+            const double nm2 = nmx * nmx + nmy * nmy + nmz * nmz;
+            const double ex = exp(-f1 * nm2);
+            const double sx = sinc_pi(mi * nmx), sy = sinc_pi(mi * nmy), sz = sinc_pi(mi * nmz);
+            const double U2 = ipow_d(sx * sy * sz, 2 * cao);
+            const bool even = ((mx + my + mz) % 2) == 0;
+            a1 += ex * ex / nm2;
+            if (ad) {
+              a2 += U2 * ex;
+              a3 += U2 * nm2;
+              a4 += U2;
+              a5 += even ? U2 * nm2 : -U2 * nm2;
+              a6 += even ? U2 : -U2;
+            } else {
+              a2 += U2 * ex * (nx * nmx + ny * nmy + nz * nmz) / nm2;
+              a3 += U2;
+              a4 += even ? U2 : -U2;
+            }
+          }
+      const double n2 = (double)(nx * nx + ny * ny + nz * nz);
+      if (method == 0 || method == 6) {
+        const double cs = cot_sum(nx, mi, cao) * cot_sum(ny, mi, cao) * cot_sum(nz, mi, cao);
+        contrib = a1 - (a2 / cs) * (a2 / cs) / n2;
+      } else if (method == 1) {
+        contrib = a1 - a2 * a2 / (0.5 * n2 * (a3 * a3 + a4 * a4));
+      } else if (method == 3) {
+        contrib = a1 - a2 * a2 / (0.5 * (a3 * a4 + a5 * a6));
+      } else if (a3 != 0.0 && a4 != 0.0) {
+        contrib = a1 - a2 * a2 / (a3 * a4);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = contrib;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+    atomicAdd(he, s);
+  }
+}
+
+}  // namespace
+
+int error_estimates(Ctx *c, double alpha, double rcut, int mc_est, double q2, double est[3]) {
+  const int m = c->mesh;
+  const size_t M = c->M;
+  const double L = c->L;
+  const int n = c->n;
+  double *d_he = nullptr;
+  P3MG_CUDA_TRY(cudaMalloc(&d_he, sizeof(double)));
+  cudaError_t e = cudaMemsetAsync(d_he, 0, sizeof(double), c->stream);
+  if (e == cudaSuccess) {
+    kspace_error_kernel<<<(unsigned)((M + 255) / 256), 256, 0, c->stream>>>(c->method, m, c->cao, mc_est, alpha, L,
+                                                                           d_he);
+    c->launches++;
+    e = cudaGetLastError();
+  }
+  double he = 0.0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&he, d_he, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d_he);
+  if (e != cudaSuccess) {
+    record_cuda_error(e);
+    return P3MG_ERR_CUDA;
+  }
+  if (c->method == 0 || c->method == 6) he -= 1.0;
+  if (c->method != 2 && c->method != 7) he = fabs(he);
+  const double ek = (n > 0) ? 2.0 * q2 * sqrt(he / (double)n) / (L * L) : 0.0;
+  const double er = (n > 0 && rcut > 0.0) ? (2.0 * q2 * exp(-(rcut * alpha) * (rcut * alpha))) /
+                                                sqrt((double)n * rcut * L * L * L)
+                                          : 0.0;
+  est[0] = sqrt(er * er + ek * ek);
+  est[1] = ek;
+  est[2] = er;
+  return P3MG_OK;
+}
+
+}  // namespace p3mg

@@ -164,6 +164,9 @@ int influence_compute(Ctx *c, double alpha);
 int kspace_prepare(Ctx *c);
 int kspace_run(Ctx *c);  // scatter, FFTs, convolution, gather, self-force into c->fk / c->f
 
+// analytic error estimates (p3mg_influence.cu): est = total, k space, real space
+int error_estimates(Ctx *c, double alpha, double rcut, int mc_est, double q2, double est[3]);
+
 // FP64 Ewald reference (p3mg_ewald.cu)
 int ewald_parameters(int n, double q2, double L, int mesh_param, double *alpha, int *kmax);
 int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, double *d_out);

@@ -90,6 +90,7 @@ def load():
     L.p3mg_get_influence.argtypes = [vp, _dp, _dp]
     L.p3mg_ewald_forces.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp, _dp,
                                     ctypes.POINTER(ctypes.c_int)]
+    L.p3mg_error_estimate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
     L.p3mg_kernel_times.argtypes = [vp, _dp]
     L.p3mg_set_graph.argtypes = [vp, ctypes.c_int]
     L.p3mg_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -232,6 +233,14 @@ class Context:
         _check(self._lib.p3mg_ewald_forces(self._h, nt, tp, _p(f[0]), _p(f[1]), _p(f[2]), ctypes.byref(a),
                                            ctypes.byref(k)), "p3mg_ewald_forces")
         return dict(f=f, alpha=a.value, kmax=k.value)
+
+    def error_estimate(self, alpha, rcut, mc_est=1):
+        """Analytic RMS error estimates (method.Error / Error_k, Realspace_error):
+        dict total, kspace, realspace."""
+        e = np.zeros(3)
+        _check(self._lib.p3mg_error_estimate(self._h, float(alpha), float(rcut), int(mc_est), _p(e)),
+               "p3mg_error_estimate")
+        return dict(total=e[0], kspace=e[1], realspace=e[2])
 
     def kernel_times(self):
         t = np.zeros(3)

@@ -1,6 +1,8 @@
 """FP64 Ewald reference forces on the GPU (p3mg_ewald_forces) against the
 oracle's Ewald, the reference's own Ewald outputs (golden fixtures) and
-the reference fixture tests-wall.for."""
+the reference fixture tests-wall.for; the analytic error estimates
+(p3mg_error_estimate) against the oracle's restatement of the reference's
+estimate functions."""
 import os
 
 import numpy as np
@@ -64,3 +66,22 @@ def test_p3m_error_close_to_reference_estimate(gpu):
     est = np.hypot(O.kspace_error(2, 24, 5, 1, 1.0, n, float(np.sum(q * q)), L),
                    O.realspace_error(n, float(np.sum(q * q)), L, 3.5, 1.0))
     assert 0.3 * est <= err <= 3.0 * est, (err, est)
+
+
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 6, 7])
+def test_error_estimates_match_oracle(gpu, method):
+    n, L = 400, 9.0
+    x, y, z, q = p3mg.generate_system(0, n, L, seed=34)
+    q2 = float(np.sum(q * q))
+    for mesh, cao, mc, alpha, rcut in [(16, 5, 1, 1.1, 3.0), (20, 3, 2, 0.9, 2.5), (12, 7, 1, 1.4, 3.0)]:
+        with p3mg.Context(method, mesh, cao, 1) as ctx:
+            ctx.set_system(x, y, z, q, L)
+            est = ctx.error_estimate(alpha, rcut, mc)
+        ek = O.kspace_error(method, mesh, cao, mc, alpha, n, q2, L)
+        er = O.realspace_error(n, q2, L, rcut, alpha)
+        # The k-space estimate is sqrt of a difference of two mesh sums
+        # (the aliased numerator minus the optimal-G term); the GPU sums them
+        # in a different order, so the cancellation leaves ~1e-10 relative.
+        assert abs(est["kspace"] - ek) <= 1e-8 * abs(ek)
+        assert abs(est["realspace"] - er) <= 1e-12 * er
+        assert abs(est["total"] - np.hypot(ek, er)) <= 1e-8 * np.hypot(ek, er)
