@@ -130,9 +130,21 @@ int p3mg_stage_times(p3mg_ctx *ctx, double t[4]);
  * range P3M_BRILLOUIN_TUNING (CLI "mc_est", default 1).  Replaces
  * method.Error / method.Error_k (p3m-ik.c:249-336, p3m-ik-i.c:249-320,
  * p3m-ad.c:436-505, p3m-ad-i.c:205-294) and Realspace_error
- * (realpart.c:343-346); for ik/ik-i at meshes the reference tabulates
- * (find_error.c:84-107) it interpolates stored values of these sums instead. */
+ * (realpart.c:343-346).  For ik (0, 6) and ik-i (1) at the meshes the
+ * reference tabulates (q.c:1), cao 1..7 and alpha*L <= 100 the reference
+ * interpolates precomputed sums at alpha*L = 0, 1, ..., 100
+ * (find_error.c:84-107); this evaluates the sums at the two bracketing
+ * points and interpolates the same way. */
 int p3mg_error_estimate(p3mg_ctx *ctx, double alpha, double rcut, int mc_est, double est[3]);
+
+/* The same estimates without a context, from the system's particle count n,
+ * q2 = sum q_i^2 and box length L (all the reference's estimate functions
+ * read from system_t), on the calling thread's current device.  The form a
+ * method table's Error(system_t*, parameters_t*) / Error_k entry can call
+ * (types.h:306-316).  mesh must be even (the estimate loops run over
+ * -mesh/2 .. mesh/2-1). */
+int p3mg_estimate_errors(int method_id, int mesh, int cao, int mc_est, int n, double q2, double L, double alpha,
+                         double rcut, double est[3]);
 
 /* FP64 Ewald reference forces for the context's particles, evaluated on nt
  * target particles (targets: host array of particle indices, or NULL with
@@ -145,6 +157,25 @@ int p3mg_error_estimate(p3mg_ctx *ctx, double alpha, double rcut, int mc_est, do
  * Ewald energy is not reproduced (ewald.c:169 accumulates only the last k). */
 int p3mg_ewald_forces(p3mg_ctx *ctx, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
                       double *alpha_out, int *kmax_out);
+
+/* The same reference computation with every output of
+ * Calculate_reference_forces: total forces f_* and k-space forces fk_*
+ * (either triple may be NULL), alpha, kmax and the Ewald error estimate the
+ * reference prints as "Reference precision" (method_ewald.Error,
+ * ewald.c:199-201, common.c:361).  What Write_exact_forces (io.c:159-177)
+ * writes for reference_out. */
+int p3mg_ewald_reference(p3mg_ctx *ctx, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
+                         double *fk_x, double *fk_y, double *fk_z, double *alpha_out, int *kmax_out,
+                         double *precision_out);
+
+/* FP64 Ewald k-space forces at a given alpha with the spherical cutoff
+ * 0 < |n|^2 <= kmax^2, written to fk_* (nt each) for the target particles
+ * (as p3mg_ewald_forces).  The reference's method 4 Kspace_force as
+ * main.c:392-396 uses it for the "error_k" column: Ewald_init with the P3M
+ * mesh and Ewald_compute_influence_function (ewald.c:84-119), i.e. kmax =
+ * mesh - 1, at each alpha of the sweep. */
+int p3mg_ewald_kspace_forces(p3mg_ctx *ctx, double alpha, int kmax, int nt, const int *targets, double *fk_x,
+                             double *fk_y, double *fk_z);
 
 /* Copy the FP64 influence function (mesh^3 doubles, full mesh, index
  * (i*mesh + j)*mesh + k as r_ind, p3m-common.h:25) and the 81 ad self-force

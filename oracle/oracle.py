@@ -50,6 +50,8 @@ def lib():
         L.oracle_ewald_parameters.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _ip]
         L.oracle_ewald.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip,
                                                               _dp, _dp, _dp, _dp, _ip]
+        L.oracle_ewald_kspace_plain.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double, ctypes.c_double,
+                                                                            ctypes.c_int, ctypes.c_int, _ip, _dp]
         L.oracle_rms_error.argtypes = [ctypes.c_int, _dp, _dp]
         L.oracle_rms_error.restype = ctypes.c_double
         L.oracle_realspace_error.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4
@@ -81,6 +83,10 @@ def ref():
         R.ref_ewald.restype = ctypes.c_double
         R.ref_error_estimates.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp,
                                                                ctypes.c_double, _dp]
+        R.ref_ewald_kspace_main.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double, ctypes.c_int,
+                                                                         ctypes.c_double, _dp]
+        R.ref_find_error.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        R.ref_find_error.restype = ctypes.c_double
         R.ref_realteil.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double] * 3 + [_dp, _dp]
         _ref = R
     return _ref
@@ -176,6 +182,27 @@ def ewald(x, y, z, q, L, mesh_param, targets=None):
     return dict(f=f.reshape(3, nt), f_k=fk.reshape(3, nt), f_r=fr.reshape(3, nt), alpha=float(a[0]), kmax=int(k[0]))
 
 
+def ewald_kspace_plain(x, y, z, q, L, alpha, kmax, targets=None):
+    """Ewald k-space forces with the cutoff 0 < |n|^2 <= kmax^2 (main.c's error_k column uses kmax = mesh - 1)."""
+    x, y, z, q = map(_arr, (x, y, z, q))
+    n = len(x)
+    if targets is None:
+        nt, tp = n, None
+    else:
+        tgt = np.ascontiguousarray(targets, dtype=np.int32)
+        nt, tp = len(tgt), tgt.ctypes.data_as(_ip)
+    fk = np.zeros(3 * nt)
+    lib().oracle_ewald_kspace_plain(n, _ptr(x), _ptr(y), _ptr(z), _ptr(q), L, alpha, kmax, nt, tp, _ptr(fk))
+    return fk.reshape(3, nt)
+
+
+def ref_ewald_kspace_main(x, y, z, q, L, mesh, alpha):
+    x, y, z, q = map(_arr, (x, y, z, q))
+    fk = np.zeros(3 * len(x))
+    ref().ref_ewald_kspace_main(len(x), _ptr(x), _ptr(y), _ptr(z), _ptr(q), L, mesh, alpha, _ptr(fk))
+    return fk.reshape(3, len(x))
+
+
 def kspace_error(method, mesh, cao, mc_est, alpha, n, q2, L):
     return lib().oracle_kspace_error(method, mesh, cao, mc_est, alpha, n, q2, L)
 
@@ -236,6 +263,14 @@ def ref_error_estimates(method, mesh, cao, mc, alpha, rcut, q, L):
     if rc:
         raise ValueError("ref_error_estimates failed")
     return e
+
+
+def ref_find_error(alphaL, mesh, cao, method):
+    return ref().ref_find_error(alphaL, mesh, cao, method)
+
+
+def estimate_table_mesh(mesh):
+    return bool(lib().oracle_estimate_table_mesh(mesh))
 
 
 def ref_realteil(x, y, z, q, L, rcut, alpha):

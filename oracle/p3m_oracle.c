@@ -583,23 +583,25 @@ int oracle_ewald_parameters(int n, double q2, double L, int mesh_param, double *
  * (Ewald_init -> Init_data, p3m-common.c:218) and again with cutoff
  * (kmax-1)^2 over indices < kmax (common.c:352), so entries with an index
  * equal to kmax keep the first cutoff. */
-static double ewald_ghat(int ax, int ay, int az, int kmax, double alpha, double L) {
+static double ewald_ghat(int ax, int ay, int az, int kmax, int shell, double alpha, double L) {
   int n2 = ax * ax + ay * ay + az * az;
-  int cut = (ax == kmax || ay == kmax || az == kmax) ? kmax * kmax : (kmax - 1) * (kmax - 1);
+  int cut = (!shell || ax == kmax || ay == kmax || az == kmax) ? kmax * kmax : (kmax - 1) * (kmax - 1);
   if (n2 == 0 || n2 > cut) return 0.0;
   return 2.0 / SQ(L) / n2 * exp(-SQ(ORC_PI / (alpha * L)) * n2);
 }
 
 /* k-space Ewald force on the targets tgt[0..nt) from all n sources
- * (ewald.c:122-166) accumulated into fk (3nt). */
-int oracle_ewald_kspace(int n, const double *x, const double *y, const double *z, const double *q, double L, double alpha,
-                        int kmax, int nt, const int *tgt, double *fk) {
+ * (ewald.c:122-166) accumulated into fk (3nt).  shell != 0: the influence
+ * table of the reference-force driver (above); shell == 0: the plain
+ * cutoff |n|^2 <= kmax^2. */
+static int ewald_kspace(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                        double alpha, int kmax, int shell, int nt, const int *tgt, double *fk) {
   const double Leni = 1.0 / L;
   for (int nx = -kmax; nx <= kmax; nx++)
     for (int ny = -kmax; ny <= kmax; ny++)
       for (int nz = -kmax; nz <= kmax; nz++) {
         if (nx * nx + ny * ny + nz * nz > kmax * kmax) continue;
-        double g = ewald_ghat(abs(nx), abs(ny), abs(nz), kmax, alpha, L);
+        double g = ewald_ghat(abs(nx), abs(ny), abs(nz), kmax, shell, alpha, L);
         double re = 0.0, im = 0.0;
         for (int i = 0; i < n; i++) {
           double kr = 2.0 * ORC_PI * Leni * (nx * x[i] + ny * y[i] + nz * z[i]);
@@ -617,6 +619,20 @@ int oracle_ewald_kspace(int n, const double *x, const double *y, const double *z
         }
       }
   return 0;
+}
+
+int oracle_ewald_kspace(int n, const double *x, const double *y, const double *z, const double *q, double L, double alpha,
+                        int kmax, int nt, const int *tgt, double *fk) {
+  return ewald_kspace(n, x, y, z, q, L, alpha, kmax, 1, nt, tgt, fk);
+}
+
+/* The Ewald k-space forces of main.c's "error_k" column (main.c:392-396):
+ * the influence table is first filled at alpha = 0 (all zero, main.c:190-196
+ * before Ewald_init) and then at alpha with kmax = mesh - 1
+ * (ewald.c:84-109), so the sum runs over 0 < |n|^2 <= (mesh-1)^2. */
+int oracle_ewald_kspace_plain(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                              double alpha, int kmax, int nt, const int *tgt, double *fk) {
+  return ewald_kspace(n, x, y, z, q, L, alpha, kmax, 0, nt, tgt, fk);
 }
 
 /* Reference forces (Calculate_reference_forces, common.c:329-363) on the
@@ -683,17 +699,12 @@ static double cot_sum(int nn, double mi, int cao) {
   return 0.0;
 }
 
-/* Analytic k-space error estimates (the non-tabulated branches):
+/* Mesh-sum part of the analytic k-space error estimates:
  * ik p3m-ik.c:264-336, ik-i p3m-ik-i.c:249-318, ad p3m-ad.c:436-497,
- * ad-i p3m-ad-i.c:205-284.  mc_est = P3M_BRILLOUIN_TUNING. */
-double oracle_kspace_error(int method, int m, int cao, int mc_est, double alpha, int n, double q2, double L) {
+ * ad-i p3m-ad-i.c:205-284.  mc_est = P3M_BRILLOUIN_TUNING.  Returns the
+ * accumulated he_q starting from `he` (before the final fabs). */
+static double kspace_he(int method, int m, int cao, int mc_est, double alpha, double L, double he) {
   const double mi = 1.0 / m, f1 = SQ(ORC_PI / (alpha * L));
-  /* ik / ik-r start from the table-lookup miss value -1 (p3m-ik.c:266-291:
-   * he_q = p3m_find_error(...) = -1, then += over the mesh); the other
-   * methods start from 0.  Only the non-tabulated branch is restated: for
-   * tabulated (mesh, cao) the reference interpolates its generated q_*.c
-   * tables instead (find_error.c:84-107). */
-  double he = (method == 0 || method == 6) ? -1.0 : 0.0;
   for (int nx = -m / 2; nx < m / 2; nx++)
     for (int ny = -m / 2; ny < m / 2; ny++)
       for (int nz = -m / 2; nz < m / 2; nz++) {
@@ -735,6 +746,47 @@ double oracle_kspace_error(int method, int m, int cao, int mc_est, double alpha,
           he += a1 - SQ(a2) / (a3 * a4);
         }
       }
-  if (method != 2 && method != 7) he = fabs(he);
+  return he;
+}
+
+/* Mesh sizes the reference ships precomputed k-space error tables for
+ * (q.c:1, 83 sizes): the even 13-smooth sizes 4..300 except 286 = 2*11*13,
+ * plus 360, 400, 480 and 512. */
+int oracle_estimate_table_mesh(int m) {
+  if (m == 360 || m == 400 || m == 480 || m == 512) return 1;
+  if (m < 4 || m > 300 || (m % 2) || (m % 143) == 0) return 0;
+  int r = m;
+  static const int primes[6] = {2, 3, 5, 7, 11, 13};
+  for (int i = 0; i < 6; i++)
+    while (r % primes[i] == 0) r /= primes[i];
+  return r == 1;
+}
+
+/* Analytic k-space error estimate (Error_k of the method table).
+ *
+ * ik (0, 6) and ik-i (1) first look alpha*L up in precomputed tables
+ * (p3m-ik.c:267, p3m-ik-i.c:301, find_error.c:84-107): for a tabulated
+ * mesh, cao 1..7 and alpha*L <= 100 the reference interpolates linearly
+ * between the table's values at alpha*L = 0, 1, ..., 100.  Those table
+ * values are the same mesh sum evaluated at the grid points (to the
+ * table's 7 printed digits) with mc_est = 0 for ik and mc_est = 1 for ik-i,
+ * so the table branch is restated by evaluating the sum at the two
+ * bracketing grid points.  On a miss, ik
+ * keeps the lookup's -1 as the start of its sum (p3m-ik.c:266-291); ik-i
+ * resets to 0 (p3m-ik-i.c:303). */
+double oracle_kspace_error(int method, int m, int cao, int mc_est, double alpha, int n, double q2, double L) {
+  const double aL = alpha * L;
+  double he;
+  if ((method == 0 || method == 1 || method == 6) && oracle_estimate_table_mesh(m) && cao >= 1 && cao <= 7 &&
+      aL <= 100.0) {
+    const int l = (int)floor(aL);
+    const double d = aL - l;
+    const int mc_tab = (method == 1) ? 1 : 0;
+    he = (1.0 - d) * fabs(kspace_he(method, m, cao, mc_tab, (double)l / L, L, 0.0));
+    if (d != 0.0) he += d * fabs(kspace_he(method, m, cao, mc_tab, (double)(l + 1) / L, L, 0.0));
+  } else {
+    he = kspace_he(method, m, cao, mc_est, alpha, L, (method == 0 || method == 6) ? -1.0 : 0.0);
+    if (method != 2 && method != 7) he = fabs(he);
+  }
   return 2.0 * q2 * sqrt(he / (double)n) / SQ(L);
 }

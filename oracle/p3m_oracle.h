@@ -15,10 +15,13 @@ int oracle_forces(int method, int mesh, int cao, int mc, double alpha, double rc
 int oracle_ewald_parameters(int n, double q2, double L, int mesh_param, double *alpha, int *kmax);
 int oracle_ewald_kspace(int n, const double *x, const double *y, const double *z, const double *q, double L, double alpha,
                         int kmax, int nt, const int *tgt, double *fk);
+int oracle_ewald_kspace_plain(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                              double alpha, int kmax, int nt, const int *tgt, double *fk);
 int oracle_ewald(int n, const double *x, const double *y, const double *z, const double *q, double L, int mesh_param,
                  int nt, const int *tgt, double *f, double *fk, double *fr, double *alpha_out, int *kmax_out);
 double oracle_rms_error(int n, const double *f, const double *ref);
 double oracle_realspace_error(int n, double q2, double L, double rcut, double alpha);
+int oracle_estimate_table_mesh(int mesh);
 double oracle_kspace_error(int method, int mesh, int cao, int mc_est, double alpha, int n, double q2, double L);
 
 #endif

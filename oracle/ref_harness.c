@@ -22,6 +22,7 @@
 #include "p3m-ad-i.h"
 #include "p3m-ik-real.h"
 #include "p3m-ad-real.h"
+#include "find_error.h"
 
 static const method_t *method_by_id(int id) {
   switch (id) {
@@ -152,6 +153,31 @@ double ref_ewald(int n, const double *x, const double *y, const double *z, const
   return err;
 }
 
+/* Ewald k-space forces the way main.c's "error_k" column gets them
+ * (main.c:190-196 copies the parameters with alpha = 0 before
+ * method_ewald.Init; main.c:392-396 per alpha): Init with the P3M mesh, then
+ * Influence_function and Kspace_force at alpha.  fk: 3n, overwritten. */
+int ref_ewald_kspace_main(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                          int mesh, double alpha, double *fk) {
+  system_t *s = make_system(n, x, y, z, q, L);
+  forces_t *f = Init_forces(n);
+  parameters_t p;
+  memset(&p, 0, sizeof(p));
+  p.mesh = mesh;
+  p.cao = 1;
+  p.cao3 = 1;
+  p.alpha = 0.0;
+  data_t *d = method_ewald.Init(s, &p);
+  p.alpha = alpha;
+  method_ewald.Influence_function(s, &p, d);
+  method_ewald.Kspace_force(s, &p, d, f);
+  copy_out(f->f_k, n, fk);
+  Free_data(d);
+  Free_forces(f);
+  Free_system(s);
+  return 0;
+}
+
 /* The method's error estimates (Error, Error_k) and Realspace_error. */
 int ref_error_estimates(int method_id, int mesh, int cao, int mc, double alpha, double rcut, int n, const double *q,
                         double L, double *est3) {
@@ -176,6 +202,12 @@ int ref_error_estimates(int method_id, int mesh, int cao, int mc, double alpha, 
   Free_system(s);
   free(zero);
   return 0;
+}
+
+/* The reference's precomputed-table lookup (find_error.c:84-107): the
+ * interpolated he_q for a tabulated (mesh, cao) or -1 on a miss. */
+double ref_find_error(double alphaL, int mesh, int cao, int method_id) {
+  return p3m_find_error(alphaL, mesh, cao, method_id);
 }
 
 /* The reference's real-space N^2 loop alone (realpart.c:124-167). */

@@ -54,14 +54,23 @@ gsl_rng *gsl_rng_alloc(const gsl_rng_type *t) {
 void gsl_rng_free(gsl_rng *r) { free(r); }
 double gsl_rng_uniform(const gsl_rng *r) { return mt_next((gsl_rng *)r) / 4294967296.0; }
 
+static double uniform_pos(const gsl_rng *r) {
+  double x;
+  do x = gsl_rng_uniform(r);
+  while (x == 0.0);
+  return x;
+}
+
+/* GSL's gsl_ran_gaussian: polar Box-Muller on two gsl_rng_uniform_pos draws
+ * (x, y) in the unit disc, returning the y-based variate. */
 double gsl_ran_gaussian(const gsl_rng *r, double sigma) {
-  double u, v, s;
+  double x, y, s;
   do {
-    u = 2.0 * gsl_rng_uniform(r) - 1.0;
-    v = 2.0 * gsl_rng_uniform(r) - 1.0;
-    s = u * u + v * v;
-  } while (s >= 1.0 || s == 0.0);
-  return sigma * u * sqrt(-2.0 * log(s) / s);
+    x = -1.0 + 2.0 * uniform_pos(r);
+    y = -1.0 + 2.0 * uniform_pos(r);
+    s = x * x + y * y;
+  } while (s > 1.0 || s == 0.0);
+  return sigma * y * sqrt(-2.0 * log(s) / s);
 }
 
 double gsl_sf_bessel_I0(double x) {

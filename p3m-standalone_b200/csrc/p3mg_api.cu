@@ -551,33 +551,34 @@ extern "C" int p3mg_error_estimate(p3mg_ctx *h, double alpha, double rcut, int m
   cudaSetDevice(c->device);
   double q2 = 0.0;
   P3MG_TRY(host_q2(c, &q2));
-  return error_estimates(c, alpha, rcut, mc_est, q2, est);
+  return error_estimates(c->method, c->mesh, c->cao, c->n, c->L, q2, alpha, rcut, mc_est, c->stream, &c->launches,
+                         est);
 }
 
-extern "C" int p3mg_ewald_forces(p3mg_ctx *h, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
-                                 double *alpha_out, int *kmax_out) {
-  if (!h) return P3MG_ERR_ARG;
-  Ctx *c = &h->c;
-  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
-  if (nt < 0 || (nt > 0 && (!f_x || !f_y || !f_z))) return P3MG_ERR_ARG;
-  if (!targets && nt != c->n) return P3MG_ERR_ARG;
-  cudaSetDevice(c->device);
-  const size_t n = (size_t)c->n;
-  if (targets)
-    for (int t = 0; t < nt; t++)
-      if (targets[t] < 0 || (size_t)targets[t] >= n) return P3MG_ERR_ARG;
-  double q2 = 0.0;
-  P3MG_TRY(host_q2(c, &q2));
-  double alpha = 0.0;
-  int kmax = 0;
-  P3MG_TRY(ewald_parameters(c->n, q2, c->L, c->mesh, &alpha, &kmax));
-  if (alpha_out) *alpha_out = alpha;
-  if (kmax_out) *kmax_out = kmax;
+extern "C" int p3mg_estimate_errors(int method_id, int mesh, int cao, int mc_est, int n, double q2, double L,
+                                    double alpha, double rcut, double est[3]) {
+  if (!est) return P3MG_ERR_ARG;
+  if (!(method_id == 0 || method_id == 1 || method_id == 2 || method_id == 3 || method_id == 6 || method_id == 7))
+    return P3MG_ERR_METHOD;
+  if (cao < 1 || cao > P3MG_MAX_CAO) return P3MG_ERR_CAO;
+  if (mesh < 2 || mesh > P3MG_MAX_MESH || (mesh % 2)) return P3MG_ERR_MESH;
+  if (n < 1 || !(q2 >= 0.0) || !(L > 0.0) || !(alpha > 0.0) || !(rcut >= 0.0) || mc_est < 0) return P3MG_ERR_ARG;
+  return error_estimates(method_id, mesh, cao, n, L, q2, alpha, rcut, mc_est, cudaStreamPerThread, nullptr, est);
+}
+
+// Shared body of the Ewald entries: checks the targets, uploads them, runs
+// the Ewald kernels and copies the requested outputs (f and/or fk, each
+// three host arrays of nt doubles or NULL) back to the host.
+static int ewald_common(Ctx *c, int nt, const int *targets, double alpha, int kmax, bool shell, double rcut_real,
+                        double *const f[3], double *const fk[3]) {
   if (nt == 0) return P3MG_OK;
   int *d_tgt = nullptr;
-  double *d_out = nullptr;
+  double *d_out = nullptr, *d_fk = nullptr;
+  const size_t bytes = 3 * (size_t)nt * sizeof(double);
   int st = P3MG_OK;
-  cudaError_t e = cudaMalloc(&d_out, 3 * (size_t)nt * sizeof(double));
+  cudaError_t e = cudaSuccess;
+  if (f) e = cudaMalloc(&d_out, bytes);
+  if (e == cudaSuccess && fk) e = cudaMalloc(&d_fk, bytes);
   if (e == cudaSuccess && targets) {
     e = cudaMalloc(&d_tgt, (size_t)nt * sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(d_tgt, targets, (size_t)nt * sizeof(int), cudaMemcpyHostToDevice);
@@ -586,11 +587,12 @@ extern "C" int p3mg_ewald_forces(p3mg_ctx *h, int nt, const int *targets, double
     record_cuda_error(e);
     st = (e == cudaErrorMemoryAllocation) ? P3MG_ERR_ALLOC : P3MG_ERR_CUDA;
   } else {
-    st = ewald_forces(c, nt, d_tgt, alpha, kmax, d_out);
-    if (st == P3MG_OK) {
-      double *dst[3] = {f_x, f_y, f_z};
-      for (int d = 0; d < 3 && e == cudaSuccess; d++)
-        e = cudaMemcpy(dst[d], d_out + (size_t)d * nt, (size_t)nt * sizeof(double), cudaMemcpyDeviceToHost);
+    st = ewald_forces(c, nt, d_tgt, alpha, kmax, shell, rcut_real, d_out, d_fk);
+    for (int w = 0; w < 2 && st == P3MG_OK; w++) {
+      double *const *dst = w ? fk : f;
+      const double *src = w ? d_fk : d_out;
+      for (int d = 0; dst && d < 3 && e == cudaSuccess; d++)
+        e = cudaMemcpy(dst[d], src + (size_t)d * nt, (size_t)nt * sizeof(double), cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) {
         record_cuda_error(e);
         st = P3MG_ERR_CUDA;
@@ -599,5 +601,58 @@ extern "C" int p3mg_ewald_forces(p3mg_ctx *h, int nt, const int *targets, double
   }
   if (d_tgt) cudaFree(d_tgt);
   if (d_out) cudaFree(d_out);
+  if (d_fk) cudaFree(d_fk);
   return st;
+}
+
+static int check_targets(const Ctx *c, int nt, const int *targets) {
+  if (nt < 0 || (!targets && nt != c->n)) return P3MG_ERR_ARG;
+  if (targets)
+    for (int t = 0; t < nt; t++)
+      if (targets[t] < 0 || targets[t] >= c->n) return P3MG_ERR_ARG;
+  return P3MG_OK;
+}
+
+extern "C" int p3mg_ewald_reference(p3mg_ctx *h, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
+                                    double *fk_x, double *fk_y, double *fk_z, double *alpha_out, int *kmax_out,
+                                    double *precision_out) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  const bool want_f = f_x || f_y || f_z, want_fk = fk_x || fk_y || fk_z;
+  if (want_f && !(f_x && f_y && f_z)) return P3MG_ERR_ARG;
+  if (want_fk && !(fk_x && fk_y && fk_z)) return P3MG_ERR_ARG;
+  P3MG_TRY(check_targets(c, nt, targets));
+  cudaSetDevice(c->device);
+  double q2 = 0.0;
+  P3MG_TRY(host_q2(c, &q2));
+  double alpha = 0.0;
+  int kmax = 0;
+  P3MG_TRY(ewald_parameters(c->n, q2, c->L, c->mesh, &alpha, &kmax));
+  if (alpha_out) *alpha_out = alpha;
+  if (kmax_out) *kmax_out = kmax;
+  if (precision_out) *precision_out = ewald_error(c->n, q2, c->L, 0.49 * c->L, kmax, alpha);
+  double *const f[3] = {f_x, f_y, f_z};
+  double *const fk[3] = {fk_x, fk_y, fk_z};
+  return ewald_common(c, nt, targets, alpha, kmax, true, 0.49 * c->L, want_f ? f : nullptr, want_fk ? fk : nullptr);
+}
+
+extern "C" int p3mg_ewald_forces(p3mg_ctx *h, int nt, const int *targets, double *f_x, double *f_y, double *f_z,
+                                 double *alpha_out, int *kmax_out) {
+  if (h && nt > 0 && (!f_x || !f_y || !f_z)) return P3MG_ERR_ARG;
+  return p3mg_ewald_reference(h, nt, targets, f_x, f_y, f_z, nullptr, nullptr, nullptr, alpha_out, kmax_out,
+                              nullptr);
+}
+
+extern "C" int p3mg_ewald_kspace_forces(p3mg_ctx *h, double alpha, int kmax, int nt, const int *targets,
+                                        double *fk_x, double *fk_y, double *fk_z) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!(alpha > 0.0) || kmax < 1 || kmax > 4096) return P3MG_ERR_ARG;
+  if (nt > 0 && (!fk_x || !fk_y || !fk_z)) return P3MG_ERR_ARG;
+  P3MG_TRY(check_targets(c, nt, targets));
+  cudaSetDevice(c->device);
+  double *const fk[3] = {fk_x, fk_y, fk_z};
+  return ewald_common(c, nt, targets, alpha, kmax, false, 0.0, nullptr, fk);
 }

@@ -34,9 +34,11 @@ namespace {
 constexpr int EW_THREADS = 256;
 constexpr int EW_KZC = 16;  // k_z values per CTA
 
-__device__ __forceinline__ double ewald_ghat(int ax, int ay, int az, int kmax, double fak1, double fak2) {
+// shell: the reference-force quirk above (cutoff (kmax-1)^2 except on the
+// outer faces); otherwise the plain spherical cutoff kmax^2.
+__device__ __forceinline__ double ewald_ghat(int ax, int ay, int az, int kmax, bool shell, double fak1, double fak2) {
   const int n2 = ax * ax + ay * ay + az * az;
-  const int cut = (ax == kmax || ay == kmax || az == kmax) ? kmax * kmax : (kmax - 1) * (kmax - 1);
+  const int cut = (!shell || ax == kmax || ay == kmax || az == kmax) ? kmax * kmax : (kmax - 1) * (kmax - 1);
   if (n2 == 0 || n2 > cut) return 0.0;
   return fak1 / n2 * exp(-fak2 * n2);
 }
@@ -104,8 +106,8 @@ __global__ void __launch_bounds__(EW_THREADS) ewald_sk_kernel(const double *__re
 __global__ void ewald_kforce_kernel(const double *__restrict__ x, const double *__restrict__ y,
                                     const double *__restrict__ z, const double *__restrict__ q,
                                     const int *__restrict__ tgt, int nt, double twopi_L, const int2 *__restrict__ cols,
-                                    int ncol, int kmax, double fak1, double fak2, const double2 *__restrict__ S,
-                                    double *__restrict__ fk) {
+                                    int ncol, int kmax, bool shell, double fak1, double fak2,
+                                    const double2 *__restrict__ S, double *__restrict__ fk) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   const int i = tgt ? tgt[t] : t;
@@ -126,7 +128,7 @@ __global__ void ewald_kforce_kernel(const double *__restrict__ x, const double *
     sincos(twopi_L * (double)kz_lo * zi, &sz, &cz);
     double er = cxy * cz - s * sz, ei = s * cz + cxy * sz;
     for (int kz = kz_lo; kz <= kz_hi; kz++) {
-      const double g = ewald_ghat(abs(kx), abs(ky), abs(kz), kmax, fak1, fak2);
+      const double g = ewald_ghat(abs(kx), abs(ky), abs(kz), kmax, shell, fak1, fak2);
       if (g != 0.0) {
         const double2 sk = S[(size_t)c * nz + (kz + kmax)];
         // q_i g (rhohat_re sin(k.r_i) + rhohat_im cos(k.r_i)), rhohat = S (ewald.c:160-161);
@@ -207,6 +209,13 @@ double err_k(double q2, int n, double L, int kmax, double a) {
 
 }  // namespace
 
+// estimated RMS force error of the Ewald sum with real-space cutoff rcut
+// (Ewald_estimate_error, ewald.c:199-201)
+double ewald_error(int n, double q2, double L, double rcut, int kmax, double alpha) {
+  const double r = err_r(q2, L, rcut, alpha), k = err_k(q2, n, L, kmax, alpha);
+  return sqrt(r * r + k * k);
+}
+
 // alpha and kmax of the reference Ewald sum (see the file comment)
 int ewald_parameters(int n, double q2, double L, int mesh_param, double *alpha, int *kmax) {
   const double rcut = 0.49 * L;
@@ -233,9 +242,12 @@ int ewald_parameters(int n, double q2, double L, int mesh_param, double *alpha, 
   return P3MG_OK;
 }
 
-// Ewald reference forces on nt targets (device index array or NULL for all);
-// out: 3 nt doubles on the device (x block, y block, z block), overwritten.
-int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, double *d_out) {
+// Ewald forces on nt targets (device index array or NULL for all).
+// d_fk (may be NULL): k-space forces, 3 nt doubles (x block, y block, z
+// block), overwritten.  d_out (may be NULL): total forces, k space plus the
+// real-space sum with cutoff rcut_real (none if rcut_real <= 0), overwritten.
+int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, bool shell, double rcut_real,
+                 double *d_out, double *d_fk) {
   const int n = c->n;
   const double L = c->L;
   const double twopi_L = 2.0 * P3MG_PI / L;
@@ -265,22 +277,31 @@ int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, doubl
   do {
     e = cudaMemcpyAsync(d_cols, cols.data(), sizeof(int2) * ncol, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_S, 0, sizeof(double2) * (size_t)ncol * nz, c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_out, 0, sizeof(double) * 3 * (size_t)nt, c->stream);
+    double *kout = d_fk ? d_fk : d_out;
+    const size_t bytes = sizeof(double) * 3 * (size_t)nt;
+    if (e == cudaSuccess && d_fk) e = cudaMemsetAsync(d_fk, 0, bytes, c->stream);
+    if (e == cudaSuccess && d_out) e = cudaMemsetAsync(d_out, 0, bytes, c->stream);
     if (e != cudaSuccess) break;
-    if (n > 0) {
+    if (n > 0 && kout) {
       dim3 grid(ncol, (nz + EW_KZC - 1) / EW_KZC);
       ewald_sk_kernel<<<grid, EW_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, twopi_L, d_cols, kmax, d_S);
       ewald_kforce_kernel<<<(nt + 127) / 128, 128, 0, c->stream>>>(c->x, c->y, c->z, c->q, d_tgt, nt, twopi_L, d_cols,
-                                                                   ncol, kmax, fak1, fak2, d_S, d_out);
+                                                                   ncol, kmax, shell, fak1, fak2, d_S, kout);
+      c->launches += 2;
+      if (d_fk && d_out) e = cudaMemcpyAsync(d_out, d_fk, bytes, cudaMemcpyDeviceToDevice, c->stream);
+      if (e == cudaSuccess) e = cudaGetLastError();
+      if (e != cudaSuccess) break;
+    }
+    if (n > 0 && d_out && rcut_real > 0.0) {
       // enough CTAs for the whole GPU: split the sources into slices
       const int tb = (nt + 255) / 256;
       int nsplit = (4 * 148 + tb - 1) / tb;
       nsplit = nsplit < 1 ? 1 : nsplit;
       const int slice = (n + nsplit - 1) / nsplit;
       nsplit = (n + slice - 1) / slice;
-      ewald_real_kernel<<<dim3(tb, nsplit), 256, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, d_tgt, nt, L, 0.49 * L,
+      ewald_real_kernel<<<dim3(tb, nsplit), 256, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, d_tgt, nt, L, rcut_real,
                                                                  alpha, slice, d_out);
-      c->launches += 3;
+      c->launches += 1;
       e = cudaGetLastError();
       if (e != cudaSuccess) break;
     }

@@ -319,30 +319,61 @@ __global__ void kspace_error_kernel(int method, int m, int cao, int mc, double a
 
 }  // namespace
 
-int error_estimates(Ctx *c, double alpha, double rcut, int mc_est, double q2, double est[3]) {
-  const int m = c->mesh;
-  const size_t M = c->M;
-  const double L = c->L;
-  const int n = c->n;
+// Mesh sizes the reference ships precomputed k-space error tables for
+// (q.c:1, 83 sizes): the even 13-smooth sizes 4..300 except 286 = 2*11*13,
+// plus 360, 400, 480 and 512.
+bool estimate_table_mesh(int m) {
+  if (m == 360 || m == 400 || m == 480 || m == 512) return true;
+  if (m < 4 || m > 300 || (m % 2) || (m % 143) == 0) return false;
+  int r = m;
+  for (int p : {2, 3, 5, 7, 11, 13})
+    while (r % p == 0) r /= p;
+  return r == 1;
+}
+
+// Analytic error estimates (Error / Error_k / Realspace_error of the method
+// table).  ik (0, 6) and ik-i (1) first look alpha*L up in precomputed
+// tables (p3m-ik.c:267, p3m-ik-i.c:301, find_error.c:84-107): for a
+// tabulated mesh, cao 1..7 and alpha*L <= 100 the reference interpolates
+// linearly between table values at alpha*L = 0, 1, ..., 100, which are the
+// mesh sum at those points with mc_est = 0 (ik) or 1 (ik-i).  Here the sum
+// is evaluated at the two bracketing grid points instead of reading a table.
+// On a miss ik starts its sum from the lookup's -1 (p3m-ik.c:266-291).
+int error_estimates(int method, int m, int cao, int n, double L, double q2, double alpha, double rcut, int mc_est,
+                    cudaStream_t stream, long long *launches, double est[3]) {
+  const size_t M = (size_t)m * m * m;
+  const double aL = alpha * L;
+  const bool ik = (method == 0 || method == 6);
+  const bool table = (ik || method == 1) && estimate_table_mesh(m) && cao >= 1 && cao <= 7 && aL <= 100.0;
+  const int l = table ? (int)floor(aL) : 0;
+  const double d = table ? aL - l : 0.0;
+  const int nsum = (table && d != 0.0) ? 2 : 1;
   double *d_he = nullptr;
-  P3MG_CUDA_TRY(cudaMalloc(&d_he, sizeof(double)));
-  cudaError_t e = cudaMemsetAsync(d_he, 0, sizeof(double), c->stream);
-  if (e == cudaSuccess) {
-    kspace_error_kernel<<<(unsigned)((M + 255) / 256), 256, 0, c->stream>>>(c->method, m, c->cao, mc_est, alpha, L,
-                                                                           d_he);
-    c->launches++;
+  P3MG_CUDA_TRY(cudaMalloc(&d_he, 2 * sizeof(double)));
+  cudaError_t e = cudaMemsetAsync(d_he, 0, 2 * sizeof(double), stream);
+  for (int s = 0; s < nsum && e == cudaSuccess; s++) {
+    const double a = table ? (double)(l + s) / L : alpha;
+    const int mc = table ? (ik ? 0 : 1) : mc_est;
+    kspace_error_kernel<<<(unsigned)((M + 255) / 256), 256, 0, stream>>>(method, m, cao, mc, a, L, d_he + s);
+    if (launches) ++*launches;
     e = cudaGetLastError();
   }
-  double he = 0.0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&he, d_he, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  double he2[2] = {0.0, 0.0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(he2, d_he, sizeof(he2), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   cudaFree(d_he);
   if (e != cudaSuccess) {
     record_cuda_error(e);
     return P3MG_ERR_CUDA;
   }
-  if (c->method == 0 || c->method == 6) he -= 1.0;
-  if (c->method != 2 && c->method != 7) he = fabs(he);
+  double he;
+  if (table) {
+    he = (1.0 - d) * fabs(he2[0]) + ((nsum == 2) ? d * fabs(he2[1]) : 0.0);
+  } else {
+    he = he2[0];
+    if (ik) he -= 1.0;
+    if (method != 2 && method != 7) he = fabs(he);
+  }
   const double ek = (n > 0) ? 2.0 * q2 * sqrt(he / (double)n) / (L * L) : 0.0;
   const double er = (n > 0 && rcut > 0.0) ? (2.0 * q2 * exp(-(rcut * alpha) * (rcut * alpha))) /
                                                 sqrt((double)n * rcut * L * L * L)

@@ -165,11 +165,14 @@ int kspace_prepare(Ctx *c);
 int kspace_run(Ctx *c);  // scatter, FFTs, convolution, gather, self-force into c->fk / c->f
 
 // analytic error estimates (p3mg_influence.cu): est = total, k space, real space
-int error_estimates(Ctx *c, double alpha, double rcut, int mc_est, double q2, double est[3]);
+int error_estimates(int method, int m, int cao, int n, double L, double q2, double alpha, double rcut, int mc_est,
+                    cudaStream_t stream, long long *launches, double est[3]);
 
 // FP64 Ewald reference (p3mg_ewald.cu)
 int ewald_parameters(int n, double q2, double L, int mesh_param, double *alpha, int *kmax);
-int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, double *d_out);
+int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, bool shell, double rcut_real,
+                 double *d_out, double *d_fk);
+double ewald_error(int n, double q2, double L, double rcut, int kmax, double alpha);
 
 // real space (p3mg_pairs.cu)
 int pairs_reserve(Ctx *c, double rcut);

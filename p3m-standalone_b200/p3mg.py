@@ -90,6 +90,11 @@ def load():
     L.p3mg_get_influence.argtypes = [vp, _dp, _dp]
     L.p3mg_ewald_forces.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp, _dp,
                                     ctypes.POINTER(ctypes.c_int)]
+    L.p3mg_ewald_reference.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)] + [_dp] * 7 + [
+        ctypes.POINTER(ctypes.c_int), _dp]
+    L.p3mg_ewald_kspace_forces.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]
+    L.p3mg_estimate_errors.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 4 + [_dp]
     L.p3mg_error_estimate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
     L.p3mg_kernel_times.argtypes = [vp, _dp]
     L.p3mg_set_graph.argtypes = [vp, ctypes.c_int]
@@ -218,21 +223,45 @@ class Context:
         _check(self._lib.p3mg_stage_times(self._h, _p(t)), "p3mg_stage_times")
         return dict(t_c=t[0], t_g=t[1], t_f=t[2], t_r=t[3])
 
+    def _targets(self, targets):
+        if targets is None:
+            return self.n, None
+        tg = np.ascontiguousarray(targets, dtype=np.int32)
+        self._tg = tg
+        return len(tg), tg.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
     def ewald_forces(self, targets=None):
         """FP64 Ewald reference forces on the targets (indices; None = all):
         dict f (3, nt), alpha, kmax (Calculate_reference_forces, common.c:329-363)."""
-        if targets is None:
-            nt, tp = self.n, None
-        else:
-            tg = np.ascontiguousarray(targets, dtype=np.int32)
-            self._tg = tg
-            nt, tp = len(tg), tg.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        nt, tp = self._targets(targets)
         f = np.zeros((3, nt))
         a = ctypes.c_double(0.0)
         k = ctypes.c_int(0)
         _check(self._lib.p3mg_ewald_forces(self._h, nt, tp, _p(f[0]), _p(f[1]), _p(f[2]), ctypes.byref(a),
                                            ctypes.byref(k)), "p3mg_ewald_forces")
         return dict(f=f, alpha=a.value, kmax=k.value)
+
+    def ewald_reference(self, targets=None):
+        """Every output of Calculate_reference_forces: dict f, f_k (3, nt), alpha,
+        kmax and the Ewald error estimate 'precision'."""
+        nt, tp = self._targets(targets)
+        f = np.zeros((3, nt))
+        fk = np.zeros((3, nt))
+        a = ctypes.c_double(0.0)
+        k = ctypes.c_int(0)
+        e = ctypes.c_double(0.0)
+        _check(self._lib.p3mg_ewald_reference(self._h, nt, tp, _p(f[0]), _p(f[1]), _p(f[2]), _p(fk[0]), _p(fk[1]),
+                                              _p(fk[2]), ctypes.byref(a), ctypes.byref(k), ctypes.byref(e)),
+               "p3mg_ewald_reference")
+        return dict(f=f, f_k=fk, alpha=a.value, kmax=k.value, precision=e.value)
+
+    def ewald_kspace_forces(self, alpha, kmax, targets=None):
+        """Ewald k-space forces (3, nt) with the cutoff 0 < |n|^2 <= kmax^2."""
+        nt, tp = self._targets(targets)
+        fk = np.zeros((3, nt))
+        _check(self._lib.p3mg_ewald_kspace_forces(self._h, float(alpha), int(kmax), nt, tp, _p(fk[0]), _p(fk[1]),
+                                                  _p(fk[2])), "p3mg_ewald_kspace_forces")
+        return fk
 
     def error_estimate(self, alpha, rcut, mc_est=1):
         """Analytic RMS error estimates (method.Error / Error_k, Realspace_error):
@@ -303,6 +332,15 @@ class Method:
     @staticmethod
     def Kspace_force(ctx, forces):
         ctx.kspace_forces(forces["f_k"], forces["f"])
+
+
+def estimate_errors(method, mesh, cao, n, q2, L, alpha, rcut, mc_est=1):
+    """Analytic RMS error estimates without a context (p3mg_estimate_errors):
+    dict total, kspace, realspace."""
+    e = np.zeros(3)
+    _check(load().p3mg_estimate_errors(int(method), int(mesh), int(cao), int(mc_est), int(n), float(q2), float(L),
+                                       float(alpha), float(rcut), _p(e)), "p3mg_estimate_errors")
+    return dict(total=e[0], kspace=e[1], realspace=e[2])
 
 
 def calculate_forces(ctx, rcut):

@@ -14,6 +14,9 @@ Outputs (numpy .npz, float64):
                 (system_type 0, charges +-1 alternating) with the reference's
                 method-7 forces (mesh 16, cao 7, rcut 3, mc 2) at three alphas
                 of the 0.1..2.5 step 0.05 sweep, and its Ewald forces.
+  cli/*.dat  -- the out.dat tables of the reference program (oracle/_ref/p3m)
+                for the command lines in CLI_CASES, each with its own
+                generated system and Ewald reference forces.
 The GPU box never runs this script; tests read the .npz files only.
 """
 import os
@@ -38,6 +41,39 @@ WALL_CASES = [
     (6, 16, 6, 1, 1.1, 3.0),
     (7, 16, 7, 2, 1.1, 3.0),
 ]
+
+
+# command lines of the reference program whose out.dat tables are kept
+CLI_CASES = {
+    "m7_type0": "particles 300 box 8 mesh 12 cao 5 rcut 2.5 method 7 mc 2 alphamin 0.5 alphamax 1.5 "
+                "alphastep 0.25 error_k",
+    "m1_type3": "particles 300 box 8 mesh 12 cao 5 rcut 2.5 method 1 system_type 3 alphamin 0.5 alphamax 1.5 "
+                "alphastep 0.25 error_k",
+    "m0_type5": "particles 400 box 9 mesh 16 cao 3 rcut 2.5 method 0 system_type 5 alphamin 0.6 alphamax 1.4 "
+                "alphastep 0.2 error_k",
+    "m3_type1": "particles 300 box 8 mesh 14 cao 4 rcut 2.5 method 3 system_type 1 alphamin 0.8 alphamax 1.2 "
+                "alphastep 0.2 mc_est 2",
+    "m6_type4": "particles 300 box 8 mesh 12 cao 6 rcut 2.5 method 6 system_type 4 alphamin 0.8 "
+                "alphamax 1.2 alphastep 0.2",
+    "m2_type2": "particles 216 box 8 mesh 12 cao 7 rcut 2.5 method 2 system_type 2 alphamin 0.9 alphamax 1.3 "
+                "alphastep 0.2",
+}
+
+
+def make_cli_goldens():
+    import subprocess
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "p3m")
+    os.makedirs(os.path.join(HERE, "cli"), exist_ok=True)
+    for name, args in CLI_CASES.items():
+        with tempfile.TemporaryDirectory() as tmp:
+            out = os.path.join(tmp, "out.dat")
+            subprocess.run([exe] + args.split() + ["outfile", out], cwd=tmp, check=True, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL)
+            with open(out) as f:
+                text = f.read()
+        with open(os.path.join(HERE, "cli", name + ".dat"), "w") as f:
+            f.write("# " + args + "\n" + text)
 
 
 def main(ref_dir):
@@ -72,7 +108,8 @@ def main(ref_dir):
     out["ewald_alpha"] = e["alpha"]
     out["ewald_kmax"] = e["kmax"]
     np.savez_compressed(os.path.join(HERE, "sweep.npz"), **out)
-    print("wrote", os.path.join(HERE, "wall.npz"), os.path.join(HERE, "sweep.npz"))
+    make_cli_goldens()
+    print("wrote", os.path.join(HERE, "wall.npz"), os.path.join(HERE, "sweep.npz"), os.path.join(HERE, "cli"))
 
 
 if __name__ == "__main__":

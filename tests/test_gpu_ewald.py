@@ -73,15 +73,57 @@ def test_error_estimates_match_oracle(gpu, method):
     n, L = 400, 9.0
     x, y, z, q = p3mg.generate_system(0, n, L, seed=34)
     q2 = float(np.sum(q * q))
-    for mesh, cao, mc, alpha, rcut in [(16, 5, 1, 1.1, 3.0), (20, 3, 2, 0.9, 2.5), (12, 7, 1, 1.4, 3.0)]:
-        with p3mg.Context(method, mesh, cao, 1) as ctx:
-            ctx.set_system(x, y, z, q, L)
-            est = ctx.error_estimate(alpha, rcut, mc)
+    # 16, 20, 12 take the reference's tabulated branch for ik/ik-i (alpha*L on
+    # and off the table's grid); 34 and 38 are untabulated (and have no FFT
+    # here, so they go through the context-free entry).
+    for mesh, cao, mc, alpha, rcut in [(16, 5, 1, 1.1, 3.0), (20, 3, 2, 0.9, 2.5), (12, 7, 1, 1.4, 3.0),
+                                       (16, 7, 2, 10.0 / 9.0, 3.0), (34, 3, 1, 1.1, 3.0), (38, 5, 2, 0.95, 3.0)]:
+        est = p3mg.estimate_errors(method, mesh, cao, n, q2, L, alpha, rcut, mc)
         ek = O.kspace_error(method, mesh, cao, mc, alpha, n, q2, L)
         er = O.realspace_error(n, q2, L, rcut, alpha)
-        # The k-space estimate is sqrt of a difference of two mesh sums
-        # (the aliased numerator minus the optimal-G term); the GPU sums them
-        # in a different order, so the cancellation leaves ~1e-10 relative.
-        assert abs(est["kspace"] - ek) <= 1e-8 * abs(ek)
+        # The k-space estimate is sqrt of a difference of mesh sums (the
+        # aliased numerator minus the optimal-G term) that cancel to ~1e-7 of
+        # their size; the GPU sums them in another order, so agreement is
+        # ~1e-7 relative rather than machine precision.
+        assert abs(est["kspace"] - ek) <= 1e-6 * abs(ek), (mesh, cao, est["kspace"], ek)
         assert abs(est["realspace"] - er) <= 1e-12 * er
-        assert abs(est["total"] - np.hypot(ek, er)) <= 1e-8 * np.hypot(ek, er)
+        assert abs(est["total"] - np.hypot(ek, er)) <= 1e-6 * np.hypot(ek, er)
+
+
+def test_ewald_reference_outputs_match_oracle(gpu):
+    x, y, z, q = p3mg.generate_system(0, 300, 9.0, seed=36)
+    ref = O.ewald(x, y, z, q, 9.0, 12)
+    tg = np.arange(0, 300, 7)
+    with p3mg.Context(2, 12, 4, 1) as ctx:
+        ctx.set_system(x, y, z, q, 9.0)
+        r = ctx.ewald_reference()
+        rt = ctx.ewald_reference(tg)
+    assert (r["alpha"], r["kmax"]) == (ref["alpha"], ref["kmax"])
+    assert O.rel_rms(r["f"].ravel(), ref["f"].ravel()) <= 1e-10
+    assert O.rel_rms(r["f_k"].ravel(), ref["f_k"].ravel()) <= 1e-10
+    assert O.rel_rms(rt["f_k"].ravel(), ref["f_k"][:, tg].ravel()) <= 1e-10
+    assert 0.0 < r["precision"] <= 1e-8
+
+
+def test_ewald_kspace_forces_error_k_column(gpu):
+    x, y, z, q = p3mg.generate_system(0, 250, 8.0, seed=37)
+    with p3mg.Context(1, 10, 5, 1) as ctx:
+        ctx.set_system(x, y, z, q, 8.0)
+        for alpha, kmax in [(0.9, 9), (1.4, 5)]:
+            fk = ctx.ewald_kspace_forces(alpha, kmax)
+            o = O.ewald_kspace_plain(x, y, z, q, 8.0, alpha, kmax)
+            assert O.rel_rms(fk.ravel(), o.ravel()) <= 1e-10
+        with pytest.raises(p3mg.P3MGError):
+            ctx.ewald_kspace_forces(0.0, 5)
+
+
+def test_context_free_estimates_match_context(gpu):
+    x, y, z, q = p3mg.generate_system(0, 500, 10.0, seed=38)
+    q2 = float(np.sum(q * q))
+    for method in (0, 1, 2, 3, 6, 7):
+        with p3mg.Context(method, 16, 5, 1) as ctx:
+            ctx.set_system(x, y, z, q, 10.0)
+            a = ctx.error_estimate(0.83, 3.0, 1)
+        b = p3mg.estimate_errors(method, 16, 5, 500, q2, 10.0, 0.83, 3.0, 1)
+        for k in ("total", "kspace", "realspace"):
+            assert abs(a[k] - b[k]) <= 1e-12 * abs(a[k])

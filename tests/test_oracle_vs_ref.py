@@ -71,3 +71,34 @@ def test_error_estimates_untabulated(method):
         ok = O.kspace_error(method, mesh, cao, mc, 1.1, 200, 200.0, 8.0)
         assert abs(ok - e[1]) <= 1e-12 * abs(e[1])
         assert abs(O.realspace_error(200, 200.0, 8.0, 3.0, 1.1) - e[2]) <= 1e-15
+
+
+def test_estimate_table_meshes_match_reference_lookup():
+    # The table lookup answers -1 exactly for the meshes the reference has no table for.
+    for mesh in range(1, 601):
+        assert (O.ref_find_error(50.5, mesh, 3, 1) >= 0.0) == O.estimate_table_mesh(mesh), mesh
+
+
+@pytest.mark.parametrize("method", [0, 1, 6])
+def test_error_estimates_tabulated(method):
+    # Tabulated (mesh, cao): the reference interpolates its precomputed tables; the
+    # oracle evaluates the same mesh sum at the two bracketing alpha*L grid points.
+    # The tables hold 7 significant digits; at alpha*L where the mesh sum falls
+    # below ~1e-8 it is a cancellation of much larger terms and the table and
+    # the sum only agree to a few digits, so the cases stay above that.
+    n, L = 200, 8.0
+    q = 1.0 - 2.0 * (np.arange(n) % 2)
+    for mesh, cao, alpha in [(16, 7, 1.25), (16, 3, 0.8), (20, 5, 1.6), (12, 2, 2.0), (32, 4, 2.2), (16, 7, 12.6)]:
+        e = O.ref_error_estimates(method, mesh, cao, 2, alpha, 3.0, q, L)
+        ok = O.kspace_error(method, mesh, cao, 2, alpha, n, float(n), L)
+        assert abs(ok - e[1]) <= 2e-6 * abs(e[1]), (mesh, cao, alpha, ok, e[1])
+        assert abs(np.hypot(ok, O.realspace_error(n, float(n), L, 3.0, alpha)) - e[0]) <= 2e-6 * e[0]
+
+
+def test_ewald_kspace_error_k_column_matches_reference():
+    # main.c's error_k column: Ewald k-space forces with the P3M mesh as table size
+    x, y, z, q = p3mg.generate_system(0, 120, 7.0, seed=5)
+    for mesh, alpha in [(6, 1.2), (8, 0.7)]:
+        r = O.ref_ewald_kspace_main(x, y, z, q, 7.0, mesh, alpha)
+        o = O.ewald_kspace_plain(x, y, z, q, 7.0, alpha, mesh - 1)
+        assert O.rel_rms(o.ravel(), r.ravel()) <= 1e-13
