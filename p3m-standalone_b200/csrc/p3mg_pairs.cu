@@ -3,16 +3,20 @@
 //   f_i += q_i q_j (erfc(alpha r)/r + 2 alpha/sqrt(pi) exp(-alpha^2 r^2)) / r^2 * d
 //   E   += 1/2 q_i q_j erfc(alpha r)/r
 // The reference loops over all N^2 pairs.  Here particles are counting-sorted
-// into a cell list of side >= rcut (nc = floor(L/rcut) >= 3 cells per side),
-// each cell split into 2x2x2 half-cells, which visits exactly the same pair
-// set.  One CTA per cell stages the 6x6x6 half-cells around it through
-// shared memory; a particle in half-cell u only tests the 5x5x5 half-cells
-// whose distance from u can be <= rcut (about 58 % of the 27-cell
-// candidates).  Within a CTA each warp takes one i at a time: its lanes test
-// 32 candidates per step, the accepted ones are compacted (ballot + prefix
-// count) into a circular per-warp queue, and 32 interactions are evaluated
-// at once whenever the queue holds 32 -- the erfc branch runs on full warps
-// although only ~15 % of the 27-cell candidates are within rcut.
+// into a cell list of side > rcut (nc = floor(L / (rcut (1 + 1e-6))) >= 3
+// cells per side), each cell split into 2x2x2 half-cells of side h, which
+// visits exactly the same pair set.  One CTA per cell stages the 6x6x6
+// half-cells around it through shared memory in (J0, J1, J2) order, so each
+// half-cell column (J0, J1) is one contiguous range.  Within a CTA each warp
+// takes one i at a time: its lanes first clip the 5x5 columns that can hold
+// partners of i (xy distance of i from the column <= rcut, z range cut to
+// the half-cells the rcut sphere reaches), concatenate the surviving ranges
+// (prefix sum + __fns over the lanes), and then test 32 candidates per step
+// with every lane busy -- about 450 candidates per i at density 1 and
+// rcut 3.5 against 180 partners.  Accepted candidates are compacted (ballot
+// + prefix count) into a circular per-warp queue, and 32 interactions are
+// evaluated at once whenever the queue holds 32, so the erfc branch runs on
+// full warps.
 //
 // FP64: a conservative FP32 filter, then every queued pair is evaluated
 // exactly like the reference (dx -= round(dx/L) L with separately rounded
@@ -120,7 +124,7 @@ template <bool DBL>
 __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__restrict__ posv,
                                                                const int *__restrict__ sidx,
                                                                const int *__restrict__ start, int nc, double L,
-                                                               double rcut, double alpha, int cull,
+                                                               double rcut, double alpha,
                                                                double *__restrict__ fr, int n,
                                                                double *__restrict__ energy) {
   typedef typename PairAcc<DBL>::type acc_t;
@@ -133,7 +137,6 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   unsigned short *queue = reinterpret_cast<unsigned short *>(sfi + 3 * PAIR_MAXI);
   __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
   __shared__ double cell_off[27][3];
-  __shared__ unsigned short runs[8][36][2];
   __shared__ double ered[PAIR_WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned short *q = queue + warp * PAIR_QCAP;
@@ -170,29 +173,6 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
     for (int sg = 0; sg < PAIR_NSEG; sg++) seg_pre[sg + 1] += seg_pre[sg];
   }
   __syncthreads();
-  // candidate runs of each sub-cell u: for every (J0, J1) in range one
-  // contiguous J2 range.  With cull, half-cells two steps away along an axis
-  // (at least 2h > rcut apart) are skipped: |J - U| <= 2.
-  for (int e = tid; e < 8 * 36; e += PAIR_CTA) {
-    const int u = e / 36, r = e % 36;
-    const int U0 = (u >> 2) & 1, U1 = (u >> 1) & 1, U2 = u & 1;
-    int lo0 = -2, hi0 = 3, lo1 = -2, hi1 = 3, lo2 = -2, hi2 = 3;
-    if (cull) {
-      lo0 = max(-2, U0 - 2); hi0 = min(3, U0 + 2);
-      lo1 = max(-2, U1 - 2); hi1 = min(3, U1 + 2);
-      lo2 = max(-2, U2 - 2); hi2 = min(3, U2 + 2);
-    }
-    const int n0 = hi0 - lo0 + 1, n1 = hi1 - lo1 + 1;
-    unsigned short a = 0, b = 0;
-    if (r < n0 * n1) {
-      const int J0 = lo0 + r / n1, J1 = lo1 + r % n1;
-      const int base = (J0 + 2) * 36 + (J1 + 2) * 6;
-      a = (unsigned short)seg_pre[base + (lo2 + 2)];
-      b = (unsigned short)seg_pre[base + (hi2 + 2) + 1];
-    }
-    runs[u][r][0] = a;
-    runs[u][r][1] = b;
-  }
   const int total = seg_pre[PAIR_NSEG];
   const bool fits = total <= PAIR_JCH;
   const int i0 = start[cell * 8], i1 = start[cell * 8 + 8];
@@ -206,6 +186,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   const double wupi = 1.77245385090551602729816748334;
   const float rc2f = DBL ? (float)(rcut * rcut * (1.0 + 1e-4)) : (float)rcut * (float)rcut;
   const float alphaf = (float)alpha, preff = (float)(2.0 * alpha / wupi);
+  const float hf = (float)(0.5 * cs), hinvf = (float)(2.0 / cs);
+  const float prune_r2 = (float)(rcut * rcut * (1.0 + 1e-4));
   const double prefd = 2.0 * alpha / wupi;
   const float4 *pos32 = reinterpret_cast<const float4 *>(posv);
   const double4 *pos64 = reinterpret_cast<const double4 *>(posv);
@@ -224,8 +206,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
       }
       sfi[3 * t] = sfi[3 * t + 1] = sfi[3 * t + 2] = (acc_t)0;
     }
-    // all candidates in one chunk when they fit (sub-cell runs), else chunks
-    // of the flat candidate order without culling
+    // all candidates in one chunk when they fit (pruned columns), else chunks
+    // of the flat candidate order
     for (int k0 = 0; k0 < total; k0 += PAIR_JCH) {
       const int kn = min(PAIR_JCH, total - k0);
       __syncthreads();
@@ -306,22 +288,72 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
           head += take;
           __syncwarp();
         };
-        const int nrun = fits ? (cull ? 25 : 36) : 1;
-        for (int r = 0; r < nrun; r++) {
-          const int a = fits ? runs[u][r][0] : 0;
-          const int b = fits ? runs[u][r][1] : kn;
-          for (int jb = a; jb < b; jb += 32) {
-            const int kk = jb + lane;
-            // branch-free test: the load index is clamped into the staged range
-            const float4 pj = cf[min(kk, PAIR_JCH - 1)];
-            const float dx = pif.x - pj.x, dy = pif.y - pj.y, dz = pif.z - pj.z;
-            const bool ok = (kk < b) & (dx * dx + dy * dy + dz * dz <= rc2f) & (kk != kself);
-            const unsigned mask = __ballot_sync(0xffffffffu, ok);
-            if (ok) q[(tail + __popc(mask & ((1u << lane) - 1u))) & (PAIR_QCAP - 1)] = (unsigned short)kk;
-            tail += __popc(mask);
-            // at most 63 queued: one full round drains it below 32
-            if (tail - head >= 32) process(32);
+        // one candidate test per lane; hits go to the warp's queue
+        auto test_push = [&](int kk, bool valid) {
+          const float4 pj = cf[valid ? kk : 0];
+          const float dx = pif.x - pj.x, dy = pif.y - pj.y, dz = pif.z - pj.z;
+          const bool ok = valid & (dx * dx + dy * dy + dz * dz <= rc2f) & (kk != kself);
+          const unsigned mask = __ballot_sync(0xffffffffu, ok);
+          if (ok) q[(tail + __popc(mask & ((1u << lane) - 1u))) & (PAIR_QCAP - 1)] = (unsigned short)kk;
+          tail += __popc(mask);
+          // at most 63 queued: one full round drains it below 32
+          if (tail - head >= 32) process(32);
+        };
+        if (fits) {
+          // Candidate columns of this i: lane r < 25 owns the half-cell column
+          // (J0, J1) = (U0 - 2 + r / 5, U1 - 2 + r % 5) (cells are wider than
+          // rcut, so |J - U| <= 2 covers every partner).  The column is skipped
+          // when its xy distance from i exceeds rcut and is otherwise clipped in
+          // z to the half-cells the sphere reaches; prune_r2 carries a small
+          // margin so no pair the exact test accepts is lost.
+          const int U0 = (u >> 2) & 1, U1 = (u >> 1) & 1, U2 = u & 1;
+          int ca = 0, clen = 0;
+          if (lane < 25) {
+            const int J0 = U0 - 2 + lane / 5, J1 = U1 - 2 + lane % 5;
+            const float x0 = J0 * hf, y0 = J1 * hf;
+            const float ddx = fmaxf(fmaxf(x0 - pif.x, pif.x - (x0 + hf)), 0.0f);
+            const float ddy = fmaxf(fmaxf(y0 - pif.y, pif.y - (y0 + hf)), 0.0f);
+            const float d2 = ddx * ddx + ddy * ddy;
+            if (d2 <= prune_r2) {
+              const float zr = sqrtf(prune_r2 - d2);
+              const int lo = max((int)floorf((pif.z - zr) * hinvf), U2 - 2);
+              const int hi = min((int)floorf((pif.z + zr) * hinvf), U2 + 2);
+              if (lo <= hi) {
+                const int base = (J0 + 2) * 36 + (J1 + 2) * 6 + 2;
+                ca = seg_pre[base + lo];
+                clen = seg_pre[base + hi + 1] - ca;
+              }
+            }
           }
+          // concatenate the non-empty columns: exclusive prefix of the lengths,
+          // then lane t holds the start / prefix of the t-th non-empty column
+          int incl = clen;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+          }
+          const int ntot = __shfl_sync(0xffffffffu, incl, 31);
+          const unsigned nem = __ballot_sync(0xffffffffu, clen > 0);
+          const int excl = incl - clen;
+          const int src = (int)__fns(nem, 0, lane + 1);
+          const int colA = __shfl_sync(0xffffffffu, ca, src & 31);
+          const int colE = __shfl_sync(0xffffffffu, excl, src & 31);
+          const unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
+          int nbefore = 0;  // non-empty columns that start before this chunk
+          for (int c0 = 0; c0 < ntot; c0 += 32) {
+            const bool st = (clen > 0) & (excl >= c0) & (excl < c0 + 32);
+            const unsigned smask = __reduce_or_sync(0xffffffffu, st ? (1u << ((excl - c0) & 31)) : 0u);
+            const int rank = nbefore + __popc(smask & le) - 1;
+            nbefore += __popc(smask);
+            const int a = __shfl_sync(0xffffffffu, colA, rank & 31);
+            const int e = __shfl_sync(0xffffffffu, colE, rank & 31);
+            const int k = c0 + lane;
+            test_push(a + (k - e), k < ntot);
+          }
+        } else {
+          // the neighbourhood did not fit: this chunk of the flat candidate order
+          for (int jb = 0; jb < kn; jb += 32) test_push(jb + lane, jb + lane < kn);
         }
         if (tail != head) process((int)(tail - head));
 #pragma unroll
@@ -368,15 +400,11 @@ int launch_pairs_cells(bool dbl, const void *pos, const int *sidx, const int *st
       P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set[dbl] = true;
   }
-  // half-cells two steps apart along one axis are >= 2h > rcut apart when
-  // the half-cell side h exceeds rcut/2 (kept when they are exactly equal)
-  const double h = 0.5 * L / nc;
-  const int cull = (4.0 * h * h > rcut * rcut * (1.0 + 1e-9)) ? 1 : 0;
   const int ncell = nc * nc * nc;
   if (dbl)
-    pairs_cell_kernel<true><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, cull, fr, n, energy);
+    pairs_cell_kernel<true><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, fr, n, energy);
   else
-    pairs_cell_kernel<false><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, cull, fr, n, energy);
+    pairs_cell_kernel<false><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, fr, n, energy);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -439,8 +467,10 @@ __global__ void __launch_bounds__(BRUTE_THREADS) pairs_brute_kernel(const double
 
 }  // namespace
 
+// Cells strictly wider than rcut (by 1e-6 relative), so every pair within
+// rcut lies within two half-cells along each axis.
 static int cells_per_side(double L, double rcut) {
-  int nc = (int)floor(L / rcut);
+  int nc = (int)floor(L / (rcut * (1.0 + 1e-6)));
   return nc > 256 ? 256 : nc;
 }
 

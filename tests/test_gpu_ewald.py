@@ -81,13 +81,15 @@ def test_error_estimates_match_oracle(gpu, method):
         est = p3mg.estimate_errors(method, mesh, cao, n, q2, L, alpha, rcut, mc)
         ek = O.kspace_error(method, mesh, cao, mc, alpha, n, q2, L)
         er = O.realspace_error(n, q2, L, rcut, alpha)
-        # The k-space estimate is sqrt of a difference of mesh sums (the
-        # aliased numerator minus the optimal-G term) that cancel to ~1e-7 of
-        # their size; the GPU sums them in another order, so agreement is
-        # ~1e-7 relative rather than machine precision.
-        assert abs(est["kspace"] - ek) <= 1e-6 * abs(ek), (mesh, cao, est["kspace"], ek)
+        # The k-space estimate is 2 q2 sqrt(he / n) / L^2 with he a difference
+        # of O(1) mesh sums (the aliased numerator minus the optimal-G term);
+        # the GPU adds them in another order, so he agrees to its roundoff
+        # floor (~1e-15 absolute) rather than relative to a tiny he.
+        he = lambda e: (e * L * L / (2.0 * q2)) ** 2 * n  # noqa: E731
+        assert abs(he(est["kspace"]) - he(ek)) <= 1e-6 * he(ek) + 1e-15, (mesh, cao, est["kspace"], ek)
         assert abs(est["realspace"] - er) <= 1e-12 * er
-        assert abs(est["total"] - np.hypot(ek, er)) <= 1e-6 * np.hypot(ek, er)
+        et = np.hypot(ek, er)
+        assert abs(est["total"] - et) <= 1e-6 * et + abs(est["kspace"] - ek)
 
 
 def test_ewald_reference_outputs_match_oracle(gpu):
