@@ -58,33 +58,36 @@ __device__ __forceinline__ C mul_i(C a, int sign) {
   return r;
 }
 
-// twiddle exp(sign * 2 pi i e / m) from the forward table
+// twiddle exp(sign * 2 pi i e / m) from the forward table, 0 <= e < m
 template <typename C>
-__device__ __forceinline__ C twiddle(const C *tw, int e, int m, int sign) {
-  C t = tw[e % m];
+__device__ __forceinline__ C twiddle(const C *tw, int e, int sign) {
+  C t = tw[e];
   if (sign > 0) t.y = -t.y;
   return t;
 }
 
 // One Stockham pass of radix P over W pencils of length m held in
-// src[e*LD + c]; writes dst.  Ns = size of the sub-transforms already done.
-template <typename C, int P>
-__device__ __forceinline__ void stockham_pass(const C *__restrict__ src, C *__restrict__ dst, const C *tw, int m, int W,
-                                              int LD, int Ns, int sign) {
+// src[e*LD + c]; writes dst.  Ns = size of the sub-transforms already done;
+// j / Ns is taken as __umulhi(j, ns_magic) with ns_magic = ceil(2^32 / Ns)
+// (exact for j * Ns < 2^32; here j < 2^13 and Ns <= 512).
+template <typename C, int P, int W>
+__device__ __forceinline__ void stockham_pass(const C *__restrict__ src, C *__restrict__ dst, const C *tw, int m,
+                                              int LD, int Ns, unsigned ns_magic, int sign) {
   const int nb = m / P;  // butterflies per pencil
   const int total = nb * W;
+  const int step = m / (Ns * P);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int c = t % W;
+    const int c = t & (W - 1);
     const int j = t / W;
-    const int k = j % Ns;
+    const int jq = (Ns == 1) ? j : (int)__umulhi((unsigned)j, ns_magic);
+    const int k = j - jq * Ns;
     C v[P];
 #pragma unroll
     for (int r = 0; r < P; r++) v[r] = src[(j + r * nb) * LD + c];
-    // twiddle by W_{Ns P}^{r k} = exp(sign 2 pi i r k m/(Ns P) / m)
+    // twiddle by W_{Ns P}^{r k} = exp(sign 2 pi i r k m/(Ns P) / m); r k step < m
     if (Ns > 1) {
-      const int step = m / (Ns * P);
 #pragma unroll
-      for (int r = 1; r < P; r++) v[r] = cmul(v[r], twiddle(tw, r * k * step, m, sign));
+      for (int r = 1; r < P; r++) v[r] = cmul(v[r], twiddle(tw, r * k * step, sign));
     }
     C u[P];
     if (P == 2) {
@@ -104,11 +107,11 @@ __device__ __forceinline__ void stockham_pass(const C *__restrict__ src, C *__re
       for (int s = 0; s < P; s++) {
         C acc = v[0];
 #pragma unroll
-        for (int r = 1; r < P; r++) acc = cadd(acc, cmul(v[r], twiddle(tw, ((s * r) % P) * stepP, m, sign)));
+        for (int r = 1; r < P; r++) acc = cadd(acc, cmul(v[r], twiddle(tw, ((s * r) % P) * stepP, sign)));
         u[s] = acc;
       }
     }
-    const int base = (j / Ns) * Ns * P + k;
+    const int base = jq * Ns * P + k;
 #pragma unroll
     for (int s = 0; s < P; s++) dst[(base + s * Ns) * LD + c] = u[s];
   }
@@ -117,13 +120,16 @@ __device__ __forceinline__ void stockham_pass(const C *__restrict__ src, C *__re
 struct PassList {
   int npass;
   int radix[24];
+  int ns[24];             // sub-transform size before each pass
+  unsigned nsmagic[24];   // ceil(2^32 / ns) (unused for ns == 1)
+  unsigned mmagic;        // ceil(2^32 / m)
 };
 
-// AXIS: 0 = x (stride m^2), 1 = y (stride m), 2 = z (contiguous)
-template <typename real, int AXIS>
+// AXIS: 0 = x (stride m^2), 1 = y (stride m), 2 = z (contiguous); W pencils per CTA
+template <typename real, int AXIS, int W>
 __global__ void __launch_bounds__(FFT_THREADS) fft_axis_kernel(typename cplx<real>::type *__restrict__ data,
                                                                const typename cplx<real>::type *__restrict__ twg, int m,
-                                                               int W, PassList passes, int sign, size_t batch_stride) {
+                                                               PassList passes, int sign, size_t batch_stride) {
   typedef typename cplx<real>::type C;
   extern __shared__ unsigned char smem_raw[];
   C *tw = reinterpret_cast<C *>(smem_raw);
@@ -152,13 +158,13 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_axis_kernel(typename cplx<rea
     int e, c;
     size_t addr;
     if (AXIS == 2) {
-      c = t / m;
-      e = t % m;
+      c = (int)__umulhi((unsigned)t, passes.mmagic);
+      e = t - c * m;
       addr = (size_t)(c0 + c) * m + e;
       if (c0 + c >= nrows) continue;
     } else {
       e = t / W;
-      c = t % W;
+      c = t & (W - 1);
       if (c0 + c >= m) continue;
       if (AXIS == 1)
         addr = ((size_t)outer * m + e) * m + c0 + c;
@@ -173,12 +179,13 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_axis_kernel(typename cplx<rea
   int Ns = 1;
   for (int p = 0; p < passes.npass; p++) {
     const int P = passes.radix[p];
+    const unsigned mg = passes.nsmagic[p];
     switch (P) {
-      case 2: stockham_pass<C, 2>(src, dst, tw, m, W, LD, Ns, sign); break;
-      case 3: stockham_pass<C, 3>(src, dst, tw, m, W, LD, Ns, sign); break;
-      case 4: stockham_pass<C, 4>(src, dst, tw, m, W, LD, Ns, sign); break;
-      case 5: stockham_pass<C, 5>(src, dst, tw, m, W, LD, Ns, sign); break;
-      case 7: stockham_pass<C, 7>(src, dst, tw, m, W, LD, Ns, sign); break;
+      case 2: stockham_pass<C, 2, W>(src, dst, tw, m, LD, Ns, mg, sign); break;
+      case 3: stockham_pass<C, 3, W>(src, dst, tw, m, LD, Ns, mg, sign); break;
+      case 4: stockham_pass<C, 4, W>(src, dst, tw, m, LD, Ns, mg, sign); break;
+      case 5: stockham_pass<C, 5, W>(src, dst, tw, m, LD, Ns, mg, sign); break;
+      case 7: stockham_pass<C, 7, W>(src, dst, tw, m, LD, Ns, mg, sign); break;
     }
     Ns *= P;
     __syncthreads();
@@ -192,13 +199,13 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_axis_kernel(typename cplx<rea
     int e, c;
     size_t addr;
     if (AXIS == 2) {
-      c = t / m;
-      e = t % m;
+      c = (int)__umulhi((unsigned)t, passes.mmagic);
+      e = t - c * m;
       if (c0 + c >= nrows) continue;
       addr = (size_t)(c0 + c) * m + e;
     } else {
       e = t / W;
-      c = t % W;
+      c = t & (W - 1);
       if (c0 + c >= m) continue;
       if (AXIS == 1)
         addr = ((size_t)outer * m + e) * m + c0 + c;
@@ -209,41 +216,66 @@ __global__ void __launch_bounds__(FFT_THREADS) fft_axis_kernel(typename cplx<rea
   }
 }
 
+static unsigned magic_div(int d) { return d <= 1 ? 0u : (unsigned)((0x100000000ull + (unsigned long long)d - 1) / d); }
+
+template <typename real, int W>
+void launch_axes(Ctx *c, typename cplx<real>::type *d, const typename cplx<real>::type *tw, const PassList &pl,
+                 int nbatch, int sign, size_t smem) {
+  const int m = c->mesh;
+  const size_t stride = c->M;
+  // axis order: z (contiguous), y, x -- any order gives the same transform
+  dim3 g2((unsigned)((size_t)m * m / W + ((size_t)m * m % W ? 1 : 0)), nbatch);
+  fft_axis_kernel<real, 2, W><<<g2, FFT_THREADS, smem, c->stream>>>(d, tw, m, pl, sign, stride);
+  const int gi = (m + W - 1) / W;
+  dim3 g01((unsigned)(m * gi), nbatch);
+  fft_axis_kernel<real, 1, W><<<g01, FFT_THREADS, smem, c->stream>>>(d, tw, m, pl, sign, stride);
+  fft_axis_kernel<real, 0, W><<<g01, FFT_THREADS, smem, c->stream>>>(d, tw, m, pl, sign, stride);
+}
+
 template <typename real>
 int launch_fft3d(Ctx *c, void *data, int nbatch, int sign) {
   typedef typename cplx<real>::type C;
   const int m = c->mesh;
   PassList pl;
   pl.npass = c->plan.npass;
-  for (int i = 0; i < pl.npass; i++) pl.radix[i] = c->plan.radix[i];
+  int ns = 1;
+  for (int i = 0; i < pl.npass; i++) {
+    pl.radix[i] = c->plan.radix[i];
+    pl.ns[i] = ns;
+    pl.nsmagic[i] = magic_div(ns);
+    ns *= pl.radix[i];
+  }
+  pl.mmagic = magic_div(m);
   // pencils per tile: 128 B of contiguous data per row segment at least
   int W = (sizeof(real) == 8) ? 8 : 16;
   if (m * W * 2 * (int)sizeof(C) > 160 * 1024) W = 4;
   const size_t smem = (size_t)m * sizeof(C) + 2 * (size_t)m * (W + 1) * sizeof(C);
-  const size_t stride = c->M;
   C *d = reinterpret_cast<C *>(data);
   const C *tw = reinterpret_cast<const C *>(c->plan.tw);
-  // axis order: z (contiguous), y, x -- any order gives the same transform
-  {
-    dim3 grid((unsigned)((size_t)m * m / W + ((size_t)m * m % W ? 1 : 0)), nbatch);
-    fft_axis_kernel<real, 2><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
-  }
-  {
-    const int gi = (m + W - 1) / W;
-    dim3 grid((unsigned)(m * gi), nbatch);
-    fft_axis_kernel<real, 1><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
-    fft_axis_kernel<real, 0><<<grid, FFT_THREADS, smem, c->stream>>>(d, tw, m, W, pl, sign, stride);
-  }
+  if (W == 16)
+    launch_axes<real, 16>(c, d, tw, pl, nbatch, sign, smem);
+  else if (W == 8)
+    launch_axes<real, 8>(c, d, tw, pl, nbatch, sign, smem);
+  else
+    launch_axes<real, 4>(c, d, tw, pl, nbatch, sign, smem);
   c->launches += 3;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
 
+template <typename real, int W>
+int set_smem_limits_w() {
+  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 0, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 1, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 2, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  return P3MG_OK;
+}
+
 template <typename real>
 int set_smem_limits() {
-  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  P3MG_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<real, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  P3MG_TRY((set_smem_limits_w<real, 4>()));
+  P3MG_TRY((set_smem_limits_w<real, 8>()));
+  P3MG_TRY((set_smem_limits_w<real, 16>()));
   return P3MG_OK;
 }
 
