@@ -285,7 +285,8 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     // brick edge for the tiled charge assignment
     c->brick = (mesh >= 64) ? 8 : 4;
     c->nbrick1 = (mesh + c->brick - 1) / c->brick;
-    const int nbr = c->nbrick1 * c->nbrick1 * c->nbrick1;
+    // sort keys: bricks x mesh points per brick
+    const int nbr = c->nbrick1 * c->nbrick1 * c->nbrick1 * c->brick * c->brick * c->brick;
 #define ALLOC(ptr, bytes)                              \
   e = cudaMalloc((void **)&(ptr), (bytes));            \
   if (e != cudaSuccess) {                              \
@@ -308,6 +309,8 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     ALLOC(c->brick_start, (nbr + 1) * sizeof(int));
     ALLOC(c->brick_fill, nbr * sizeof(int));
 #undef ALLOC
+    st = scan_tmp_reserve(c, nbr);
+    if (st != P3MG_OK) break;
     cudaMemset(c->self_b, 0, 81 * sizeof(double));
     memset(c->self_b_host, 0, sizeof(c->self_b_host));
     st = fft_plan_init(c);

@@ -38,6 +38,9 @@ namespace {
 
 // ---------------------------------------------------------------- binning
 
+// Sort key of a particle: its brick (the B^3 mesh points holding the base
+// of its stencil), then the stencil base inside the brick in row-major
+// order, so that consecutive particles share mesh rows.
 __global__ void bin_bricks_kernel(const double *__restrict__ x, const double *__restrict__ y,
                                   const double *__restrict__ z, int n, double Hi, double shift, int m, int B, int nb,
                                   int *__restrict__ key, int *__restrict__ count) {
@@ -47,7 +50,8 @@ __global__ void bin_bricks_kernel(const double *__restrict__ x, const double *__
   mesh_geometry(x[i], Hi, shift, 0, m, &b0, &a);
   mesh_geometry(y[i], Hi, shift, 0, m, &b1, &a);
   mesh_geometry(z[i], Hi, shift, 0, m, &b2, &a);
-  const int k = ((b0 / B) * nb + (b1 / B)) * nb + (b2 / B);
+  const int brick = ((b0 / B) * nb + (b1 / B)) * nb + (b2 / B);
+  const int k = brick * (B * B * B) + ((b0 % B) * B + (b1 % B)) * B + (b2 % B);
   key[i] = k;
   atomicAdd(&count[k], 1);
 }
@@ -89,6 +93,69 @@ __global__ void scan_kernel(const int *__restrict__ counts, int *__restrict__ st
   if (threadIdx.x == T - 1) start[nb] = sums[T - 1];
 }
 
+// Multi-CTA exclusive scan for long count arrays: per-tile sums, a scan of
+// the tile sums (scan_kernel), then each tile scanned with its offset.
+constexpr int SCAN_TILE = 4096;  // elements per CTA: 1024 threads x 4
+
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(1024) scan_tile_sums_kernel(const int *__restrict__ counts, int nb,
+                                                               int *__restrict__ tsum) {
+  __shared__ int ws[32];
+  const int base = blockIdx.x * SCAN_TILE + threadIdx.x * 4;
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) s += (base + k < nb) ? counts[base + k] : 0;
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = warp_sum(ws[threadIdx.x]);
+    if (threadIdx.x == 0) tsum[blockIdx.x] = s;
+  }
+}
+
+__global__ void __launch_bounds__(1024) scan_tiles_kernel(const int *__restrict__ counts, int nb,
+                                                           const int *__restrict__ tstart, int *__restrict__ start) {
+  __shared__ int ws[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int base = blockIdx.x * SCAN_TILE + threadIdx.x * 4;
+  int v[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) v[k] = (base + k < nb) ? counts[base + k] : 0;
+  const int t = v[0] + v[1] + v[2] + v[3];
+  int incl = t;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += u;
+  }
+  if (lane == 31) ws[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = ws[lane], wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += u;
+    }
+    ws[lane] = wi - w;  // exclusive prefix of the warp totals
+  }
+  __syncthreads();
+  int run = tstart[blockIdx.x] + ws[warp] + incl - t;
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+    if (base + k < nb) {
+      start[base + k] = run;
+      run += v[k];
+    }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) start[nb] = tstart[gridDim.x];
+}
+
 __global__ void g_to_f32_kernel(const double *__restrict__ G, float *__restrict__ G32, size_t M) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < M) G32[t] = (float)G[t];
@@ -111,9 +178,34 @@ int scan_counts(const int *counts, int *start, int nb, cudaStream_t stream) {
   return P3MG_OK;
 }
 
+int scan_tmp_reserve(Ctx *c, int nb) {
+  const int need = 2 * (nb / SCAN_TILE + 2);
+  if (need <= c->scan_cap) return P3MG_OK;
+  if (c->scan_tmp) cudaFree(c->scan_tmp);
+  c->scan_tmp = nullptr;
+  c->scan_cap = 0;
+  P3MG_CUDA_TRY(cudaMalloc(&c->scan_tmp, sizeof(int) * need));
+  c->scan_cap = need;
+  return P3MG_OK;
+}
+
+// Exclusive scan of nb counts into start[0..nb] (start[nb] = total): one
+// CTA for short arrays, the tiled three-launch scan with the context's
+// scratch (scan_tmp_reserve, done before any graph capture) otherwise.
 int exclusive_scan(Ctx *c, const int *counts, int *start, int nb) {
-  scan_kernel<<<1, 1024, 0, c->stream>>>(counts, start, nb);
-  c->launches++;
+  if (nb <= 16 * SCAN_TILE) {
+    scan_kernel<<<1, 1024, 0, c->stream>>>(counts, start, nb);
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
+    return P3MG_OK;
+  }
+  const int ntile = (nb + SCAN_TILE - 1) / SCAN_TILE;
+  if (2 * (ntile + 1) > c->scan_cap) return P3MG_ERR_STATE;
+  int *tsum = c->scan_tmp, *tstart = c->scan_tmp + ntile + 1;
+  scan_tile_sums_kernel<<<ntile, 1024, 0, c->stream>>>(counts, nb, tsum);
+  scan_kernel<<<1, 1024, 0, c->stream>>>(tsum, tstart, ntile);
+  scan_tiles_kernel<<<ntile, 1024, 0, c->stream>>>(counts, nb, tstart, start);
+  c->launches += 3;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -121,7 +213,7 @@ int exclusive_scan(Ctx *c, const int *counts, int *start, int nb) {
 // Sort particles by brick (counting sort) for the tiled scatter / gather.
 int kspace_prepare(Ctx *c) {
   const int nb = c->nbrick1;
-  const int nbr = nb * nb * nb;
+  const int nbr = nb * nb * nb * c->brick * c->brick * c->brick;  // sort keys
   const int threads = 256;
   const int blocks = (c->n + threads - 1) / threads;
   const double Hi = (double)c->mesh / c->L;

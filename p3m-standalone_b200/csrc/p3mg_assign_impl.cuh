@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
   real *sw = tile0 + NMESH * T3;                                   // [NMESH*CHUNK][3][CAO]
   int *soff = reinterpret_cast<int *>(sw + NMESH * SCATTER_CHUNK * 3 * CAO);  // tile offset of the stencil origin
   const int bid = blockIdx.x;
-  const int p0 = start[bid], p1 = start[bid + 1];
+  const int p0 = start[bid * B * B * B], p1 = start[(bid + 1) * B * B * B];
   if (p0 == p1) return;
   for (int t = threadIdx.x; t < NMESH * T3; t += blockDim.x) tile0[t] = (real)0;
   const int bz = bid % nb, by = (bid / nb) % nb, bx = bid / (nb * nb);

@@ -80,8 +80,11 @@ struct Ctx {
   // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
   int brick = 8;
   int nbrick1 = 0;  // bricks per dimension
+  // particle counts / starts per sort key: brick, then mesh point in the
+  // brick (B^3 keys per brick); the range of brick b is
+  // brick_start[b B^3] .. brick_start[(b + 1) B^3]
   int *brick_count = nullptr, *brick_start = nullptr, *brick_fill = nullptr;
-  int *part_key = nullptr;     // brick id per particle (input order)
+  int *part_key = nullptr;     // sort key per particle (input order)
   int *sorted_idx = nullptr;   // input index of each sorted particle
   double4 *sorted_xyzq = nullptr;
 
@@ -127,6 +130,7 @@ struct Ctx {
 
   // scratch for a single-CTA scan
   int *scan_tmp = nullptr;
+  int scan_cap = 0;           // ints in scan_tmp
 };
 
 // event slots: stage markers and kernel brackets
@@ -187,6 +191,7 @@ int g_to_f32(Ctx *c);
 
 // single-CTA exclusive scan of counts[0..nb) into start[0..nb] (start[nb] = total)
 int exclusive_scan(Ctx *c, const int *counts, int *start, int nb);
+int scan_tmp_reserve(Ctx *c, int nb);
 int scan_counts(const int *counts, int *start, int nb, cudaStream_t stream);
 
 // ------------------------------------------------------------ device helpers

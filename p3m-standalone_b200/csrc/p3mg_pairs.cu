@@ -491,6 +491,7 @@ int pairs_reserve(Ctx *c, double rcut) {
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_start, sizeof(int) * (nkey + 1)));
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_fill, sizeof(int) * nkey));
     c->ncell_cap = nkey;
+    P3MG_TRY(scan_tmp_reserve(c, nkey));
   }
   return P3MG_OK;
 }
