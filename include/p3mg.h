@@ -146,6 +146,31 @@ int p3mg_error_estimate(p3mg_ctx *ctx, double alpha, double rcut, int mc_est, do
 int p3mg_estimate_errors(int method_id, int mesh, int cao, int mc_est, int n, double q2, double L, double alpha,
                          double rcut, double est[3]);
 
+/* The alphas of the reference's sweep loop `for (alpha = alphamin; alpha
+ * <= alphamax; alpha += alphastep)` (main.c:375), accumulated in double as
+ * there (0.1 .. 2.5 step 0.05 gives 49 values, the last
+ * 2.4999999999999991).  Writes min(count, cap) values to alphas (may be
+ * NULL) and returns the count (>= 0), or P3MG_ERR_ARG. */
+int p3mg_alpha_range(double alphamin, double alphamax, double alphastep, int cap, double *alphas);
+
+/* The alpha sweep of the reference's main loop (main.c:375-446) as one
+ * batched GPU pass: for each of the nalpha alphas, G_opt (as p3mg_influence)
+ * and one force evaluation (as p3mg_calculate_forces with rcut).  The
+ * charge assignment and forward FFT run once; G, pairs, convolution,
+ * backward FFTs, gather and self forces run batched over the alphas.  Each
+ * alpha's forces are the ones the single calls give.
+ *   ref_x/y/z (host, n each, may all be NULL): reference forces; then
+ *   rms_out (host, nalpha, may be NULL) receives sqrt(sum |f - ref|^2) /
+ *   sqrt(n) per alpha (Calculate_errors, error.c:21-34, main.c:446).
+ *   f_out (host, 3 n nalpha doubles, may be NULL): total forces, alpha k
+ *   component d particle i at f_out[(k * 3 + d) * n + i].
+ *   max_batch: most alphas per batched pass (0: as many as half the free
+ *   device memory holds, at most 16 GiB of buffers).
+ * The context's own influence function and forces are left as they were
+ * (its charge mesh is overwritten). */
+int p3mg_sweep(p3mg_ctx *ctx, double rcut, int nalpha, const double *alphas, const double *ref_x,
+               const double *ref_y, const double *ref_z, double *rms_out, double *f_out, int max_batch);
+
 /* FP64 Ewald reference forces for the context's particles, evaluated on nt
  * target particles (targets: host array of particle indices, or NULL with
  * nt == n for all), written (not accumulated) to the host arrays f_x/f_y/f_z

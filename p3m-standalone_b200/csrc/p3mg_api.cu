@@ -8,6 +8,8 @@
 
 #include <new>
 
+#include <vector>
+
 #include "p3mg_internal.cuh"
 
 namespace p3mg {
@@ -100,6 +102,7 @@ int free_all(Ctx *c) {
   dfree(c->fk);
   dfree(c->fr);
   dfree(c->energy);
+  dfree(c->d_alpha);
   dfree(c->brick_count);
   dfree(c->brick_start);
   dfree(c->brick_fill);
@@ -142,7 +145,7 @@ static int enqueue_step(Ctx *c, double rcut) {
     for (int s = EV_K0; s <= EV_K5; s++) cudaEventRecord(c->ev[s], c->stream);
   }
   mark(c, EV_S0);
-  if (rcut != 0.0) P3MG_TRY(pairs_run(c, rcut, c->alpha));
+  if (rcut != 0.0) P3MG_TRY(pairs_run(c, rcut, c->d_alpha, 1, c->fr, c->energy));
   mark(c, EV_S1);
   if (c->n > 0) {
     P3MG_TRY(kspace_prepare(c));
@@ -305,6 +308,7 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     }
     ALLOC(c->self_b, 81 * sizeof(double));
     ALLOC(c->energy, 2 * sizeof(double));
+    ALLOC(c->d_alpha, 2 * sizeof(double));
     ALLOC(c->brick_count, nbr * sizeof(int));
     ALLOC(c->brick_start, (nbr + 1) * sizeof(int));
     ALLOC(c->brick_fill, nbr * sizeof(int));
@@ -429,7 +433,9 @@ int p3mg_real_forces(p3mg_ctx *h, double rcut, double alpha, double *fr_x, doubl
   if (!(rcut >= 0.0) || !(alpha >= 0.0)) return P3MG_ERR_ARG;
   cudaSetDevice(c->device);
   P3MG_TRY(zero_forces(c));
-  P3MG_TRY(pairs_run(c, rcut, alpha));
+  c->h_alpha_arg = alpha;
+  P3MG_CUDA_TRY(cudaMemcpyAsync(c->d_alpha + 1, &c->h_alpha_arg, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  P3MG_TRY(pairs_run(c, rcut, c->d_alpha + 1, 1, c->fr, c->energy));
   P3MG_TRY(copy_out3(c, c->fr, fr_x, fr_y, fr_z, true));
   if (energy) {
     double e;
@@ -567,6 +573,51 @@ extern "C" int p3mg_estimate_errors(int method_id, int mesh, int cao, int mc_est
   if (mesh < 2 || mesh > P3MG_MAX_MESH || (mesh % 2)) return P3MG_ERR_MESH;
   if (n < 1 || !(q2 >= 0.0) || !(L > 0.0) || !(alpha > 0.0) || !(rcut >= 0.0) || mc_est < 0) return P3MG_ERR_ARG;
   return error_estimates(method_id, mesh, cao, n, L, q2, alpha, rcut, mc_est, cudaStreamPerThread, nullptr, est);
+}
+
+extern "C" int p3mg_alpha_range(double alphamin, double alphamax, double alphastep, int cap, double *alphas) {
+  if (!(alphastep > 0.0) || !isfinite(alphamin) || !isfinite(alphamax) || cap < 0) return P3MG_ERR_ARG;
+  // the reference's loop: alpha accumulated in double (main.c:375)
+  int k = 0;
+  for (double a = alphamin; a <= alphamax; a += alphastep) {
+    if (alphas && k < cap) alphas[k] = a;
+    k++;
+    if (k > (1 << 24)) return P3MG_ERR_ARG;
+  }
+  return k;
+}
+
+extern "C" int p3mg_sweep(p3mg_ctx *h, double rcut, int nalpha, const double *alphas, const double *ref_x,
+                          const double *ref_y, const double *ref_z, double *rms_out, double *f_out, int max_batch) {
+  if (!h || nalpha < 0 || (nalpha > 0 && !alphas) || max_batch < 0) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!(rcut >= 0.0)) return P3MG_ERR_ARG;
+  const bool want_ref = ref_x || ref_y || ref_z;
+  if (want_ref && !(ref_x && ref_y && ref_z)) return P3MG_ERR_ARG;
+  if (rms_out && !want_ref) return P3MG_ERR_ARG;
+  for (int k = 0; k < nalpha; k++)
+    if (!isfinite(alphas[k]) || alphas[k] < 0.0) return P3MG_ERR_ARG;
+  if (nalpha == 0) return P3MG_OK;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->n;
+  std::vector<double> ref;
+  if (want_ref) {
+    ref.resize(3 * n + 1);
+    memcpy(ref.data(), ref_x, n * sizeof(double));
+    memcpy(ref.data() + n, ref_y, n * sizeof(double));
+    memcpy(ref.data() + 2 * n, ref_z, n * sizeof(double));
+  }
+  size_t free_b = 0, total_b = 0;
+  P3MG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  size_t budget = free_b / 2;
+  const size_t cap = (size_t)16 << 30;
+  if (budget > cap) budget = cap;
+  if (max_batch > 0) {
+    const size_t b = (size_t)max_batch * sweep_bytes_per_alpha(c);
+    if (b < budget) budget = b;
+  }
+  return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref.data() : nullptr, rms_out, f_out, budget);
 }
 
 // Shared body of the Ewald entries: checks the targets, uploads them, runs

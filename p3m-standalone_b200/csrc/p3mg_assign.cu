@@ -164,9 +164,11 @@ __global__ void g_to_f32_kernel(const double *__restrict__ G, float *__restrict_
 }  // namespace
 
 
-int g_to_f32(Ctx *c) {
+int g_to_f32(Ctx *c) { return g_to_f32_n(c, c->G, c->G32, c->M); }
+
+int g_to_f32_n(Ctx *c, const double *G, float *G32, size_t count) {
   const int threads = 256;
-  g_to_f32_kernel<<<(unsigned)((c->M + threads - 1) / threads), threads, 0, c->stream>>>(c->G, c->G32, c->M);
+  g_to_f32_kernel<<<(unsigned)((count + threads - 1) / threads), threads, 0, c->stream>>>(G, G32, count);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
@@ -238,10 +240,17 @@ int kspace_prepare(Ctx *c) {
 
 int kspace_run_f64(Ctx *c);
 int kspace_run_f32(Ctx *c);
+int kspace_batch_f64(Ctx *c, const KspaceBatch &b);
+int kspace_batch_f32(Ctx *c, const KspaceBatch &b);
 
 int kspace_run(Ctx *c) {
   if (c->precision == P3MG_FP64) return kspace_run_f64(c);
   return kspace_run_f32(c);
+}
+
+int kspace_batch(Ctx *c, const KspaceBatch &b) {
+  if (c->precision == P3MG_FP64) return kspace_batch_f64(c, b);
+  return kspace_batch_f32(c, b);
 }
 
 }  // namespace p3mg

@@ -3,6 +3,8 @@
 #pragma once
 #include <math.h>
 
+#include <type_traits>
+
 #include "p3mg_internal.cuh"
 
 namespace p3mg {
@@ -144,6 +146,9 @@ __global__ void conv_ik_kernel(const typename cplx<real>::type *__restrict__ Q, 
   typedef typename cplx<real>::type C;
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= M) return;
+  // alpha batch (grid.y): G and the three field meshes of entry y
+  G += (size_t)blockIdx.y * M;
+  F += (size_t)blockIdx.y * 3 * M;
   const int k = (int)(t % m), j = (int)((t / m) % m), i = (int)(t / ((size_t)m * m));
   const C qv = Q[t];
   const real g = (real)G[t];
@@ -163,14 +168,19 @@ __global__ void conv_ik_kernel(const typename cplx<real>::type *__restrict__ Q, 
 }
 
 template <typename real, typename Gt>
-__global__ void conv_ad_kernel(typename cplx<real>::type *__restrict__ Q, const Gt *__restrict__ G, size_t M) {
+// Qout = G Qin (in place when Qout == Qin); alpha batch over grid.y with
+// G and Qout of entry y
+__global__ void conv_ad_kernel(const typename cplx<real>::type *Qin, const Gt *__restrict__ G, size_t M,
+                               typename cplx<real>::type *Qout) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= M) return;
+  G += (size_t)blockIdx.y * M;
+  Qout += (size_t)blockIdx.y * M;
   const real g = (real)G[t];
-  typename cplx<real>::type v = Q[t];
+  typename cplx<real>::type v = Qin[t];
   v.x *= g;
   v.y *= g;
-  Q[t] = v;
+  Qout[t] = v;
 }
 
 // ---------------------------------------------------------------- gather
@@ -185,6 +195,8 @@ __global__ void pack_ik_kernel(const typename cplx<real>::type *__restrict__ F, 
   typedef typename cplx<real>::vec4 V;
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= M) return;
+  F += (size_t)blockIdx.y * 3 * M;  // alpha batch (grid.y)
+  P += (size_t)blockIdx.y * NMESH * M;
   const typename cplx<real>::type f0 = F[t], f1 = F[M + t], f2 = F[2 * M + t];
   V v;
   v.x = f0.x;
@@ -212,8 +224,11 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_kernel(const double4 *_
                                                                  double *__restrict__ fk, int n) {
   typedef typename cplx<real>::type C;
   typedef typename cplx<real>::vec4 V;
-  const C *__restrict__ F = reinterpret_cast<const C *>(Fv);
-  const V *__restrict__ P = reinterpret_cast<const V *>(Fv);
+  // alpha batch (grid.y): the potential (ad) or packed fields (ik) and the
+  // forces of entry y
+  const C *__restrict__ F = reinterpret_cast<const C *>(Fv) + (size_t)blockIdx.y * M;
+  const V *__restrict__ P = reinterpret_cast<const V *>(Fv) + (size_t)blockIdx.y * NMESH * M;
+  fk += (size_t)blockIdx.y * 3 * (size_t)n;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
   const double4 r = sxyzq[p];
@@ -281,6 +296,9 @@ __global__ void self_force_kernel(const double *__restrict__ x, const double *__
                                   const double *__restrict__ z, const double *__restrict__ q, int n, double h,
                                   const double *__restrict__ b81, double *__restrict__ f) {
   __shared__ double b[81];
+  // alpha batch (grid.y): coefficients and forces of entry y
+  b81 += (size_t)blockIdx.y * 81;
+  f += (size_t)blockIdx.y * 3 * (size_t)n;
   if (threadIdx.x < 81) b[threadIdx.x] = b81[threadIdx.x];
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -408,40 +426,68 @@ int dispatch_scatter(Ctx *c) {
   return launch_scatter<real, CAO, 1>(c, tile + scatter_stage_bytes<real, CAO, 1>(), SR, SP);
 }
 
+// Gather launch for na batch entries (grid.y): fields / potential Fv of
+// entry y at the batch stride of the kernel, forces into fk + 3 n y.
 template <typename real, int CAO>
-int dispatch_gather(Ctx *c) {
-  typedef typename cplx<real>::type C;
+int dispatch_gather(Ctx *c, const void *Fv, double *fk, int na) {
   const double Hi = (double)c->mesh / c->L;
   const double shift = (double)((c->cao - 1) / 2);
   const double L3 = c->L * c->L * c->L;
   const double Leni = 1.0 / c->L;
-  const int blocks = (c->n + ASSIGN_THREADS - 1) / ASSIGN_THREADS;
+  const dim3 grid((c->n + ASSIGN_THREADS - 1) / ASSIGN_THREADS, na);
   const bool il = method_interlaced(c->method);
-  const void *F = method_ad(c->method) ? c->Q : c->P;
   mark(c, EV_K4);
   if (method_ad(c->method)) {
     // prefactor Mesh * Leni^3 (p3m-ad.c:202, p3m-ad-i.c:199, p3m-ad-real.c:110)
     const double pref = (double)c->mesh * Leni * Leni * Leni;
     if (il)
-      gather_kernel<real, CAO, 2, true><<<blocks, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, F, c->M, c->fk, c->n);
+      gather_kernel<real, CAO, 2, true><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
     else
-      gather_kernel<real, CAO, 1, true><<<blocks, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, F, c->M, c->fk, c->n);
+      gather_kernel<real, CAO, 1, true><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
   } else {
     // prefactor 1 / (2 L^3) (p3m-ik.c:242, p3m-ik-i.c:241, p3m-ik-real.c:144)
     const double pref = 1.0 / (2.0 * L3);
     if (il)
-      gather_kernel<real, CAO, 2, false><<<blocks, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, F, c->M, c->fk, c->n);
+      gather_kernel<real, CAO, 2, false><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
     else
-      gather_kernel<real, CAO, 1, false><<<blocks, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, F, c->M, c->fk, c->n);
+      gather_kernel<real, CAO, 1, false><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
   }
   c->launches++;
   mark(c, EV_K5);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
+}
+
+template <typename real>
+int gather_any(Ctx *c, const void *Fv, double *fk, int na) {
+  switch (c->cao) {
+    case 1: return dispatch_gather<real, 1>(c, Fv, fk, na);
+    case 2: return dispatch_gather<real, 2>(c, Fv, fk, na);
+    case 3: return dispatch_gather<real, 3>(c, Fv, fk, na);
+    case 4: return dispatch_gather<real, 4>(c, Fv, fk, na);
+    case 5: return dispatch_gather<real, 5>(c, Fv, fk, na);
+    case 6: return dispatch_gather<real, 6>(c, Fv, fk, na);
+    case 7: return dispatch_gather<real, 7>(c, Fv, fk, na);
+  }
+  return P3MG_ERR_CAO;
+}
+
+template <typename real>
+int scatter_any(Ctx *c) {
+  switch (c->cao) {
+    case 1: return dispatch_scatter<real, 1>(c);
+    case 2: return dispatch_scatter<real, 2>(c);
+    case 3: return dispatch_scatter<real, 3>(c);
+    case 4: return dispatch_scatter<real, 4>(c);
+    case 5: return dispatch_scatter<real, 5>(c);
+    case 6: return dispatch_scatter<real, 6>(c);
+    case 7: return dispatch_scatter<real, 7>(c);
+  }
+  return P3MG_ERR_CAO;
 }
 
 template <typename real>
@@ -452,23 +498,17 @@ int run_kspace(Ctx *c) {
   const unsigned mblocks = (unsigned)((M + threads - 1) / threads);
   // charge assignment (the brick binning ran in kspace_prepare)
   P3MG_CUDA_TRY(cudaMemsetAsync(c->Q, 0, M * sizeof(C), c->stream));
-  switch (c->cao) {
-    case 1: P3MG_TRY((dispatch_scatter<real, 1>(c))); break;
-    case 2: P3MG_TRY((dispatch_scatter<real, 2>(c))); break;
-    case 3: P3MG_TRY((dispatch_scatter<real, 3>(c))); break;
-    case 4: P3MG_TRY((dispatch_scatter<real, 4>(c))); break;
-    case 5: P3MG_TRY((dispatch_scatter<real, 5>(c))); break;
-    case 6: P3MG_TRY((dispatch_scatter<real, 6>(c))); break;
-    case 7: P3MG_TRY((dispatch_scatter<real, 7>(c))); break;
-  }
+  P3MG_TRY(scatter_any<real>(c));
   mark(c, EV_S2);
   // forward FFT, convolution, backward FFT(s)
   P3MG_TRY(fft3d(c, c->Q, 1, -1));
   if (method_ad(c->method)) {
     if (c->precision == P3MG_FP64)
-      conv_ad_kernel<real, double><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<C *>(c->Q), c->G, M);
+      conv_ad_kernel<real, double><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<C *>(c->Q), c->G, M,
+                                                                       reinterpret_cast<C *>(c->Q));
     else
-      conv_ad_kernel<real, float><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<C *>(c->Q), c->G32, M);
+      conv_ad_kernel<real, float><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<C *>(c->Q), c->G32, M,
+                                                                      reinterpret_cast<C *>(c->Q));
     c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
     P3MG_TRY(fft3d(c, c->Q, 1, +1));
@@ -495,15 +535,7 @@ int run_kspace(Ctx *c) {
   }
   mark(c, EV_S3);
   // back-interpolation
-  switch (c->cao) {
-    case 1: P3MG_TRY((dispatch_gather<real, 1>(c))); break;
-    case 2: P3MG_TRY((dispatch_gather<real, 2>(c))); break;
-    case 3: P3MG_TRY((dispatch_gather<real, 3>(c))); break;
-    case 4: P3MG_TRY((dispatch_gather<real, 4>(c))); break;
-    case 5: P3MG_TRY((dispatch_gather<real, 5>(c))); break;
-    case 6: P3MG_TRY((dispatch_gather<real, 6>(c))); break;
-    case 7: P3MG_TRY((dispatch_gather<real, 7>(c))); break;
-  }
+  P3MG_TRY(gather_any<real>(c, method_ad(c->method) ? c->Q : c->P, c->fk, 1));
   if (method_self_force(c->method)) {
     const int blocks = (c->n + threads - 1) / threads;
     self_force_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, c->L / c->mesh, c->self_b,
@@ -512,6 +544,58 @@ int run_kspace(Ctx *c) {
     P3MG_CUDA_TRY(cudaGetLastError());
   }
   mark(c, EV_S4);
+  return P3MG_OK;
+}
+
+// The alpha-dependent half of the k-space pass for b.na alphas at once
+// (the charge assignment and forward FFT do not depend on alpha and, with
+// b.forward, run once into Q): convolution with each alpha's G, the
+// backward FFTs of all na meshes in one batched transform, the gather and
+// the ad self-force correction, each one launch over grid.y = alpha.
+template <typename real>
+int run_kspace_batch(Ctx *c, const KspaceBatch &b) {
+  typedef typename cplx<real>::type C;
+  typedef typename cplx<real>::vec4 V;
+  typedef typename std::conditional<sizeof(real) == 8, double, float>::type Gt;
+  const size_t M = c->M;
+  const int threads = 256;
+  const int na = b.na;
+  const dim3 mgrid((unsigned)((M + threads - 1) / threads), na);
+  if (b.forward) {
+    P3MG_CUDA_TRY(cudaMemsetAsync(c->Q, 0, M * sizeof(C), c->stream));
+    P3MG_TRY(scatter_any<real>(c));
+    P3MG_TRY(fft3d(c, c->Q, 1, -1));
+  }
+  const Gt *G = reinterpret_cast<const Gt *>(b.G);
+  if (method_ad(c->method)) {
+    conv_ad_kernel<real, Gt><<<mgrid, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), G, M,
+                                                               reinterpret_cast<C *>(b.F));
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
+    P3MG_TRY(fft3d(c, b.F, na, +1));
+    P3MG_TRY(gather_any<real>(c, b.F, b.fk, na));
+  } else {
+    conv_ik_kernel<real, Gt><<<mgrid, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), G, c->mesh,
+                                                               2.0 * P3MG_PI / c->L, M, reinterpret_cast<C *>(b.F));
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
+    P3MG_TRY(fft3d(c, b.F, 3 * na, +1));
+    if (method_interlaced(c->method))
+      pack_ik_kernel<real, 2><<<mgrid, threads, 0, c->stream>>>(reinterpret_cast<const C *>(b.F), M,
+                                                                 reinterpret_cast<V *>(b.P));
+    else
+      pack_ik_kernel<real, 1><<<mgrid, threads, 0, c->stream>>>(reinterpret_cast<const C *>(b.F), M,
+                                                                 reinterpret_cast<V *>(b.P));
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
+    P3MG_TRY(gather_any<real>(c, b.P, b.fk, na));
+  }
+  if (method_self_force(c->method)) {
+    const dim3 pgrid((c->n + threads - 1) / threads, na);
+    self_force_kernel<<<pgrid, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, c->L / c->mesh, b.b81, b.f);
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
+  }
   return P3MG_OK;
 }
 

@@ -35,10 +35,14 @@ __device__ __forceinline__ double signed_freq(int i, int m) {
   return (double)i - round((double)i / (double)m) * (double)m;
 }
 
-__global__ void influence_kernel(double *__restrict__ G, int method, int m, int cao, int mc, double alpha, double L) {
+__global__ void influence_kernel(double *__restrict__ G, int method, int m, int cao, int mc, double alpha_v,
+                                 const double *__restrict__ alphas, double L) {
   const size_t M = (size_t)m * m * m;
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ind >= M) return;
+  // alpha batch: grid.y = alpha index (alphas on the device), G of entry y
+  const double alpha = alphas ? alphas[blockIdx.y] : alpha_v;
+  G += (size_t)blockIdx.y * M;
   const int NZ = (int)(ind % m);
   const int NY = (int)((ind / m) % m);
   const int NX = (int)(ind / ((size_t)m * m));
@@ -122,6 +126,8 @@ __global__ void self_force_sum_kernel(const double *__restrict__ G, int m, int c
   __shared__ double red[26][8];
   const size_t M = (size_t)m * m * m;
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  G += (size_t)blockIdx.y * M;  // alpha batch (grid.y)
+  S26 += 26 * blockIdx.y;
   double acc[26];
 #pragma unroll
   for (int t = 0; t < 26; t++) acc[t] = 0.0;
@@ -172,14 +178,59 @@ __global__ void self_force_sum_kernel(const double *__restrict__ G, int m, int c
   }
 }
 
+// b_d(m') = pi m'_d mesh / L^4 * S(m'), zero where m'_d == 0 or alpha == 0
+// (p3m-ad-self-forces.c:79-88, layout of Init_self_forces :98-106, and the
+// early return of the ad influence function at alpha == 0,
+// p3m-ad.c:120-123); one thread per coefficient, grid.y = alpha index.
+__global__ void self_coeff_kernel(const double *__restrict__ S26, const double *__restrict__ alphas, int m, double L,
+                                  double *__restrict__ b81) {
+  const int t = threadIdx.x;
+  if (t >= 81) return;
+  const int y = blockIdx.y;
+  const int ind = t / 3, d = t % 3;
+  const int a0 = ind / 9 - 1, a1 = (ind / 3) % 3 - 1, a2 = ind % 3 - 1;
+  const int mm[3] = {a0, a1, a2};
+  const bool zero = (a0 == 0 && a1 == 0 && a2 == 0);
+  const int slot = ind - (ind > 13 ? 1 : 0);  // the 26 sums skip m' = 0 (index 13)
+  const double L4 = (L * L) * (L * L);
+  double v = 0.0;
+  if (!zero && mm[d] != 0 && alphas[y] != 0.0) v = (P3MG_PI * mm[d] * m) / L4 * S26[26 * y + slot];
+  b81[81 * y + t] = v;
+}
+
 }  // namespace
+
+// G_opt (and for methods 2 and 7 the self-force coefficients) for na alphas
+// at once: G_all holds na meshes, b81_all 81 coefficients per alpha, S26
+// is 26 na doubles of scratch.  Same kernels and arithmetic as
+// influence_compute, so each alpha's G is the one a single call gives.
+int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, double *S26, double *b81_all) {
+  const int m = c->mesh;
+  const size_t M = c->M;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((M + threads - 1) / threads);
+  influence_kernel<<<dim3(blocks, na), threads, 0, c->stream>>>(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas,
+                                                                 c->L);
+  c->launches++;
+  P3MG_CUDA_TRY(cudaGetLastError());
+  if (method_self_force(c->method)) {
+    P3MG_CUDA_TRY(cudaMemsetAsync(S26, 0, 26 * (size_t)na * sizeof(double), c->stream));
+    self_force_sum_kernel<<<dim3(blocks, na), threads, 0, c->stream>>>(G_all, m, c->cao, S26);
+    self_coeff_kernel<<<dim3(1, na), 96, 0, c->stream>>>(S26, d_alphas, m, c->L, b81_all);
+    c->launches += 2;
+    P3MG_CUDA_TRY(cudaGetLastError());
+  } else {
+    P3MG_CUDA_TRY(cudaMemsetAsync(b81_all, 0, 81 * (size_t)na * sizeof(double), c->stream));
+  }
+  return P3MG_OK;
+}
 
 int influence_compute(Ctx *c, double alpha) {
   const int m = c->mesh;
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
-  influence_kernel<<<blocks, threads, 0, c->stream>>>(c->G, c->method, m, c->cao, c->mc, alpha, c->L);
+  influence_kernel<<<blocks, threads, 0, c->stream>>>(c->G, c->method, m, c->cao, c->mc, alpha, nullptr, c->L);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   if (c->precision != P3MG_FP64) {
@@ -212,9 +263,12 @@ int influence_compute(Ctx *c, double alpha) {
           if (!zero) t++;
         }
   }
-  P3MG_CUDA_TRY(cudaMemcpyAsync(c->self_b, c->self_b_host, 81 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->alpha = alpha;
+  P3MG_CUDA_TRY(cudaMemcpyAsync(c->self_b, c->self_b_host, 81 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // the step's kernels read alpha from the device, so a captured step stays
+  // valid when the influence function is recomputed for another alpha
+  P3MG_CUDA_TRY(cudaMemcpyAsync(c->d_alpha, &c->alpha, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->have_G = true;
   return P3MG_OK;
 }

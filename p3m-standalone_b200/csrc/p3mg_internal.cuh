@@ -108,6 +108,8 @@ struct Ctx {
   FftPlan plan;
 
   double alpha = 0.0;
+  double *d_alpha = nullptr;  // device: [0] alpha of G (read by the step's kernels), [1] scratch
+  double h_alpha_arg = 0.0;   // host source of the [1] upload
   bool have_G = false;
 
   // timing: CUDA events on the context stream (see EV_* below)
@@ -180,7 +182,30 @@ double ewald_error(int n, double q2, double L, double rcut, int kmax, double alp
 
 // real space (p3mg_pairs.cu)
 int pairs_reserve(Ctx *c, double rcut);
-int pairs_run(Ctx *c, double rcut, double alpha);
+int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr, double *energy);
+
+// Buffers of a batched k-space pass over na alphas (all on the device):
+// G (na meshes, FP64 or FP32 by precision), b81 (81 self-force
+// coefficients per alpha), mesh scratch for the na field meshes (ik: 3 na
+// complex meshes in F, na x (1 or 2) packed meshes in P; ad: na complex
+// meshes in F), and the outputs fk (gather) and f (self forces), 3 n per
+// alpha, both accumulated.
+struct KspaceBatch {
+  int na = 0;
+  const void *G = nullptr;
+  const double *b81 = nullptr;
+  void *F = nullptr;
+  void *P = nullptr;
+  double *fk = nullptr;
+  double *f = nullptr;
+  bool forward = true;  // run the scatter and forward FFT into Q first
+};
+int kspace_batch(Ctx *c, const KspaceBatch &b);
+int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, double *S26, double *b81_all);
+int g_to_f32_n(Ctx *c, const double *G, float *G32, size_t count);
+size_t sweep_bytes_per_alpha(const Ctx *c);
+int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
+              size_t budget);
 
 // misc kernels (p3mg_api.cu)
 int zero_forces(Ctx *c);

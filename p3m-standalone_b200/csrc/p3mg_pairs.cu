@@ -124,10 +124,16 @@ template <bool DBL>
 __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__restrict__ posv,
                                                                const int *__restrict__ sidx,
                                                                const int *__restrict__ start, int nc, double L,
-                                                               double rcut, double alpha,
+                                                               double rcut, double alpha_v,
+                                                               const double *__restrict__ alphas,
                                                                double *__restrict__ fr, int n,
                                                                double *__restrict__ energy) {
   typedef typename PairAcc<DBL>::type acc_t;
+  // alpha batch: grid.y = alpha index (alphas on the device), outputs per
+  // alpha at fr + 3 n y and energy + y; without alphas the scalar alpha_v
+  const double alpha = alphas ? alphas[blockIdx.y] : alpha_v;
+  fr += (size_t)blockIdx.y * 3 * (size_t)n;
+  energy += blockIdx.y;
   extern __shared__ __align__(16) unsigned char pair_smem[];
   float4 *cf = reinterpret_cast<float4 *>(pair_smem);
   int *csrc = reinterpret_cast<int *>(cf + PAIR_JCH);  // FP64: sorted slot of each staged candidate
@@ -390,7 +396,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
 
 // Launch the cell kernel (FP64 or FP32 positions, already half-cell sorted).
 int launch_pairs_cells(bool dbl, const void *pos, const int *sidx, const int *start, int nc, double L, double rcut,
-                       double alpha, double *fr, int n, double *energy, cudaStream_t s) {
+                       double alpha, const double *alphas, int nalpha, double *fr, int n, double *energy,
+                       cudaStream_t s) {
   static bool attr_set[2] = {false, false};
   const size_t smem = pair_smem_bytes(dbl);
   if (!attr_set[dbl]) {
@@ -400,11 +407,11 @@ int launch_pairs_cells(bool dbl, const void *pos, const int *sidx, const int *st
       P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set[dbl] = true;
   }
-  const int ncell = nc * nc * nc;
+  const dim3 grid(nc * nc * nc, nalpha);
   if (dbl)
-    pairs_cell_kernel<true><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, fr, n, energy);
+    pairs_cell_kernel<true><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, fr, n, energy);
   else
-    pairs_cell_kernel<false><<<ncell, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, fr, n, energy);
+    pairs_cell_kernel<false><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, fr, n, energy);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -415,8 +422,14 @@ __global__ void __launch_bounds__(BRUTE_THREADS) pairs_brute_kernel(const double
                                                                      const double *__restrict__ y,
                                                                      const double *__restrict__ z,
                                                                      const double *__restrict__ q, int n, double L,
-                                                                     double rcut, double alpha, double *__restrict__ fr,
+                                                                     double rcut, double alpha_v,
+                                                                     const double *__restrict__ alphas,
+                                                                     double *__restrict__ fr,
                                                                      double *__restrict__ energy) {
+  // alpha batch as in pairs_cell_kernel
+  const double alpha = alphas ? alphas[blockIdx.y] : alpha_v;
+  fr += (size_t)blockIdx.y * 3 * (size_t)n;
+  energy += blockIdx.y;
   __shared__ double4 sj[BRUTE_THREADS];
   __shared__ double ered[BRUTE_THREADS / 32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -496,7 +509,9 @@ int pairs_reserve(Ctx *c, double rcut) {
   return P3MG_OK;
 }
 
-int pairs_run(Ctx *c, double rcut, double alpha) {
+// Real-space forces of the context's particles for nalpha alphas (device
+// array) into fr + 3 n k and energy + k, k = 0 .. nalpha-1 (accumulated).
+int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr, double *energy) {
   const int n = c->n;
   if (n == 0 || rcut <= 0.0) return P3MG_OK;
   const int nc = cells_per_side(c->L, rcut);
@@ -504,8 +519,8 @@ int pairs_run(Ctx *c, double rcut, double alpha) {
   const int blocks = (n + threads - 1) / threads;
   if (nc < 3) {
     mark(c, EV_K0);
-    pairs_brute_kernel<<<blocks, BRUTE_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, rcut, alpha, c->fr,
-                                                                 c->energy);
+    pairs_brute_kernel<<<dim3(blocks, nalpha), BRUTE_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, rcut,
+                                                                               0.0, alphas, fr, energy);
     c->launches++;
     mark(c, EV_K1);
     P3MG_CUDA_TRY(cudaGetLastError());
@@ -531,8 +546,8 @@ int pairs_run(Ctx *c, double rcut, double alpha) {
                                                                   reinterpret_cast<float4 *>(c->cell_pos));
   P3MG_CUDA_TRY(cudaGetLastError());
   mark(c, EV_K0);
-  P3MG_TRY(launch_pairs_cells(dbl, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut, alpha, c->fr, n,
-                              c->energy, c->stream));
+  P3MG_TRY(launch_pairs_cells(dbl, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut, 0.0, alphas, nalpha, fr,
+                              n, energy, c->stream));
   c->launches += 2;
   mark(c, EV_K1);
   return P3MG_OK;
@@ -617,7 +632,7 @@ extern "C" int p3mg_real_forces_noalloc(int n, const double *x, const double *y,
   const int blocks = (n + threads - 1) / threads;
   int nc = cells_per_side(L, rcut);
   if (nc < 3) {
-    pairs_brute_kernel<<<blocks, BRUTE_THREADS, 0, s>>>(x, y, z, q, n, L, rcut, alpha, fr, energy);
+    pairs_brute_kernel<<<blocks, BRUTE_THREADS, 0, s>>>(x, y, z, q, n, L, rcut, alpha, nullptr, fr, energy);
     P3MG_CUDA_TRY(cudaGetLastError());
     return P3MG_OK;
   }
@@ -639,12 +654,12 @@ extern "C" int p3mg_real_forces_noalloc(int n, const double *x, const double *y,
     place_cells_kernel<double4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
                                                            reinterpret_cast<double4 *>(pos));
     P3MG_CUDA_TRY(cudaGetLastError());
-    P3MG_TRY(launch_pairs_cells(true, pos, idx, start, nc, L, rcut, alpha, fr, n, energy, s));
+    P3MG_TRY(launch_pairs_cells(true, pos, idx, start, nc, L, rcut, alpha, nullptr, 1, fr, n, energy, s));
   } else {
     place_cells_kernel<float4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
                                                           reinterpret_cast<float4 *>(pos));
     P3MG_CUDA_TRY(cudaGetLastError());
-    P3MG_TRY(launch_pairs_cells(false, pos, idx, start, nc, L, rcut, alpha, fr, n, energy, s));
+    P3MG_TRY(launch_pairs_cells(false, pos, idx, start, nc, L, rcut, alpha, nullptr, 1, fr, n, energy, s));
   }
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;

@@ -11,7 +11,10 @@
  * on the GPU, or a forces file), and the analytic estimates.
  *
  * Additions: "fp32" runs the FP32-mixed pipeline instead of FP64; "alpha"
- * alone runs that single alpha.  Parameters the reference parses for its
+ * alone runs that single alpha; "batched" computes the whole alpha range
+ * in one batched GPU pass (p3mg_sweep) and reports its time divided evenly
+ * over the alphas (not with error_k, which needs each alpha's k-space
+ * forces).  Parameters the reference parses for its
  * analysis side paths (rdf, rdf_species, cdf, tune, inhomo_error,
  * error_map) are accepted and reported as not provided here. */
 #include <math.h>
@@ -123,6 +126,7 @@ int main(int argc, char **argv) {
   add_param("error_map_mesh", ARG_TYPE_INT, ARG_OPTIONAL, &error_map_mesh, &params);
   add_param("error_map_cao", ARG_TYPE_INT, ARG_OPTIONAL, &error_map_cao, &params);
   add_param("fp32", ARG_TYPE_NONE, ARG_OPTIONAL, NULL, &params);
+  add_param("batched", ARG_TYPE_NONE, ARG_OPTIONAL, NULL, &params);
 
   parse_parameters(argc - 1, argv + 1, &params);
 
@@ -229,12 +233,39 @@ int main(int argc, char **argv) {
 
   const size_t n = (size_t)system->nparticles;
   double walltime = 0.0, estimate = 0.0, error_k_est = 0.0;
+
+  /* batched sweep: every alpha's RMS error from one p3mg_sweep call */
+  double *batch_rms = NULL, batch_time = 0.0;
+  const int batched = param_isset("batched", &params) && !calc_k_error && !param_isset("no_calculation", &params);
+  if (param_isset("batched", &params) && !batched)
+    fprintf(stderr, "Note: 'batched' is not combined with error_k or no_calculation; running alpha by alpha.\n");
+  if (batched) {
+    const int na = p3mg_alpha_range(alphamin, alphamax, alphastep, 0, NULL);
+    if (na < 0) p3m_host_die(na, "p3mg_alpha_range");
+    double *al = (double *)malloc((size_t)(na > 0 ? na : 1) * sizeof(double));
+    batch_rms = (double *)calloc((size_t)(na > 0 ? na : 1), sizeof(double));
+    if (!al || !batch_rms) {
+      fputs("out of memory\n", stderr);
+      exit(1);
+    }
+    p3mg_alpha_range(alphamin, alphamax, alphastep, na, al);
+    const forces_t *r = system->reference;
+    batch_time = wtime();
+    const int st = p3mg_sweep(data->ctx, parameters.rcut, na, al, r->f->x, r->f->y, r->f->z, batch_rms, NULL, 0);
+    batch_time = wtime() - batch_time;
+    if (st != P3MG_OK) p3m_host_die(st, "p3mg_sweep");
+    if (na > 0) batch_time /= na;
+    free(al);
+  }
+  int ia = 0;
   printf("# %8s\t%8s\t%8s\t%8s\t%8s\n", "alpha", "DeltaF", "Estimate", "R-Error-Est",
          "K-Error-Est Generic-K-Space-err");
-  for (parameters.alpha = alphamin; parameters.alpha <= alphamax; parameters.alpha += alphastep) {
-    method->Influence_function(system, &parameters, data);
+  for (parameters.alpha = alphamin; parameters.alpha <= alphamax; parameters.alpha += alphastep, ia++) {
+    if (!batched) method->Influence_function(system, &parameters, data);
 
-    if (!param_isset("no_calculation", &params)) {
+    if (batched) {
+      walltime = batch_time;
+    } else if (!param_isset("no_calculation", &params)) {
       walltime = wtime();
       Calculate_forces(method, system, &parameters, data, forces);
       walltime = wtime() - walltime;
@@ -255,12 +286,16 @@ int main(int argc, char **argv) {
 
     const double ewald_error_k_est = ewald_error_k_estimate(system, &parameters, parameters.alpha);
     double ef = 0.0;
-    for (size_t i = 0; i < n; i++)
-      for (int j = 0; j < 3; j++) {
-        const double dv = forces->f->fields[j][i] - system->reference->f->fields[j][i];
-        ef += dv * dv;
-      }
-    ef = sqrt(ef);
+    if (batched) {
+      ef = batch_rms[ia] * sqrt((double)n);
+    } else {
+      for (size_t i = 0; i < n; i++)
+        for (int j = 0; j < 3; j++) {
+          const double dv = forces->f->fields[j][i] - system->reference->f->fields[j][i];
+          ef += dv * dv;
+        }
+      ef = sqrt(ef);
+    }
 
     if (calc_est) {
       estimate = method->Error(system, &parameters);
@@ -277,6 +312,7 @@ int main(int argc, char **argv) {
     fflush(fout);
   }
   fclose(fout);
+  free(batch_rms);
 
   Free_data(data);
   Free_forces(forces);

@@ -94,6 +94,8 @@ def load():
         ctypes.POINTER(ctypes.c_int), _dp]
     L.p3mg_ewald_kspace_forces.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]
+    L.p3mg_alpha_range.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, _dp]
+    L.p3mg_sweep.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
     L.p3mg_estimate_errors.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 4 + [_dp]
     L.p3mg_error_estimate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
     L.p3mg_kernel_times.argtypes = [vp, _dp]
@@ -263,6 +265,22 @@ class Context:
                                                   _p(fk[2])), "p3mg_ewald_kspace_forces")
         return fk
 
+    def sweep(self, rcut, alphas, ref=None, want_forces=False, max_batch=0):
+        """Batched alpha sweep (p3mg_sweep): dict rms (per alpha, when ref (3, n)
+        is given) and forces (nalpha, 3, n) when want_forces."""
+        al = np.ascontiguousarray(alphas, dtype=np.float64)
+        na = len(al)
+        rms = np.zeros(na) if ref is not None else None
+        f = np.zeros((na, 3, self.n)) if want_forces else None
+        if ref is not None:
+            r = np.ascontiguousarray(ref, dtype=np.float64).reshape(3, self.n)
+            rx, ry, rz = (np.ascontiguousarray(r[d]) for d in range(3))
+        else:
+            rx = ry = rz = None
+        _check(self._lib.p3mg_sweep(self._h, float(rcut), na, _p(al), _p(rx), _p(ry), _p(rz), _p(rms), _p(f),
+                                    int(max_batch)), "p3mg_sweep")
+        return dict(rms=rms, forces=f)
+
     def error_estimate(self, alpha, rcut, mc_est=1):
         """Analytic RMS error estimates (method.Error / Error_k, Realspace_error):
         dict total, kspace, realspace."""
@@ -332,6 +350,17 @@ class Method:
     @staticmethod
     def Kspace_force(ctx, forces):
         ctx.kspace_forces(forces["f_k"], forces["f"])
+
+
+def alpha_range(alphamin, alphamax, alphastep):
+    """The reference sweep's alphas (p3mg_alpha_range, main.c:375)."""
+    L = load()
+    k = L.p3mg_alpha_range(float(alphamin), float(alphamax), float(alphastep), 0, None)
+    if k < 0:
+        raise P3MGError(k, "p3mg_alpha_range")
+    out = np.zeros(k)
+    L.p3mg_alpha_range(float(alphamin), float(alphamax), float(alphastep), k, _p(out))
+    return out
 
 
 def estimate_errors(method, mesh, cao, n, q2, L, alpha, rcut, mc_est=1):

@@ -91,3 +91,17 @@ def test_fp32_flag_runs_mixed_pipeline(gpu, tmp_path):
     for i in range(ref.shape[0]):
         if ref[i, 1] > 1e-3:
             assert abs(our[i, 1] - ref[i, 1]) <= 0.1 * ref[i, 1]
+
+
+@pytest.mark.parametrize("name", ["m3_type1", "m6_type4", "m2_type2"])
+def test_batched_sweep_matches_reference_program(gpu, tmp_path, name):
+    case = os.path.join(ROOT, "tests", "golden", "cli", name + ".dat")
+    args = open(case).readline()[1:].split()
+    r = subprocess.run([EXE] + args + ["batched", "outfile", "out.dat"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    ref_alpha, ref = read_table(case)
+    our_alpha, our = read_table(str(tmp_path / "out.dat"))
+    assert our_alpha == ref_alpha
+    for i in range(ref.shape[0]):
+        assert close(our[i, 1], ref[i, 1], 1e-5), (i, our[i], ref[i])

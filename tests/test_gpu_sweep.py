@@ -1,0 +1,78 @@
+"""Batched alpha sweep (p3mg_sweep) against single-alpha evaluations, the
+reference's own sweep forces (golden sweep.npz: method 7, 1000 particles,
+mesh 16, cao 7, mc 2, rcut 3, alphas of 0.1..2.5 step 0.05) and its RMS
+errors against the reference's Ewald forces."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import p3mg
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_alpha_range_matches_reference_loop():
+    a = p3mg.alpha_range(0.1, 2.5, 0.05)
+    assert len(a) == 49 and a[-1] == 2.4999999999999991
+    ref = []
+    x = 0.1
+    while x <= 2.5:
+        ref.append(x)
+        x += 0.05
+    assert np.array_equal(a, np.array(ref))
+
+
+@pytest.mark.parametrize("method", [0, 1, 2, 3, 6, 7])
+@pytest.mark.parametrize("precision", [p3mg.FP64, p3mg.FP32_MIXED])
+def test_sweep_equals_single_alpha_steps(gpu, method, precision):
+    x, y, z, q = p3mg.generate_system(0, 400, 9.0, seed=51)
+    alphas = np.array([0.6, 0.85, 1.1, 1.35, 1.6])
+    with p3mg.Context(method, 16, 5, 1, precision) as ctx:
+        ctx.set_system(x, y, z, q, 9.0)
+        singles = []
+        for a in alphas:
+            ctx.influence(a)
+            singles.append(ctx.calculate_forces(2.8)["f"].copy())
+        for mb in (0, 2):  # one pass, and passes of two alphas
+            sw = ctx.sweep(2.8, alphas, want_forces=True, max_batch=mb)["forces"]
+            for k in range(len(alphas)):
+                tol = 1e-13 if precision == p3mg.FP64 else 1e-6
+                assert O.rel_rms(sw[k].ravel(), singles[k].ravel()) <= tol, (mb, k)
+
+
+def test_sweep_golden_method7_config(gpu):
+    g = np.load(os.path.join(GOLD, "sweep.npz"))
+    x, y, z, q, L = g["x"], g["y"], g["z"], g["q"], float(g["L"])
+    alphas = p3mg.alpha_range(0.1, 2.5, 0.05)
+    assert len(alphas) == int(g["n_alphas"])
+    ref = np.asarray(g["ewald_f"]).reshape(3, len(x))
+    with p3mg.Context(7, 16, 7, 2) as ctx:
+        ctx.set_system(x, y, z, q, L)
+        r = ctx.sweep(3.0, alphas, ref=ref, want_forces=True)
+    for j, k in enumerate((0, 24, 48)):
+        assert alphas[k] == g["alphas"][j]
+        assert O.rel_rms(r["forces"][k].ravel(), np.asarray(g["f_%d" % j]).ravel()) <= 1e-10
+    # RMS error column of the reference's out.dat: sqrt(sum |f - f_ewald|^2) / sqrt(N)
+    for k in range(len(alphas)):
+        want = np.sqrt(np.sum((r["forces"][k] - ref) ** 2)) / np.sqrt(len(x))
+        assert abs(r["rms"][k] - want) <= 1e-12 * want
+
+
+def test_graph_replay_follows_alpha_changes(gpu):
+    # a captured step reads alpha from the device, so recomputing G for a new
+    # alpha between replays gives that alpha's real-space forces too
+    x, y, z, q = p3mg.generate_system(0, 500, 10.0, seed=52)
+    with p3mg.Context(1, 16, 5, 1) as ref_ctx, p3mg.Context(1, 16, 5, 1) as ctx:
+        ref_ctx.set_system(x, y, z, q, 10.0)
+        ctx.set_system(x, y, z, q, 10.0)
+        ctx.set_graph(True)
+        for a in (0.7, 0.9, 1.1, 1.3):
+            ctx.influence(a)
+            got = ctx.calculate_forces(3.0)
+            ref_ctx.influence(a)
+            want = ref_ctx.calculate_forces(3.0)
+            assert O.rel_rms(got["f"].ravel(), want["f"].ravel()) <= 1e-14
+            assert O.rel_rms(got["f_r"].ravel(), want["f_r"].ravel()) <= 1e-14
