@@ -171,6 +171,31 @@ int p3mg_alpha_range(double alphamin, double alphamax, double alphastep, int cap
 int p3mg_sweep(p3mg_ctx *ctx, double rcut, int nalpha, const double *alphas, const double *ref_x,
                const double *ref_y, const double *ref_z, double *rms_out, double *f_out, int max_batch);
 
+/* Electrostatic energy of the P3M approximation (no counterpart in the
+ * reference, which computes no P3M energy): parts = {total, k space, real
+ * space, self, neutralising}, with
+ *   E_k    = c/(2 L^3 nmesh) sum_k G(k) |Q^(k)|^2 over the method's mesh(es)
+ *            (charge assignment with the exact B-spline offsets, G = the
+ *            context's G_opt at its alpha; nmesh = 2 for interlaced methods;
+ *            c = 1 for ad and 1/2 for ik influence functions, matching the
+ *            normalisation of their forces),
+ *   E_r    = 1/2 sum_{i != j, r <= rcut} q_i q_j erfc(alpha r)/r,
+ *   E_self = -alpha/sqrt(pi) sum q^2 (as ewald.c:60-62),
+ *   E_neut = -pi Q^2/(2 alpha^2 L^3) for net charge Q.
+ * Needs p3mg_influence first (alpha > 0). */
+int p3mg_energy(p3mg_ctx *ctx, double rcut, double parts[5]);
+
+/* Adjoint of p3mg_energy (no counterpart in the reference): grad_E times
+ * dE/dx, dE/dy, dE/dz and dE/dq (host arrays of n, each may be NULL; x, y, z
+ * all or none), dE/dalpha and dE/dL (box length at fixed fractional
+ * coordinates; -L dE/dL is the isotropic virial) in grad_alpha / grad_L
+ * (may be NULL), and the energy parts (may be NULL).  dE/dx is minus the
+ * exact force of this energy: for ad methods the ad force without the
+ * self-force correction, for ik methods the gradient of E, which differs
+ * from the ik force by its discretisation error. */
+int p3mg_backward(p3mg_ctx *ctx, double rcut, double grad_E, double *grad_x, double *grad_y, double *grad_z,
+                  double *grad_q, double *grad_alpha, double *grad_L, double parts[5]);
+
 /* FP64 Ewald reference forces for the context's particles, evaluated on nt
  * target particles (targets: host array of particle indices, or NULL with
  * nt == n for all), written (not accumulated) to the host arrays f_x/f_y/f_z

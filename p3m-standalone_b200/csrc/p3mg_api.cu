@@ -123,6 +123,15 @@ int free_all(Ctx *c) {
   dfree(c->self_b);
   dfree(c->scan_tmp);
   dfree(c->scatter_tab);
+  if (c->sweep_ws) cudaFree(c->sweep_ws);
+  c->sweep_ws = nullptr;
+  c->sweep_cap = 0;
+  dfree(c->adj_G);
+  dfree(c->adj_dG);
+  dfree(c->adj_sums);
+  dfree(c->adj_grad);
+  dfree(c->adj_phi);
+  c->adj_cap = 0;
   fft_plan_free(c);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   c->gexec = nullptr;
@@ -618,6 +627,45 @@ extern "C" int p3mg_sweep(p3mg_ctx *h, double rcut, int nalpha, const double *al
     if (b < budget) budget = b;
   }
   return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref.data() : nullptr, rms_out, f_out, budget);
+}
+
+extern "C" int p3mg_backward(p3mg_ctx *h, double rcut, double grad_E, double *grad_x, double *grad_y,
+                             double *grad_z, double *grad_q, double *grad_alpha, double *grad_L, double parts[5]) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!c->have_G) return P3MG_ERR_STATE;
+  if (!(c->alpha > 0.0) || !(rcut >= 0.0) || !isfinite(grad_E)) return P3MG_ERR_ARG;
+  const bool want_x = grad_x || grad_y || grad_z;
+  if (want_x && !(grad_x && grad_y && grad_z)) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->n;
+  if (!c->adj_grad || c->adj_cap < c->n) {
+    if (c->adj_grad) cudaFree(c->adj_grad);
+    c->adj_grad = nullptr;
+    c->adj_cap = 0;
+    P3MG_CUDA_TRY(cudaMalloc(&c->adj_grad, 4 * (n > 0 ? n : 1) * sizeof(double)));
+    c->adj_cap = c->n;
+  }
+  double *gx = c->adj_grad, *gq = c->adj_grad + 3 * n;
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->adj_grad, 0, 4 * n * sizeof(double), c->stream));
+  double e5[5], da = 0.0, dl = 0.0;
+  P3MG_TRY(adjoint(c, rcut, grad_E, gx, gq, e5, &da, &dl));
+  if (parts)
+    for (int k = 0; k < 5; k++) parts[k] = e5[k];
+  if (grad_alpha) *grad_alpha = da;
+  if (grad_L) *grad_L = dl;
+  double *dst[4] = {grad_x, grad_y, grad_z, grad_q};
+  for (int k = 0; k < 4; k++)
+    if (dst[k] && n) P3MG_CUDA_TRY(cudaMemcpyAsync(dst[k], c->adj_grad + k * n, n * sizeof(double),
+                                                   cudaMemcpyDeviceToHost, c->stream));
+  P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return P3MG_OK;
+}
+
+extern "C" int p3mg_energy(p3mg_ctx *h, double rcut, double parts[5]) {
+  if (!parts) return P3MG_ERR_ARG;
+  return p3mg_backward(h, rcut, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, parts);
 }
 
 // Shared body of the Ewald entries: checks the targets, uploads them, runs

@@ -35,8 +35,10 @@ __device__ __forceinline__ double signed_freq(int i, int m) {
   return (double)i - round((double)i / (double)m) * (double)m;
 }
 
+// dG (may be NULL): dG/dalpha as well (each exp(-(pi/alpha)^2 |n|^2)
+// factor differentiated; the rest of the formula is linear in those sums).
 __global__ void influence_kernel(double *__restrict__ G, int method, int m, int cao, int mc, double alpha_v,
-                                 const double *__restrict__ alphas, double L) {
+                                 const double *__restrict__ alphas, double L, double *__restrict__ dG = nullptr) {
   const size_t M = (size_t)m * m * m;
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ind >= M) return;
@@ -49,15 +51,18 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
   const int half = m / 2;
   if ((NX | NY | NZ) == 0) {
     G[ind] = 0.0;
+    if (dG) dG[ind] = 0.0;
     return;
   }
   const bool ad = method_ad(method);
   if (ad && alpha == 0.0) {
     G[ind] = 0.0;
+    if (dG) dG[ind] = 0.0;
     return;
   }
   if (!ad && (NX % half == 0) && (NY % half == 0) && (NZ % half == 0)) {
     G[ind] = 0.0;
+    if (dG) dG[ind] = 0.0;
     return;
   }
   const double Leni = 1.0 / L, fak1 = 1.0 / (double)m;
@@ -65,6 +70,8 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
   const double fak2 = pa * pa;
   const double nx = signed_freq(NX, m), ny = signed_freq(NY, m), nz = signed_freq(NZ, m);
   double Zx = 0.0, Zy = 0.0, Zz = 0.0, Z = 0.0, N1 = 0.0, N2 = 0.0, N3 = 0.0, N4 = 0.0;
+  double dZx = 0.0, dZy = 0.0, dZz = 0.0, dZ = 0.0;
+  const double dfac = 2.0 * fak2 / alpha;  // d/dalpha of -fak2 NM2 is dfac NM2
   for (int MX = -mc; MX <= mc; MX++) {
     const double NMX = nx + (double)(m * MX);
     const double sx = sinc_pi(fak1 * NMX);
@@ -80,6 +87,7 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
         const double a = NMX * Leni, b = NMY * Leni, cc = NMZ * Leni;
         const double NM2 = a * a + b * b + cc * cc;
         const double TE = exp(-fak2 * NM2);
+        const double dTE = dG ? TE * NM2 * dfac : 0.0;
         const bool even = ((MX + MY + MZ) % 2) == 0;
         N1 += S3;
         if (ad) {
@@ -87,33 +95,48 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
           N3 += even ? S3 : -S3;
           N4 += even ? S3 * NM2 : -(S3 * NM2);
           Z += S3 * TE;
+          dZ += S3 * dTE;
         } else {
           const double zwi = S3 * TE / NM2;
           Zx += NMX * zwi * Leni;
           Zy += NMY * zwi * Leni;
           Zz += NMZ * zwi * Leni;
+          if (dG) {
+            const double dzwi = S3 * dTE / NM2;
+            dZx += NMX * dzwi * Leni;
+            dZy += NMY * dzwi * Leni;
+            dZz += NMZ * dzwi * Leni;
+          }
           N2 += even ? S3 : -S3;
         }
       }
     }
   }
-  double g;
+  double g, dg = 0.0;
   if (ad) {
-    g = (method == 3) ? Z / (0.5 * P3MG_PI * (N1 * N2 + N3 * N4)) : Z / (P3MG_PI * N1 * N2);
+    const double den = (method == 3) ? (0.5 * P3MG_PI * (N1 * N2 + N3 * N4)) : (P3MG_PI * N1 * N2);
+    g = Z / den;
+    if (dG) dg = dZ / den;
   } else {
     const double Dx = (NX == half) ? 0.0 : nx, Dy = (NY == half) ? 0.0 : ny, Dz = (NZ == half) ? 0.0 : nz;
     double num = Dx * Zx * Leni + Dy * Zy * Leni + Dz * Zz * Leni;
+    double dnum = Dx * dZx * Leni + Dy * dZy * Leni + Dz * dZz * Leni;
     const double dxl = Dx * Leni, dyl = Dy * Leni, dzl = Dz * Leni;
     const double d2 = dxl * dxl + dyl * dyl + dzl * dzl;
     if (method == 1) {
       num /= d2;
       num /= 0.5 * (N1 * N1 + N2 * N2);
+      dnum /= d2;
+      dnum /= 0.5 * (N1 * N1 + N2 * N2);
     } else {
       num /= d2 * (N1 * N1);
+      dnum /= d2 * (N1 * N1);
     }
     g = 2.0 * num / P3MG_PI;
+    dg = 2.0 * dnum / P3MG_PI;
   }
   G[ind] = g;
+  if (dG) dG[ind] = dg;
 }
 
 // ad self-force sums S(m') for the 26 non-zero m' in {-1,0,1}^3
@@ -222,6 +245,18 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
   } else {
     P3MG_CUDA_TRY(cudaMemsetAsync(b81_all, 0, 81 * (size_t)na * sizeof(double), c->stream));
   }
+  return P3MG_OK;
+}
+
+// G and dG/dalpha at the context's alpha into G_out / dG_out (M doubles each).
+int influence_with_derivative(Ctx *c, double *G_out, double *dG_out) {
+  const size_t M = c->M;
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((M + threads - 1) / threads);
+  influence_kernel<<<blocks, threads, 0, c->stream>>>(G_out, c->method, c->mesh, c->cao, c->mc, c->alpha, nullptr,
+                                                       c->L, dG_out);
+  c->launches++;
+  P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
 

@@ -133,6 +133,13 @@ struct Ctx {
   // scratch for a single-CTA scan
   int *scan_tmp = nullptr;
   int scan_cap = 0;           // ints in scan_tmp
+  void *sweep_ws = nullptr;  // workspace of p3mg_sweep, kept between calls
+  // energy / adjoint buffers (allocated on first use): G and dG/dalpha at
+  // alpha, the potential mesh, 8 reduction slots, the gradients (3 n + n)
+  double *adj_G = nullptr, *adj_dG = nullptr, *adj_sums = nullptr, *adj_grad = nullptr;
+  void *adj_phi = nullptr;
+  int adj_cap = 0;
+  size_t sweep_cap = 0;
 };
 
 // event slots: stage markers and kernel brackets
@@ -183,6 +190,9 @@ double ewald_error(int n, double q2, double L, double rcut, int kmax, double alp
 // real space (p3mg_pairs.cu)
 int pairs_reserve(Ctx *c, double rcut);
 int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr, double *energy);
+int pairs_bin(Ctx *c, double rcut, int *nc_out);
+int influence_with_derivative(Ctx *c, double *G_out, double *dG_out);
+int adjoint(Ctx *c, double rcut, double ge, double *gx, double *gq, double energy[5], double *dalpha, double *dL);
 
 // Buffers of a batched k-space pass over na alphas (all on the device):
 // G (na meshes, FP64 or FP32 by precision), b81 (81 self-force
@@ -249,9 +259,10 @@ __device__ inline void mesh_geometry(double xc, double Hi, double shift, int ii,
 // (de Boor; Essmann et al. 1995) and dw[j] = M_{CAO-1}(u+k) - M_{CAO-1}(u+k-1),
 // k = CAO-1-j.  These are the charge-assignment polynomials of
 // window-functions.c:46-183.
+// The same weights at an arbitrary offset u = x + 1/2 in [0, 1) (used
+// where the weights must be smooth functions of the position).
 template <typename real, int CAO, bool DERIV>
-__device__ __forceinline__ void bspline_weights(int arg, real *w, real *dw) {
-  const real u = (real)(arg - P3MG_NINTERP / 2) * (real)(1.0 / P3MG_NINTERP) + (real)0.5;
+__device__ __forceinline__ void bspline_weights_u(real u, real *w, real *dw) {
   real a[CAO];
   real prev[CAO];
   a[0] = (real)1;
@@ -282,6 +293,22 @@ __device__ __forceinline__ void bspline_weights(int arg, real *w, real *dw) {
         dw[j] = prev[k] - (k > 0 ? prev[k - 1] : (real)0);
     }
   }
+}
+
+template <typename real, int CAO, bool DERIV>
+__device__ __forceinline__ void bspline_weights(int arg, real *w, real *dw) {
+  const real u = (real)(arg - P3MG_NINTERP / 2) * (real)(1.0 / P3MG_NINTERP) + (real)0.5;
+  bspline_weights_u<real, CAO, DERIV>(u, w, dw);
+}
+
+// Stencil base and exact in-cell offset u in [0, 1) of a coordinate (the
+// geometry of mesh_geometry without the 2^-17 quantisation of the offset).
+__device__ inline void mesh_geometry_exact(double xc, double Hi, double shift, int ii, int m, int *base, double *u) {
+  double pos = xc * Hi - shift;
+  if (ii) pos += 0.5;
+  const double nf = floor(pos + 0.5);
+  *u = pos - nf + 0.5;
+  *base = wrap_full((int)nf, m);
 }
 
 }  // namespace p3mg

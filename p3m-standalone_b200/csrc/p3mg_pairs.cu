@@ -509,23 +509,16 @@ int pairs_reserve(Ctx *c, double rcut) {
   return P3MG_OK;
 }
 
-// Real-space forces of the context's particles for nalpha alphas (device
-// array) into fr + 3 n k and energy + k, k = 0 .. nalpha-1 (accumulated).
-int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr, double *energy) {
+// Bin the context's particles into the half-cell list of this rcut; sets
+// *nc_out to the cells per side (0: fewer than 3, nothing binned).
+int pairs_bin(Ctx *c, double rcut, int *nc_out) {
   const int n = c->n;
+  *nc_out = 0;
   if (n == 0 || rcut <= 0.0) return P3MG_OK;
   const int nc = cells_per_side(c->L, rcut);
+  if (nc < 3) return P3MG_OK;
   const int threads = 256;
   const int blocks = (n + threads - 1) / threads;
-  if (nc < 3) {
-    mark(c, EV_K0);
-    pairs_brute_kernel<<<dim3(blocks, nalpha), BRUTE_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, rcut,
-                                                                               0.0, alphas, fr, energy);
-    c->launches++;
-    mark(c, EV_K1);
-    P3MG_CUDA_TRY(cudaGetLastError());
-    return P3MG_OK;
-  }
   const int nkey = 8 * nc * nc * nc;
   P3MG_TRY(pairs_reserve(c, rcut));
   c->ncell1 = nc;
@@ -535,8 +528,7 @@ int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr,
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   P3MG_TRY(exclusive_scan(c, c->cell_count, c->cell_start, nkey));
-  const bool dbl = (c->precision == P3MG_FP64);
-  if (dbl)
+  if (c->precision == P3MG_FP64)
     place_cells_kernel<double4><<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, nc, c->cell_key,
                                                                    c->cell_start, c->cell_fill, c->cell_idx,
                                                                    reinterpret_cast<double4 *>(c->cell_pos));
@@ -544,11 +536,34 @@ int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr,
     place_cells_kernel<float4><<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, nc, c->cell_key,
                                                                   c->cell_start, c->cell_fill, c->cell_idx,
                                                                   reinterpret_cast<float4 *>(c->cell_pos));
+  c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
+  *nc_out = nc;
+  return P3MG_OK;
+}
+
+// Real-space forces of the context's particles for nalpha alphas (device
+// array) into fr + 3 n k and energy + k, k = 0 .. nalpha-1 (accumulated).
+int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr, double *energy) {
+  const int n = c->n;
+  if (n == 0 || rcut <= 0.0) return P3MG_OK;
+  int nc = 0;
+  if (cells_per_side(c->L, rcut) < 3) {
+    const int threads = 256;
+    const int blocks = (n + threads - 1) / threads;
+    mark(c, EV_K0);
+    pairs_brute_kernel<<<dim3(blocks, nalpha), BRUTE_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, rcut,
+                                                                               0.0, alphas, fr, energy);
+    c->launches++;
+    mark(c, EV_K1);
+    P3MG_CUDA_TRY(cudaGetLastError());
+    return P3MG_OK;
+  }
+  P3MG_TRY(pairs_bin(c, rcut, &nc));
   mark(c, EV_K0);
-  P3MG_TRY(launch_pairs_cells(dbl, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut, 0.0, alphas, nalpha, fr,
-                              n, energy, c->stream));
-  c->launches += 2;
+  P3MG_TRY(launch_pairs_cells(c->precision == P3MG_FP64, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut,
+                              0.0, alphas, nalpha, fr, n, energy, c->stream));
+  c->launches++;
   mark(c, EV_K1);
   return P3MG_OK;
 }

@@ -49,33 +49,46 @@ __global__ void combine_batch_kernel(double *__restrict__ f, const double *__res
   if (t < count) f[t] += fk[t] + fr[t];
 }
 
-template <typename T>
-void dfree(T *&p) {
-  if (p) cudaFree((void *)p);
-  p = nullptr;
-}
-
+// Sub-buffers of the sweep, carved from one workspace that the context
+// keeps between calls (grown when a call needs more).
 struct SweepMem {
   double *alphas = nullptr, *G = nullptr, *S26 = nullptr, *b81 = nullptr;
   float *G32 = nullptr;
   void *F = nullptr, *P = nullptr;
   double *f = nullptr, *fk = nullptr, *fr = nullptr, *energy = nullptr, *rms2 = nullptr, *ref = nullptr;
-  void release() {
-    dfree(alphas);
-    dfree(G);
-    dfree(S26);
-    dfree(b81);
-    dfree(G32);
-    dfree(F);
-    dfree(P);
-    dfree(f);
-    dfree(fk);
-    dfree(fr);
-    dfree(energy);
-    dfree(rms2);
-    dfree(ref);
-  }
 };
+
+// Lay the buffers out from base (nullptr: only count); returns the bytes.
+size_t sweep_layout(const Ctx *c, int na, int chunk, bool with_ref, unsigned char *base, SweepMem *w) {
+  const size_t n3 = 3 * (size_t)c->n;
+  const size_t M = c->M;
+  const size_t csz = (c->precision == P3MG_FP64) ? 16 : 8;
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> void * {
+    void *p = base ? (void *)(base + off) : nullptr;
+    off += (bytes + 255) & ~(size_t)255;
+    return p;
+  };
+  w->alphas = (double *)take((size_t)na * sizeof(double));
+  w->G = (double *)take((size_t)chunk * M * sizeof(double));
+  w->S26 = (double *)take(26 * (size_t)chunk * sizeof(double));
+  w->b81 = (double *)take(81 * (size_t)chunk * sizeof(double));
+  w->G32 = (c->precision != P3MG_FP64) ? (float *)take((size_t)chunk * M * sizeof(float)) : nullptr;
+  if (method_ad(c->method)) {
+    w->F = take((size_t)chunk * M * csz);
+    w->P = nullptr;
+  } else {
+    w->F = take(3 * (size_t)chunk * M * csz);
+    w->P = take((size_t)chunk * (method_interlaced(c->method) ? 2 : 1) * M * 2 * csz);
+  }
+  w->f = (double *)take((size_t)chunk * n3 * sizeof(double) + 8);
+  w->fk = (double *)take((size_t)chunk * n3 * sizeof(double) + 8);
+  w->fr = (double *)take((size_t)chunk * n3 * sizeof(double) + 8);
+  w->energy = (double *)take((size_t)chunk * sizeof(double));
+  w->rms2 = (double *)take((size_t)na * sizeof(double));
+  w->ref = with_ref ? (double *)take(n3 * sizeof(double) + 8) : nullptr;
+  return off;
+}
 
 }  // namespace
 
@@ -101,35 +114,22 @@ int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *r
   if (chunk < 1) chunk = 1;
   if (chunk > na) chunk = na;
   const size_t M = c->M;
-  const size_t csz = (c->precision == P3MG_FP64) ? 16 : 8;
   SweepMem w;
   int st = P3MG_OK;
   cudaError_t e = cudaSuccess;
-#define SW_ALLOC(ptr, bytes) \
-  if (e == cudaSuccess) e = cudaMalloc((void **)&(ptr), (bytes))
-  SW_ALLOC(w.alphas, (size_t)na * sizeof(double));
-  SW_ALLOC(w.G, (size_t)chunk * M * sizeof(double));
-  SW_ALLOC(w.S26, 26 * (size_t)chunk * sizeof(double));
-  SW_ALLOC(w.b81, 81 * (size_t)chunk * sizeof(double));
-  if (c->precision != P3MG_FP64) SW_ALLOC(w.G32, (size_t)chunk * M * sizeof(float));
-  if (method_ad(c->method)) {
-    SW_ALLOC(w.F, (size_t)chunk * M * csz);
-  } else {
-    SW_ALLOC(w.F, 3 * (size_t)chunk * M * csz);
-    SW_ALLOC(w.P, (size_t)chunk * (method_interlaced(c->method) ? 2 : 1) * M * 2 * csz);
+  const size_t need = sweep_layout(c, na, chunk, ref != nullptr, nullptr, &w);
+  if (need > c->sweep_cap) {
+    if (c->sweep_ws) cudaFree(c->sweep_ws);
+    c->sweep_ws = nullptr;
+    c->sweep_cap = 0;
+    e = cudaMalloc(&c->sweep_ws, need);
+    if (e != cudaSuccess) {
+      record_cuda_error(e);
+      return (e == cudaErrorMemoryAllocation) ? P3MG_ERR_ALLOC : P3MG_ERR_CUDA;
+    }
+    c->sweep_cap = need;
   }
-  SW_ALLOC(w.f, (size_t)chunk * n3 * sizeof(double) + 8);
-  SW_ALLOC(w.fk, (size_t)chunk * n3 * sizeof(double) + 8);
-  SW_ALLOC(w.fr, (size_t)chunk * n3 * sizeof(double) + 8);
-  SW_ALLOC(w.energy, (size_t)chunk * sizeof(double));
-  SW_ALLOC(w.rms2, (size_t)na * sizeof(double));
-  if (ref) SW_ALLOC(w.ref, n3 * sizeof(double) + 8);
-#undef SW_ALLOC
-  if (e != cudaSuccess) {
-    record_cuda_error(e);
-    w.release();
-    return (e == cudaErrorMemoryAllocation) ? P3MG_ERR_ALLOC : P3MG_ERR_CUDA;
-  }
+  sweep_layout(c, na, chunk, ref != nullptr, reinterpret_cast<unsigned char *>(c->sweep_ws), &w);
   do {
     e = cudaMemcpyAsync(w.alphas, alphas, (size_t)na * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess && ref) e = cudaMemcpyAsync(w.ref, ref, n3 * sizeof(double), cudaMemcpyHostToDevice, c->stream);
@@ -204,7 +204,6 @@ int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *r
     st = P3MG_ERR_CUDA;
   }
   cudaStreamSynchronize(c->stream);
-  w.release();
   return st;
 }
 

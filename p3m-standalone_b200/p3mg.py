@@ -96,6 +96,8 @@ def load():
                                            ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]
     L.p3mg_alpha_range.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, _dp]
     L.p3mg_sweep.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
+    L.p3mg_energy.argtypes = [vp, ctypes.c_double, _dp]
+    L.p3mg_backward.argtypes = [vp, ctypes.c_double, ctypes.c_double] + [_dp] * 7
     L.p3mg_estimate_errors.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 4 + [_dp]
     L.p3mg_error_estimate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
     L.p3mg_kernel_times.argtypes = [vp, _dp]
@@ -280,6 +282,23 @@ class Context:
         _check(self._lib.p3mg_sweep(self._h, float(rcut), na, _p(al), _p(rx), _p(ry), _p(rz), _p(rms), _p(f),
                                     int(max_batch)), "p3mg_sweep")
         return dict(rms=rms, forces=f)
+
+    def energy(self, rcut):
+        """P3M energy parts (p3mg_energy): dict total, kspace, realspace, self, neutral."""
+        e = np.zeros(5)
+        _check(self._lib.p3mg_energy(self._h, float(rcut), _p(e)), "p3mg_energy")
+        return dict(zip(("total", "kspace", "realspace", "self", "neutral"), e))
+
+    def backward(self, rcut, grad_E=1.0):
+        """Adjoint (p3mg_backward): dict energy (parts), dx (3, n), dq (n), dalpha, dL,
+        each grad_E times the derivative of the total energy."""
+        n = self.n
+        gx, gq, e = np.zeros((3, n)), np.zeros(n), np.zeros(5)
+        da, dl = np.zeros(1), np.zeros(1)
+        _check(self._lib.p3mg_backward(self._h, float(rcut), float(grad_E), _p(gx[0]), _p(gx[1]), _p(gx[2]),
+                                       _p(gq), _p(da), _p(dl), _p(e)), "p3mg_backward")
+        return dict(energy=dict(zip(("total", "kspace", "realspace", "self", "neutral"), e)), dx=gx, dq=gq,
+                    dalpha=float(da[0]), dL=float(dl[0]))
 
     def error_estimate(self, alpha, rcut, mc_est=1):
         """Analytic RMS error estimates (method.Error / Error_k, Realspace_error):
