@@ -196,6 +196,34 @@ int p3mg_energy(p3mg_ctx *ctx, double rcut, double parts[5]);
 int p3mg_backward(p3mg_ctx *ctx, double rcut, double grad_E, double *grad_x, double *grad_y, double *grad_z,
                   double *grad_q, double *grad_alpha, double *grad_L, double parts[5]);
 
+/* Tile shapes (no counterpart in the reference): brick edge of the
+ * charge-assignment tiles (4 or 8 mesh points; the default is 8 for meshes
+ * of 64 and more, else 4) and pencils per FFT tile (4, 8 or 16; 0 for the
+ * default, 16 in FP32 and 8 in FP64).  Results differ only by the order of
+ * floating-point additions. */
+int p3mg_set_tiles(p3mg_ctx *ctx, int brick, int fft_w);
+
+/* Tile autotuner (no counterpart in the reference): times the context's
+ * force evaluation with rcut for every brick edge and FFT tile width, keeps
+ * the fastest and returns it with its mean time in ms (outputs may be
+ * NULL).  Needs p3mg_influence first. */
+int p3mg_autotune(p3mg_ctx *ctx, double rcut, int *brick, int *fft_w, double *ms);
+
+/* The reference's parameter tuner (Tune, tuning.c:250-370) on the GPU: for
+ * the given system, method, precision mode and real-space cutoff, alpha
+ * from the real-space estimate at rcut (tuning.c:292); then over the even
+ * mesh sizes this library transforms (2^a 3^b 5^c 7^d, 8 .. mesh_max, 0 =
+ * 256) in ascending order and cao from the top down (cao_fixed != 0: that
+ * cao only) while the analytic estimate (mc_est 1) meets target, each
+ * candidate's full force evaluation is timed on the GPU; the fastest wins.
+ * The reference's search stops the same way (a mesh whose cheapest cao is
+ * slower than the best ends it).  Returns mesh, cao, alpha, the estimate and
+ * the time in ms (outputs may be NULL); P3MG_ERR_ARG when no candidate
+ * meets the target. */
+int p3mg_tune(int method_id, int precision, int n, const double *x, const double *y, const double *z,
+              const double *q, double L, double rcut, double target, int cao_fixed, int mesh_max, int *mesh,
+              int *cao, double *alpha, double *estimate, double *ms);
+
 /* FP64 Ewald reference forces for the context's particles, evaluated on nt
  * target particles (targets: host array of particle indices, or NULL with
  * nt == n for all), written (not accumulated) to the host arrays f_x/f_y/f_z

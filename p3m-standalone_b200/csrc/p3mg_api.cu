@@ -668,6 +668,169 @@ extern "C" int p3mg_energy(p3mg_ctx *h, double rcut, double parts[5]) {
   return p3mg_backward(h, rcut, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, parts);
 }
 
+// Brick edge of the charge-assignment tiles and pencils per FFT tile.
+static int set_tiles(Ctx *c, int brick, int fft_w) {
+  if (brick != 4 && brick != 8) return P3MG_ERR_ARG;
+  if (fft_w != 0 && fft_w != 4 && fft_w != 8 && fft_w != 16) return P3MG_ERR_ARG;
+  drop_graph(c);
+  c->fft_w = fft_w;
+  if (brick == c->brick) return P3MG_OK;
+  c->brick = brick;
+  c->nbrick1 = (c->mesh + brick - 1) / brick;
+  const size_t nkey = (size_t)c->nbrick1 * c->nbrick1 * c->nbrick1 * brick * brick * brick;
+  dfree(c->brick_count);
+  dfree(c->brick_start);
+  dfree(c->brick_fill);
+  dfree(c->scatter_tab);  // its pitches depend on the tile edge; rebuilt on the next step
+  P3MG_CUDA_TRY(cudaMalloc(&c->brick_count, nkey * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->brick_start, (nkey + 1) * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->brick_fill, nkey * sizeof(int)));
+  return scan_tmp_reserve(c, (int)nkey);
+}
+
+extern "C" int p3mg_set_tiles(p3mg_ctx *h, int brick, int fft_w) {
+  if (!h) return P3MG_ERR_ARG;
+  cudaSetDevice(h->c.device);
+  return set_tiles(&h->c, brick, fft_w);
+}
+
+// Mean device time of `reps` steps after `warm` untimed ones (events on the
+// context stream; no graph).
+static int time_steps(Ctx *c, double rcut, int warm, int reps, double *ms) {
+  for (int i = 0; i < warm; i++) P3MG_TRY(enqueue_step(c, rcut));
+  cudaEvent_t a, b;
+  P3MG_CUDA_TRY(cudaEventCreate(&a));
+  P3MG_CUDA_TRY(cudaEventCreate(&b));
+  cudaEventRecord(a, c->stream);
+  int st = P3MG_OK;
+  for (int i = 0; i < reps && st == P3MG_OK; i++) st = enqueue_step(c, rcut);
+  cudaEventRecord(b, c->stream);
+  cudaError_t e = cudaEventSynchronize(b);
+  float t = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (st != P3MG_OK) return st;
+  if (e != cudaSuccess) {
+    record_cuda_error(e);
+    return P3MG_ERR_CUDA;
+  }
+  *ms = (double)t / reps;
+  return P3MG_OK;
+}
+
+extern "C" int p3mg_autotune(p3mg_ctx *h, double rcut, int *brick_out, int *fft_w_out, double *ms_out) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!c->have_G) return P3MG_ERR_STATE;
+  if (!(rcut >= 0.0)) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  const bool timing = c->timing;
+  c->timing = false;
+  P3MG_TRY(pairs_reserve(c, rcut));
+  const int bricks[2] = {4, 8}, ws[3] = {4, 8, 16};
+  int bb = c->brick, bw = c->fft_w;
+  double best = 1e300;
+  int st = P3MG_OK;
+  for (int ib = 0; ib < 2 && st == P3MG_OK; ib++)
+    for (int iw = 0; iw < 3 && st == P3MG_OK; iw++) {
+      if (bricks[ib] > c->mesh) continue;
+      st = set_tiles(c, bricks[ib], ws[iw]);
+      double ms = 0.0;
+      if (st == P3MG_OK) st = time_steps(c, rcut, 2, 5, &ms);
+      if (st == P3MG_OK && ms < best) {
+        best = ms;
+        bb = bricks[ib];
+        bw = ws[iw];
+      }
+    }
+  if (st == P3MG_OK) st = set_tiles(c, bb, bw);
+  c->timing = timing;
+  if (st != P3MG_OK) return st;
+  if (brick_out) *brick_out = bb;
+  if (fft_w_out) *fft_w_out = bw;
+  if (ms_out) *ms_out = best;
+  return P3MG_OK;
+}
+
+// Even mesh sizes the FFT supports (2^a 3^b 5^c 7^d), ascending, in [lo, hi].
+static int smooth_meshes(int lo, int hi, int *out, int cap) {
+  int k = 0;
+  int rad[24], np;
+  for (int m = lo; m <= hi && k < cap; m++)
+    if (m % 2 == 0 && fft_factor(m, rad, &np) == 0) out[k++] = m;
+  return k;
+}
+
+extern "C" int p3mg_tune(int method_id, int precision, int n, const double *x, const double *y, const double *z,
+                         const double *q, double L, double rcut, double target, int cao_fixed, int mesh_max,
+                         int *mesh_out, int *cao_out, double *alpha_out, double *est_out, double *ms_out) {
+  if (n < 1 || !x || !y || !z || !q || !(L > 0.0) || !(rcut > 0.0) || !(target > 0.0)) return P3MG_ERR_ARG;
+  if (cao_fixed < 0 || cao_fixed > P3MG_MAX_CAO) return P3MG_ERR_CAO;
+  if (mesh_max <= 0) mesh_max = 256;
+  if (mesh_max > P3MG_MAX_MESH) mesh_max = P3MG_MAX_MESH;
+  double q2 = 0.0;
+  for (int i = 0; i < n; i++) q2 += q[i] * q[i];
+  // alpha from the real-space estimate at rcut (tuning.c:292)
+  const double V = L * L * L;
+  const double arg = (target * sqrt((double)n * rcut * V)) / (2.0 * sqrt(2.0) * q2);
+  if (!(arg > 0.0 && arg < 1.0)) return P3MG_ERR_ARG;
+  const double alpha = sqrt(-log(arg)) / rcut;
+  int meshes[512];
+  const int nm = smooth_meshes(8, mesh_max, meshes, 512);
+  const int cmin = cao_fixed ? cao_fixed : 1, cmax = cao_fixed ? cao_fixed : P3MG_MAX_CAO;
+  double best = 1e300, best_est = 0.0;
+  int bm = 0, bc = 0, cao_last = cmax;
+  bool success = false;
+  // the reference's search (tuning.c:250-370): meshes ascending; per mesh
+  // cao descending while the estimate meets the target, each candidate
+  // timed; stop when the cheapest cao of a mesh is already slower than
+  // the best, or no cao below the last working one is left
+  for (int im = 0; im < nm; im++) {
+    const int m = meshes[im];
+    int cstart = cmax;
+    if (success) {
+      if (cao_last <= cmin) break;
+      cstart = cao_last - 1;
+    }
+    double tmin = 1e300;
+    for (int cao = cstart; cao >= cmin; cao--) {
+      if (cao > m) continue;
+      double est[3];
+      int st = p3mg_estimate_errors(method_id, m, cao, 1, n, q2, L, alpha, rcut, est);
+      if (st != P3MG_OK) return st;
+      if (est[0] > target) break;
+      cao_last = cao;
+      success = true;
+      p3mg_ctx *ctx = nullptr;
+      st = p3mg_create(&ctx, method_id, m, cao, 1, precision);
+      if (st == P3MG_OK) st = p3mg_set_system(ctx, n, x, y, z, q, L);
+      if (st == P3MG_OK) st = p3mg_influence(ctx, alpha);
+      double ms = 0.0;
+      if (st == P3MG_OK) st = pairs_reserve(&ctx->c, rcut);
+      if (st == P3MG_OK) st = time_steps(&ctx->c, rcut, 2, 5, &ms);
+      p3mg_destroy(ctx);
+      if (st != P3MG_OK) return st;
+      if (ms < tmin) tmin = ms;
+      if (ms < best) {
+        best = ms;
+        bm = m;
+        bc = cao;
+        best_est = est[0];
+      }
+    }
+    if (success && tmin > best) break;
+  }
+  if (!success) return P3MG_ERR_ARG;
+  if (mesh_out) *mesh_out = bm;
+  if (cao_out) *cao_out = bc;
+  if (alpha_out) *alpha_out = alpha;
+  if (est_out) *est_out = best_est;
+  if (ms_out) *ms_out = best;
+  return P3MG_OK;
+}
+
 // Shared body of the Ewald entries: checks the targets, uploads them, runs
 // the Ewald kernels and copies the requested outputs (f and/or fk, each
 // three host arrays of nt doubles or NULL) back to the host.

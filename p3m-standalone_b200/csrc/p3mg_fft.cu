@@ -248,6 +248,7 @@ int launch_fft3d(Ctx *c, void *data, int nbatch, int sign) {
   pl.mmagic = magic_div(m);
   // pencils per tile: 128 B of contiguous data per row segment at least
   int W = (sizeof(real) == 8) ? 8 : 16;
+  if (c->fft_w == 4 || c->fft_w == 8 || c->fft_w == 16) W = c->fft_w;  // set by the tile autotuner
   if (m * W * 2 * (int)sizeof(C) > 160 * 1024) W = 4;
   const size_t smem = (size_t)m * sizeof(C) + 2 * (size_t)m * (W + 1) * sizeof(C);
   C *d = reinterpret_cast<C *>(data);

@@ -79,6 +79,7 @@ struct Ctx {
 
   // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
   int brick = 8;
+  int fft_w = 0;    // pencils per FFT tile (0: 16 for FP32, 8 for FP64)
   int nbrick1 = 0;  // bricks per dimension
   // particle counts / starts per sort key: brick, then mesh point in the
   // brick (B^3 keys per brick); the range of brick b is

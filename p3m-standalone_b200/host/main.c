@@ -14,9 +14,12 @@
  * alone runs that single alpha; "batched" computes the whole alpha range
  * in one batched GPU pass (p3mg_sweep) and reports its time divided evenly
  * over the alphas (not with error_k, which needs each alpha's k-space
- * forces).  Parameters the reference parses for its
- * analysis side paths (rdf, rdf_species, cdf, tune, inhomo_error,
- * error_map) are accepted and reported as not provided here. */
+ * forces); "tune" with "prec" picks mesh, cao (cao 0: any; otherwise that
+ * cao) and alpha with the reference's tuning search (tuning.c:250-370,
+ * which the reference's main parses but never runs) timed on the GPU, then
+ * runs that single alpha.  Parameters the reference parses for its
+ * analysis side paths (rdf, rdf_species, cdf, inhomo_error, error_map) are
+ * accepted and reported as not provided here. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -137,9 +140,14 @@ int main(int argc, char **argv) {
   parameters.alpha = 0.0;
   parameters.precision = param_isset("fp32", &params) ? P3MG_FP32_MIXED : P3MG_FP64;
 
+  const int tune = param_isset("tune", &params);
   const int have_range =
       param_isset("alphamin", &params) && param_isset("alphamax", &params) && param_isset("alphastep", &params);
-  if (!have_range && !param_isset("alpha", &params)) {
+  if (tune && !param_isset("prec", &params)) {
+    puts("Need 'prec' (target RMS force error) with 'tune'.");
+    exit(1);
+  }
+  if (!have_range && !param_isset("alpha", &params) && !tune) {
     puts("Need to provide either alpha-range (alphamin, alphamax, alphastep) or alpha.");
     exit(1);
   }
@@ -156,7 +164,7 @@ int main(int argc, char **argv) {
     exit(1);
   }
 
-  static const char *const side_paths[] = {"rdf", "rdf_species", "cdf", "tune", "inhomo_error", "error_map"};
+  static const char *const side_paths[] = {"rdf", "rdf_species", "cdf", "inhomo_error", "error_map"};
   for (size_t i = 0; i < sizeof side_paths / sizeof side_paths[0]; i++)
     if (param_isset(side_paths[i], &params))
       fprintf(stderr, "Note: '%s' is not provided by this program; ignored.\n", side_paths[i]);
@@ -176,6 +184,27 @@ int main(int argc, char **argv) {
     }
     if (!system) exit(1);
     puts("Done.");
+  }
+
+  if (tune) {
+    if (!method_by_id(methodnr)) {
+      fprintf(stderr, "Method %d not know.", methodnr);
+      exit(126);
+    }
+    int tm = 0, tc = 0;
+    double ta = 0.0, te = 0.0, tms = 0.0;
+    const int st = p3mg_tune(methodnr, parameters.precision, system->nparticles, system->p->x, system->p->y,
+                             system->p->z, system->q, system->length, parameters.rcut, prec, parameters.cao, 0, &tm,
+                             &tc, &ta, &te, &tms);
+    if (st != P3MG_OK) p3m_host_die(st, "p3mg_tune");
+    printf("Tuned for precision %e: mesh %d cao %d alpha %lf (estimate %e, %e ms per force evaluation)\n", prec, tm,
+           tc, ta, te, tms);
+    parameters.mesh = tm;
+    parameters.cao = tc;
+    parameters.cao3 = tc * tc * tc;
+    parameters.ip = tc - 1;
+    alphamin = alphamax = ta;
+    alphastep = 1.0;
   }
 
   if (param_isset("vtf_file", &params)) write_vtf(vtf_file, system);
@@ -218,6 +247,7 @@ int main(int argc, char **argv) {
     fprintf(stderr, "Method %d not know.", methodnr);
     exit(126);
   }
+
   fprintf(stderr, "Using %s.\n", method->method_name);
 
   FILE *fout = fopen(param_isset("outfile", &params) ? out_file : "out.dat", "w");

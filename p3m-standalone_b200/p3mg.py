@@ -98,6 +98,11 @@ def load():
     L.p3mg_sweep.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
     L.p3mg_energy.argtypes = [vp, ctypes.c_double, _dp]
     L.p3mg_backward.argtypes = [vp, ctypes.c_double, ctypes.c_double] + [_dp] * 7
+    L.p3mg_set_tiles.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    _ip = ctypes.POINTER(ctypes.c_int)
+    L.p3mg_autotune.argtypes = [vp, ctypes.c_double, _ip, _ip, _dp]
+    L.p3mg_tune.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_dp] * 4 + [ctypes.c_double] * 3 + [
+        ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
     L.p3mg_estimate_errors.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 4 + [_dp]
     L.p3mg_error_estimate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
     L.p3mg_kernel_times.argtypes = [vp, _dp]
@@ -300,6 +305,16 @@ class Context:
         return dict(energy=dict(zip(("total", "kspace", "realspace", "self", "neutral"), e)), dx=gx, dq=gq,
                     dalpha=float(da[0]), dL=float(dl[0]))
 
+    def set_tiles(self, brick, fft_w=0):
+        _check(self._lib.p3mg_set_tiles(self._h, int(brick), int(fft_w)), "p3mg_set_tiles")
+
+    def autotune(self, rcut):
+        """Tile autotuner (p3mg_autotune): dict brick, fft_w, ms."""
+        b, w, t = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0.0)
+        _check(self._lib.p3mg_autotune(self._h, float(rcut), ctypes.byref(b), ctypes.byref(w), ctypes.byref(t)),
+               "p3mg_autotune")
+        return dict(brick=b.value, fft_w=w.value, ms=t.value)
+
     def error_estimate(self, alpha, rcut, mc_est=1):
         """Analytic RMS error estimates (method.Error / Error_k, Realspace_error):
         dict total, kspace, realspace."""
@@ -380,6 +395,17 @@ def alpha_range(alphamin, alphamax, alphastep):
     out = np.zeros(k)
     L.p3mg_alpha_range(float(alphamin), float(alphamax), float(alphastep), k, _p(out))
     return out
+
+
+def tune(method, x, y, z, q, L, rcut, target, precision=FP64, cao=0, mesh_max=0):
+    """The reference's Tune on the GPU (p3mg_tune): dict mesh, cao, alpha, estimate, ms."""
+    x, y, z, q = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z, q))
+    m, c = ctypes.c_int(0), ctypes.c_int(0)
+    a, e, t = ctypes.c_double(0.0), ctypes.c_double(0.0), ctypes.c_double(0.0)
+    _check(load().p3mg_tune(int(method), int(precision), len(x), _p(x), _p(y), _p(z), _p(q), float(L), float(rcut),
+                            float(target), int(cao), int(mesh_max), ctypes.byref(m), ctypes.byref(c), ctypes.byref(a),
+                            ctypes.byref(e), ctypes.byref(t)), "p3mg_tune")
+    return dict(mesh=m.value, cao=c.value, alpha=a.value, estimate=e.value, ms=t.value)
 
 
 def estimate_errors(method, mesh, cao, n, q2, L, alpha, rcut, mc_est=1):
