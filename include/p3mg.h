@@ -224,6 +224,22 @@ int p3mg_tune(int method_id, int precision, int n, const double *x, const double
               const double *q, double L, double rcut, double target, int cao_fixed, int mesh_max, int *mesh,
               int *cao, double *alpha, double *estimate, double *ms);
 
+/* Batches of independent systems (no counterpart in the reference): the
+ * force evaluations of several contexts (their own systems, meshes, methods
+ * and precisions, on one device) run as the parallel branches of one CUDA
+ * graph, so that many small systems occupy the GPU together.  Each
+ * context's results are read as after p3mg_compute (p3mg_get_forces or
+ * p3mg_get_forces_device).  The first p3mg_batch_compute of a batch runs
+ * eagerly, the second captures the graph, later ones replay it; new
+ * particle counts, box lengths or cutoffs re-capture.  A context belongs to at most one
+ * batch at a time and must not be used on its own while a batch call is in
+ * flight; p3mg_batch_destroy leaves the contexts alive. */
+typedef struct p3mg_batch p3mg_batch;
+int p3mg_batch_create(p3mg_batch **batch, p3mg_ctx *const *ctxs, int count);
+int p3mg_batch_compute(p3mg_batch *batch, const double *rcuts);
+int p3mg_batch_synchronize(p3mg_batch *batch);
+void p3mg_batch_destroy(p3mg_batch *batch);
+
 /* FP64 Ewald reference forces for the context's particles, evaluated on nt
  * target particles (targets: host array of particle indices, or NULL with
  * nt == n for all), written (not accumulated) to the host arrays f_x/f_y/f_z

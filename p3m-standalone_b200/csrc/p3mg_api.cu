@@ -354,8 +354,10 @@ static int set_system_common(Ctx *c, int n, const double *x, const double *y, co
   if (n < 0 || !(L > 0.0) || !isfinite(L)) return P3MG_ERR_ARG;
   if (n > 0 && (!x || !y || !z || !q)) return P3MG_ERR_ARG;
   cudaSetDevice(c->device);
-  const bool same_shape = (n == c->n) && c->x != nullptr;
-  if (!same_shape) drop_graph(c);  // a captured step holds the old buffers and sizes
+  // a captured step holds the old buffers, sizes and box (cell counts,
+  // mesh spacing are kernel arguments)
+  const bool same_shape = (n == c->n) && c->x != nullptr && L == c->L;
+  if (!same_shape) drop_graph(c);
   P3MG_TRY(alloc_system(c, n));
   if (L != c->L) c->have_G = false;  // G_opt and the self-force depend on L
   c->L = L;
@@ -828,6 +830,169 @@ extern "C" int p3mg_tune(int method_id, int precision, int n, const double *x, c
   if (alpha_out) *alpha_out = alpha;
   if (est_out) *est_out = best_est;
   if (ms_out) *ms_out = best;
+  return P3MG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches of independent systems (no counterpart in the reference): one CUDA
+// graph whose parallel branches are the force evaluations of several
+// contexts (each on its own stream, joined to the batch stream for the
+// capture), launched as one unit so that small systems fill the GPU
+// together.  The first run of a batch is eager (allocations, lane tables),
+// the second captures, later runs replay; a change of any context's
+// particle count or of the cutoffs re-captures.
+struct p3mg_batch {
+  std::vector<p3mg_ctx *> ctx;
+  std::vector<double> rcut;
+  std::vector<int> n;
+  std::vector<double> L;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec = nullptr;
+  int runs = 0;
+  long long launches = 0;
+  int device = 0;
+};
+
+extern "C" int p3mg_batch_create(p3mg_batch **out, p3mg_ctx *const *ctxs, int count) {
+  if (!out || !ctxs || count < 1) return P3MG_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < count; i++)
+    if (!ctxs[i] || ctxs[i]->c.device != ctxs[0]->c.device) return P3MG_ERR_ARG;
+  for (int i = 0; i < count; i++)
+    for (int j = i + 1; j < count; j++)
+      if (ctxs[i] == ctxs[j]) return P3MG_ERR_ARG;
+  p3mg_batch *b = new (std::nothrow) p3mg_batch();
+  if (!b) return P3MG_ERR_ALLOC;
+  b->ctx.assign(ctxs, ctxs + count);
+  b->device = ctxs[0]->c.device;
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+  b->join.assign(count, nullptr);
+  for (int i = 0; i < count && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    record_cuda_error(e);
+    p3mg_batch_destroy(b);
+    return P3MG_ERR_CUDA;
+  }
+  *out = b;
+  return P3MG_OK;
+}
+
+extern "C" void p3mg_batch_destroy(p3mg_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  for (cudaEvent_t ev : b->join)
+    if (ev) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->done) cudaEventDestroy(b->done);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+// All branches: fork from the batch stream, one step per context, join.
+static int batch_enqueue(p3mg_batch *b, const double *rcuts) {
+  P3MG_CUDA_TRY(cudaEventRecord(b->fork, b->stream));
+  for (size_t i = 0; i < b->ctx.size(); i++) {
+    Ctx *c = &b->ctx[i]->c;
+    P3MG_CUDA_TRY(cudaStreamWaitEvent(c->stream, b->fork, 0));
+    P3MG_TRY(enqueue_step(c, rcuts[i]));
+    P3MG_CUDA_TRY(cudaEventRecord(b->join[i], c->stream));
+    P3MG_CUDA_TRY(cudaStreamWaitEvent(b->stream, b->join[i], 0));
+  }
+  return P3MG_OK;
+}
+
+extern "C" int p3mg_batch_compute(p3mg_batch *b, const double *rcuts) {
+  if (!b || !rcuts) return P3MG_ERR_ARG;
+  const size_t k = b->ctx.size();
+  for (size_t i = 0; i < k; i++) {
+    Ctx *c = &b->ctx[i]->c;
+    if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+    if (!c->have_G) return P3MG_ERR_STATE;
+    if (!(rcuts[i] >= 0.0)) return P3MG_ERR_ARG;
+  }
+  cudaSetDevice(b->device);
+  bool same = (b->rcut.size() == k);
+  for (size_t i = 0; same && i < k; i++)
+    same = (b->rcut[i] == rcuts[i]) && (b->n[i] == b->ctx[i]->c.n) && (b->L[i] == b->ctx[i]->c.L);
+  if (!same) {
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+    b->runs = 0;
+    b->rcut.assign(rcuts, rcuts + k);
+    b->n.resize(k);
+    b->L.resize(k);
+    for (size_t i = 0; i < k; i++) {
+      b->n[i] = b->ctx[i]->c.n;
+      b->L[i] = b->ctx[i]->c.L;
+    }
+  }
+  // stage timing events are not captured; switch them off for the batch
+  std::vector<bool> timing(k);
+  for (size_t i = 0; i < k; i++) {
+    timing[i] = b->ctx[i]->c.timing;
+    b->ctx[i]->c.timing = false;
+  }
+  int st = P3MG_OK;
+  if (b->runs == 0) {
+    for (size_t i = 0; i < k && st == P3MG_OK; i++) st = pairs_reserve(&b->ctx[i]->c, rcuts[i]);
+    if (st == P3MG_OK) st = batch_enqueue(b, rcuts);
+    if (st == P3MG_OK) b->runs = 1;
+  } else {
+    if (!b->gexec) {
+      cudaGraph_t g = nullptr;
+      long long before = 0;
+      for (size_t i = 0; i < k; i++) before += b->ctx[i]->c.launches;
+      cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        st = batch_enqueue(b, rcuts);
+        e = cudaStreamEndCapture(b->stream, &g);
+      }
+      long long after = 0;
+      for (size_t i = 0; i < k; i++) after += b->ctx[i]->c.launches;
+      b->launches = after - before;
+      if (st == P3MG_OK && e == cudaSuccess) e = cudaGraphInstantiate(&b->gexec, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (st == P3MG_OK && e != cudaSuccess) {
+        record_cuda_error(e);
+        b->gexec = nullptr;
+        st = P3MG_ERR_CUDA;
+      }
+    }
+    if (st == P3MG_OK) {
+      cudaError_t e = cudaGraphLaunch(b->gexec, b->stream);
+      if (e != cudaSuccess) {
+        record_cuda_error(e);
+        st = P3MG_ERR_CUDA;
+      }
+      // the captured launches count towards the first context
+      b->ctx[0]->c.launches += b->launches;
+      b->runs++;
+    }
+  }
+  // later work on each context stream follows the batch
+  if (st == P3MG_OK) {
+    cudaError_t e = cudaEventRecord(b->done, b->stream);
+    for (size_t i = 0; i < k && e == cudaSuccess; i++) e = cudaStreamWaitEvent(b->ctx[i]->c.stream, b->done, 0);
+    if (e != cudaSuccess) {
+      record_cuda_error(e);
+      st = P3MG_ERR_CUDA;
+    }
+  }
+  for (size_t i = 0; i < k; i++) b->ctx[i]->c.timing = timing[i];
+  return st;
+}
+
+extern "C" int p3mg_batch_synchronize(p3mg_batch *b) {
+  if (!b) return P3MG_ERR_ARG;
+  cudaSetDevice(b->device);
+  P3MG_CUDA_TRY(cudaStreamSynchronize(b->stream));
   return P3MG_OK;
 }
 

@@ -103,6 +103,11 @@ def load():
     L.p3mg_autotune.argtypes = [vp, ctypes.c_double, _ip, _ip, _dp]
     L.p3mg_tune.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_dp] * 4 + [ctypes.c_double] * 3 + [
         ctypes.c_int, ctypes.c_int, _ip, _ip, _dp, _dp, _dp]
+    L.p3mg_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_int]
+    L.p3mg_batch_compute.argtypes = [vp, _dp]
+    L.p3mg_batch_synchronize.argtypes = [vp]
+    L.p3mg_batch_destroy.argtypes = [vp]
+    L.p3mg_batch_destroy.restype = None
     L.p3mg_estimate_errors.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 4 + [_dp]
     L.p3mg_error_estimate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
     L.p3mg_kernel_times.argtypes = [vp, _dp]
@@ -395,6 +400,35 @@ def alpha_range(alphamin, alphamax, alphastep):
     out = np.zeros(k)
     L.p3mg_alpha_range(float(alphamin), float(alphamax), float(alphastep), k, _p(out))
     return out
+
+
+class Batch:
+    """Several contexts' force evaluations as one CUDA graph (p3mg_batch_*)."""
+
+    def __init__(self, contexts):
+        self._lib = load()
+        self.contexts = list(contexts)
+        arr = (ctypes.c_void_p * len(self.contexts))(*[c._h.value for c in self.contexts])
+        self._h = ctypes.c_void_p(0)
+        _check(self._lib.p3mg_batch_create(ctypes.byref(self._h), arr, len(self.contexts)), "p3mg_batch_create")
+
+    def compute(self, rcuts):
+        r = np.ascontiguousarray(np.broadcast_to(np.asarray(rcuts, dtype=np.float64), (len(self.contexts),)))
+        _check(self._lib.p3mg_batch_compute(self._h, _p(r)), "p3mg_batch_compute")
+
+    def synchronize(self):
+        _check(self._lib.p3mg_batch_synchronize(self._h), "p3mg_batch_synchronize")
+
+    def close(self):
+        if self._h:
+            self._lib.p3mg_batch_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def tune(method, x, y, z, q, L, rcut, target, precision=FP64, cao=0, mesh_max=0):

@@ -76,3 +76,18 @@ def test_graph_replay_follows_alpha_changes(gpu):
             want = ref_ctx.calculate_forces(3.0)
             assert O.rel_rms(got["f"].ravel(), want["f"].ravel()) <= 1e-14
             assert O.rel_rms(got["f_r"].ravel(), want["f_r"].ravel()) <= 1e-14
+
+
+def test_graph_replay_follows_box_changes(gpu):
+    # a new box length with the same particle count re-captures the step
+    x, y, z, q = p3mg.generate_system(0, 600, 10.0, seed=53)
+    with p3mg.Context(7, 16, 5, 1) as ctx, p3mg.Context(7, 16, 5, 1) as ref:
+        ctx.set_graph(True)
+        for L in (10.0, 10.0, 10.0, 11.5, 11.5, 12.25):
+            s = L / 10.0
+            for c in (ctx, ref):
+                c.set_system(x * s, y * s, z * s, q, L)
+                c.influence(1.0)
+            got = ctx.calculate_forces(3.0)["f"]
+            want = ref.calculate_forces(3.0)["f"]
+            assert O.rel_rms(got.ravel(), want.ravel()) <= 1e-14, L
