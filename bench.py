@@ -131,16 +131,19 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(kernel):
-    """DRAM bytes per launch of `kernel` at this workload from a committed
-    ncu summary (profiles/traffic.json), or None."""
+def profile_counters(kernel):
+    """DRAM bytes and warp instructions per launch of `kernel` at the headline
+    workload from the committed ncu summary (profiles/traffic.json), or {}."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
-            d = json.load(fh)
-        v = d.get(kernel)
-        return None if v is None else float(v["bytes_per_launch"])
+            return json.load(fh).get(kernel, {})
     except Exception:
-        return None
+        return {}
+
+
+def profile_traffic(kernel):
+    v = profile_counters(kernel).get("bytes_per_launch")
+    return None if v is None else float(v)
 
 
 # ------------------------------------------------------------- our arm
@@ -283,6 +286,29 @@ def run_ours(args, rank, world, local_rank):
         achieved = abytes / (k[dom] * 1e-3) / 1e9
         kernel_names = {"gather": "gather_kernel", "scatter": "scatter_kernel", "pairs": "pairs_cell_kernel"}
         traffic = profile_traffic(kernel_names[dom])
+        g_bytes = gather_bytes(W["method"], n, W["mesh"], s)
+        g_achieved = g_bytes / (k["gather"] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": kernel_names[dom], "achieved": round(achieved, 2), "peak": peak,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                    "algorithmic_bytes": int(abytes), "traffic": traffic}
+        inst = profile_counters("pairs_cell_kernel").get("warp_instructions_per_launch")
+        if dom == "pairs" and inst and n == W["n"]:
+            # The pair kernel moves ~48 MB per launch and uses no tensor cores:
+            # its ceiling is instruction issue (4 warp instructions per clock
+            # per SM).  Achieved = the warp instructions of one launch (ncu,
+            # this workload) over the live CUDA-event time of the launch.
+            sm_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+            ipeak = 4 * 148 * sm_mhz * 1e6 / 1e9
+            iach = inst / (k["pairs"] * 1e-3) / 1e9
+            pairs_unique = 2.0 * math.pi / 3.0 * W["rcut"] ** 3 * n * (n / L ** 3)
+            roofline = {"bound": "issue", "kernel": "pairs_cell_kernel", "achieved": round(iach, 1),
+                        "peak": round(ipeak, 1), "unit": "G warp-instructions/s", "frac": round(iach / ipeak, 4),
+                        "peak_source": "4 warp instructions/clock/SM x 148 SMs x sampled SM clock",
+                        "traffic": traffic, "algorithmic_bytes": int(abytes),
+                        "hbm_frac": round(achieved / peak, 4),
+                        "pairs_per_s": round(pairs_unique / (k["pairs"] * 1e-3), 1),
+                        "unique_pairs_within_rcut": int(pairs_unique),
+                        "instructions_source": "profiles/traffic.json (ncu smsp__inst_executed.sum)"}
         out = {
             "metric": METRIC,
             "value": round(value, 3),
@@ -309,10 +335,11 @@ def run_ours(args, rank, world, local_rank):
                            "fp64": {k2: round(v, 4) for k2, v in r64["kernels"].items()}},
             "e2e": {"value": round(e2e, 3), "unit": "steps/s", "h2d_bytes_per_step": 4 * 8 * n,
                     "d2h_bytes_per_step": 3 * 8 * n},
-            "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": round(achieved, 2),
-                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "peak_source": peak_kind, "algorithmic_bytes": int(abytes),
-                         "traffic": traffic},
+            "roofline": roofline,
+            "roofline_hbm": {"kernel": "gather_kernel", "achieved": round(g_achieved, 2), "peak": peak,
+                             "unit": "GB/s", "frac": round(g_achieved / peak, 4), "peak_source": peak_kind,
+                             "algorithmic_bytes": int(g_bytes), "traffic": profile_traffic("gather_kernel"),
+                             "note": "the gather is bound by L1 throughput (78 % under ncu), not HBM"},
             "step_roofline": {"algorithmic_bytes": int(algorithmic_bytes(W["method"], n, W["mesh"], 4)),
                               "achieved_gbs": round(algorithmic_bytes(W["method"], n, W["mesh"], 4)
                                                     / (r32["ms"] * 1e-3) / 1e9, 2)},
@@ -321,6 +348,184 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clocks,
         }
     return out, results
+
+
+# ------------------------------------------------- secondary workloads
+
+def _events(stream):
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _timed(stream, fn, reps=3):
+    """Median device time (ms) of fn() bracketed by events on `stream`."""
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def _smooth_even(m):
+    while True:
+        r = m
+        for p in (2, 3, 5, 7):
+            while r % p == 0:
+                r //= p
+        if r == 1 and m % 2 == 0:
+            return m
+        m += 1
+
+
+def secondary_workloads(dev):
+    """The batched, differentiated and multi-system workloads, each timed on
+    the device (median of three runs after one warm-up)."""
+    import torch
+    import p3mg
+    out = {}
+
+    def stream_of(ctx):
+        return torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    # alpha sweep: the reference's example (method 7, 1000 particles, box 10,
+    # mesh 16, cao 7, mc 2, rcut 3, alpha 0.1..2.5 step 0.05: 49 alphas), FP64
+    x, y, z, q = p3mg.generate_system(0, 1000, 10.0, seed=12345)
+    with p3mg.Context(7, 16, 7, 2, p3mg.FP64) as ctx:
+        ctx.set_system(x, y, z, q, 10.0)
+        st = stream_of(ctx)
+        al = p3mg.alpha_range(0.1, 2.5, 0.05)
+        ctx.influence(1.0)
+        ctx.set_graph(True)
+        step = _timed(st, lambda: ctx.compute(3.0), reps=7)
+        loop = _timed(st, lambda: [(ctx.influence(a), ctx.compute(3.0)) for a in al])
+        sweep = _timed(st, lambda: ctx.sweep(3.0, al))
+        a64 = np.linspace(0.1, 2.5, 64)
+        sweep64 = _timed(st, lambda: ctx.sweep(3.0, a64))
+    out["alpha_sweep_1000"] = {
+        "workload": "method 7, 1000 particles, box 10, mesh 16, cao 7, mc 2, rcut 3, FP64",
+        "step_ms": round(step, 4), "alphas": len(al), "sweep_ms": round(sweep, 3),
+        "per_alpha_loop_ms": round(loop, 3), "sweep_64_alphas_ms": round(sweep64, 3),
+        "sweep_64_over_step": round(sweep64 / step, 2)}
+
+    # the same 64-alpha sweep at the headline size (method 1, 1M, mesh 128), FP32
+    W = WORKLOAD
+    x, y, z, q = p3mg.generate_system(0, W["n"], W["box"], seed=W["seed"])
+    with p3mg.Context(W["method"], W["mesh"], W["cao"], W["mc"], p3mg.FP32_MIXED) as ctx:
+        ctx.set_system(x, y, z, q, W["box"])
+        st = stream_of(ctx)
+        ctx.influence(W["alpha"])
+        ctx.set_graph(True)
+        step = _timed(st, lambda: ctx.compute(W["rcut"]), reps=5)
+        a64 = np.linspace(0.6, 1.2, 64)
+        sweep64 = _timed(st, lambda: ctx.sweep(W["rcut"], a64), reps=1)
+    out["alpha_sweep_1m"] = {"workload": W["workload"] + ", FP32, 64 alphas 0.6..1.2",
+                             "step_ms": round(step, 4), "sweep_64_alphas_ms": round(sweep64, 2),
+                             "sweep_64_over_step": round(sweep64 / step, 2)}
+
+    # adjoint: 50,000 separated dipoles, box 46.4, method 2, mesh 64, cao 5,
+    # rcut 3, alpha 1, FP32; -dE/dx against FP64 Ewald forces on 2000 targets
+    x, y, z, q = p3mg.generate_system(3, 100000, 46.4, seed=12345)
+    with p3mg.Context(2, 64, 5, 1, p3mg.FP32_MIXED) as ctx:
+        ctx.set_system(x, y, z, q, 46.4)
+        ctx.influence(1.0)
+        st = stream_of(ctx)
+        fwd = _timed(st, lambda: ctx.compute(3.0))
+        bwd = _timed(st, lambda: ctx.backward(3.0))
+        g = ctx.backward(3.0)
+        tg = np.sort(np.random.default_rng(7).choice(len(x), 2000, replace=False))
+        ew = ctx.ewald_forces(tg)["f"]
+        err = float(np.sqrt(np.sum((-g["dx"][:, tg] - ew) ** 2) / len(tg)))
+        f = ctx.calculate_forces(3.0)["f"]
+        ferr = float(np.sqrt(np.sum((f[:, tg] - ew) ** 2) / len(tg)))
+    out["adjoint_dipoles_100k"] = {
+        "workload": "method 2, 50000 dipoles (100000 charges), box 46.4, mesh 64, cao 5, rcut 3, alpha 1, FP32",
+        "force_step_ms": round(fwd, 3), "energy_and_gradients_ms": round(bwd, 3),
+        "energy": g["energy"]["total"], "dE_dalpha": g["dalpha"], "virial_minus_L_dE_dL": -46.4 * g["dL"],
+        "rms_minus_grad_vs_ewald": err, "rms_force_vs_ewald": ferr}
+
+    # uneven multi-system batch: 16 systems, N log-uniform in 2e3..2e6 at
+    # density 1, uniform / Gaussian (sigma L/6) alternating, mesh the next
+    # even 7-smooth size >= clamp(1.28 L, 32, 160), cao 7, rcut 3.5,
+    # alpha 0.9, methods 1 and 3 alternating
+    rng = np.random.default_rng(16)
+    ns = np.sort(np.exp(rng.uniform(np.log(2e3), np.log(2e6), 16)).astype(int))
+    res = {}
+    for prec, tag in ((p3mg.FP32_MIXED, "fp32"), (p3mg.FP64, "fp64")):
+        ctxs = []
+        for k, nk in enumerate(ns):
+            Lk = float(nk) ** (1.0 / 3.0)
+            mk = _smooth_even(int(np.ceil(min(max(1.28 * Lk, 32), 160))))
+            xs = p3mg.generate_system(0 if k % 2 == 0 else 4, int(nk), Lk, seed=1000 + k)
+            c = p3mg.Context(1 if k % 2 == 0 else 3, mk, 7, 1, prec)
+            c.set_system(*xs, Lk)
+            c.influence(0.9)
+            ctxs.append(c)
+        # host clock around device-synchronised calls: the contexts run on
+        # their own streams, which one stream's events would not cover
+        for c in ctxs:
+            c.compute(3.5)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            for c in ctxs:
+                c.compute(3.5)
+        torch.cuda.synchronize()
+        seq = (time.perf_counter() - t0) / 3 * 1e3
+        with p3mg.Batch(ctxs) as b:
+            b.compute([3.5] * len(ctxs))
+            b.compute([3.5] * len(ctxs))
+            b.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(3):
+                b.compute([3.5] * len(ctxs))
+            b.synchronize()
+            bt = (time.perf_counter() - t0) / 3 * 1e3
+        for c in ctxs:
+            c.close()
+        res[tag] = {"batch_graph_ms": round(bt, 3), "sequential_ms": round(seq, 3),
+                    "systems_per_s": round(16 * 1000.0 / bt, 2)}
+    out["multi_system_batch"] = {"particles": [int(v) for v in ns], "timing": "host clock, device synchronised",
+                                 **res}
+
+    # tuning grid: slab of 20,000 charges in [0.25L, 0.75L) x [0,L)^2, L 34.2,
+    # method 7, mesh {32,48,64,96} x cao 3..7 x 64 alphas 0.1..2.5, FP32;
+    # RMS error of every point against the FP64 Ewald forces and the estimate
+    Lg = 34.2
+    x, y, z, q = p3mg.generate_system(5, 20000, Lg, seed=12345)
+    q2 = float(np.sum(q * q))
+    al = np.linspace(0.1, 2.5, 64)
+    with p3mg.Context(7, 32, 7, 1, p3mg.FP64) as ec:
+        ec.set_system(x, y, z, q, Lg)
+        ref = ec.ewald_forces()["f"]
+    total_ms, best = 0.0, None
+    t_all = time.perf_counter()
+    for mesh in (32, 48, 64, 96):
+        for cao in range(3, 8):
+            with p3mg.Context(7, mesh, cao, 1, p3mg.FP32_MIXED) as ctx:
+                ctx.set_system(x, y, z, q, Lg)
+                st = stream_of(ctx)
+                e0, e1 = _events(st)
+                e0.record(st)
+                r = ctx.sweep(3.0, al, ref=ref)
+                e1.record(st)
+                e1.synchronize()
+                total_ms += e0.elapsed_time(e1)
+                for a, rms in zip(al, r["rms"]):
+                    if best is None or rms < best[0]:
+                        est = p3mg.estimate_errors(7, mesh, cao, len(x), q2, Lg, a, 3.0)["total"]
+                        best = (float(rms), mesh, cao, float(a), est)
+    out["tuning_grid_slab_20k"] = {
+        "points": 4 * 5 * 64, "grid_device_ms": round(total_ms, 2),
+        "grid_wall_s": round(time.perf_counter() - t_all, 2),
+        "best": {"rms_error": best[0], "mesh": best[1], "cao": best[2], "alpha": best[3], "estimate": best[4]}}
+    return out
 
 
 # ----------------------------------------------------------- CPU baseline
@@ -429,6 +634,8 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="particles (default: the workload's 1,000,000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the Ewald error report")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the sweep / adjoint / batch / tuning-grid workloads")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -439,6 +646,9 @@ def main():
             print(json.dumps(out))
         return
     out, _ = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_workloads:
+        import torch
+        out["workloads"] = secondary_workloads(torch.device("cuda", local_rank))
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             t, desc, kind, parts = reference_sample()

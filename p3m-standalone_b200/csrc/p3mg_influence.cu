@@ -167,20 +167,33 @@ __global__ void self_force_sum_kernel(const double *__restrict__ G, int m, int c
         sy[c] = sinc_pi(mi * (double)(ty + (c - 2) * m));
         sz[c] = sinc_pi(mi * (double)(tz + (c - 2) * m));
       }
-      // U over c in {-2..2}^3 is needed at a (|a|<=1) and a+m' (|.|<=2)
+      // U(c) = (sx sy sz)^cao over c in {-2..2}^3 is needed at a (|a|<=1)
+      // and a+m' (|.|<=2); per-axis integer powers, multiplied
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        sx[c] = ipow_d(sx[c], cao);
+        sy[c] = ipow_d(sy[c], cao);
+        sz[c] = ipow_d(sz[c], cao);
+      }
+#pragma unroll
       for (int ax = 0; ax < 3; ax++)
+#pragma unroll
         for (int ay = 0; ay < 3; ay++)
+#pragma unroll
           for (int az = 0; az < 3; az++) {
-            const double U = pow(sx[ax + 1] * sy[ay + 1] * sz[az + 1], (double)cao);
-            const double gU = g * U;
+            const double gU = g * (sx[ax + 1] * sy[ay + 1] * sz[az + 1]);
             int t = 0;
+#pragma unroll
             for (int px = -1; px <= 1; px++)
-              for (int py = -1; py <= 1; py++)
+#pragma unroll
+              for (int py = -1; py <= 1; py++) {
+                const double uxy = sx[ax + 1 + px] * sy[ay + 1 + py];
+#pragma unroll
                 for (int pz = -1; pz <= 1; pz++) {
                   if (px == 0 && py == 0 && pz == 0) continue;
-                  const double Us = pow(sx[ax + 1 + px] * sy[ay + 1 + py] * sz[az + 1 + pz], (double)cao);
-                  acc[t++] += gU * Us;
+                  acc[t++] += gU * (uxy * sz[az + 1 + pz]);
                 }
+              }
           }
     }
   }
