@@ -28,19 +28,21 @@ __host__ __device__ constexpr size_t scatter_stage_bytes() {
 // One CTA per mesh brick.  Round by round, SCATTER_CHUNK particles of the
 // brick are staged: one thread per particle computes its stencil origin in
 // the tile and its B-spline weights (charge folded into the x weights) for
-// each mesh.  Then each warp deposits whole particles: its 32 lanes take
-// distinct stencil points (a, b, c) of the same particle, so the shared-
-// memory atomics of one instruction never hit the same address.  The tile
-// is added to the global mesh at the end (periodic wrap, one global atomic
-// per non-zero tile point).
+// each mesh.  Then each warp deposits whole particles: each lane owns one
+// (b, c) column of the stencil (cao^2 columns over one or two passes of 32
+// lanes), forms Wy_b Wz_c once and adds Wx_a Wy_b Wz_c for a = 0..cao-1
+// down the column; the host picks the row pitch so that the 32 columns of a
+// pass fall in 32 different banks (16 per half-warp for 8-byte elements),
+// so one instruction's shared-memory atomics neither collide nor conflict.
+// The tile is added to the global mesh at the end (periodic wrap, one
+// global atomic per non-zero tile point).
 template <typename real, int CAO, int NMESH>
 __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *__restrict__ sxyzq,
                                                                   const int *__restrict__ start, int m, int B, int nb,
                                                                   double Hi, double shift, int SR, int SP,
-                                                                  const int2 *__restrict__ lanetab,
+                                                                  const int4 *__restrict__ lanetab,
                                                                   typename cplx<real>::type *__restrict__ Q) {
-  constexpr int S = CAO * CAO * CAO;
-  constexpr int IT = (S + 31) / 32;  // points per lane: the host picks pitches with even bank classes
+  constexpr int NPASS = (CAO * CAO + 31) / 32;  // passes of 32 (b, c) columns
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int T = brick_tile(B, CAO, NMESH);
   const int T3 = T * SP;  // tile elements: T planes of pitch SP, rows of pitch SR
@@ -55,15 +57,15 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
   const int bz = bid % nb, by = (bid / nb) % nb, bx = bid / (nb * nb);
   const int o0 = bx * B, o1 = by * B, o2 = bz * B;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  // This lane's stencil points (tile offset, packed a/b/c), from the host
-  // table that assigns each lane the points of one shared-memory bank class
-  // (scatter_lane_table): the 32 atomics of one instruction hit 32 banks.
-  int loff[IT], labc[IT];
+  // This lane's stencil columns: tile offset b*SR + c and (b, c), or b < 0
+  // (scatter_lane_table).
+  int loff[NPASS], lb[NPASS], lc[NPASS];
 #pragma unroll
-  for (int it = 0; it < IT; it++) {
-    const int2 e = lanetab[it * 32 + lane];
-    loff[it] = e.x;
-    labc[it] = e.y;
+  for (int ps = 0; ps < NPASS; ps++) {
+    const int4 e = lanetab[ps * 32 + lane];
+    loff[ps] = e.x;
+    lb[ps] = e.y;
+    lc[ps] = e.z;
   }
   for (int pc = p0; pc < p1; pc += SCATTER_CHUNK) {
     const int cnt = min(SCATTER_CHUNK, p1 - pc);
@@ -100,12 +102,16 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
       const real *wv = sw + (size_t)v * 3 * CAO;
       real *tile = (NMESH == 2 && (v & 1)) ? tile1 : tile0;
       real *org = tile + soff[v];
+      real wx[CAO];
 #pragma unroll
-      for (int it = 0; it < IT; it++) {
-        if (labc[it] >= 0) {
-          const int abc = labc[it];
-          const real val = (wv[abc >> 16] * wv[CAO + ((abc >> 8) & 0xff)]) * wv[2 * CAO + (abc & 0xff)];
-          atomicAdd(org + loff[it], val);
+      for (int a = 0; a < CAO; a++) wx[a] = wv[a];
+#pragma unroll
+      for (int ps = 0; ps < NPASS; ps++) {
+        if (lb[ps] >= 0) {
+          const real wyz = wv[CAO + lb[ps]] * wv[2 * CAO + lc[ps]];
+          real *col = org + loff[ps];
+#pragma unroll
+          for (int a = 0; a < CAO; a++) atomicAdd(col + a * SP, wx[a] * wyz);
         }
       }
     }
@@ -323,64 +329,44 @@ __global__ void self_force_kernel(const double *__restrict__ x, const double *__
 
 // ---------------------------------------------------------------- launch
 
-// Row and plane pitches of the scatter tile (in elements) such that the
-// CAO^3 stencil offsets split evenly over the shared-memory bank classes
-// (32 for 4-byte, 16 for 8-byte elements): searched once per shape.
-inline void scatter_pitch(int cao, int T, int word_bytes, int *SRo, int *SPo) {
-  static int cache[8][32][2][2];
-  static bool have[8][32][2];
-  const int wi = word_bytes == 8 ? 1 : 0;
-  if (cao < 8 && T < 32 && have[cao][T][wi]) {
-    *SRo = cache[cao][T][wi][0];
-    *SPo = cache[cao][T][wi][1];
-    return;
-  }
-  const int R = 32 / (word_bytes / 4), nsplit = 32 / R, S = cao * cao * cao;
-  int best_m = 1 << 30, best_mem = 1 << 30, bSR = T, bSP = T * T;
-  for (int SR = T; SR <= T + 8; SR++)
-    for (int SP = T * SR; SP <= T * SR + 32; SP++) {
-      int counts[32] = {0}, seen[32] = {0};
-      for (int sp = 0; sp < S; sp++) {
-        const int a = sp / (cao * cao), b = (sp / cao) % cao, cc = sp % cao;
-        const int cls = (a * SP + b * SR + cc) % R;
-        counts[cls + R * (seen[cls] % nsplit)]++;
-        seen[cls]++;
-      }
-      int mx = 0;
-      for (int l = 0; l < 32; l++) mx = counts[l] > mx ? counts[l] : mx;
-      if (mx < best_m || (mx == best_m && SP * T < best_mem)) {
-        best_m = mx;
-        best_mem = SP * T;
-        bSR = SR;
-        bSP = SP;
-      }
+// Lane table of the scatter for row pitch SR: entry ps*32 + lane = (b*SR + c,
+// b, c, 0) of the (b, c) stencil column that lane owns in pass ps, or
+// (0, -1, 0, 0).  Columns are placed greedily in (b, c) order on the first
+// free lane of their bank class (b*SR + c modulo 32 for 4-byte elements;
+// modulo 16 in each half-warp for 8-byte elements, which are served 16
+// lanes at a time).  Returns false when some column finds no lane.
+inline bool scatter_lane_table(int cao, int SR, int word_bytes, int4 *tab) {
+  const int npass = (cao * cao + 31) / 32;
+  const int R = word_bytes == 8 ? 16 : 32;
+  for (int e = 0; e < 32 * npass; e++) tab[e] = make_int4(0, -1, 0, 0);
+  for (int b = 0; b < cao; b++)
+    for (int cc = 0; cc < cao; cc++) {
+      const int off = b * SR + cc, cls = off % R;
+      bool placed = false;
+      for (int ps = 0; ps < npass && !placed; ps++)
+        for (int h = 0; h < 32 / R && !placed; h++) {
+          int4 &e = tab[ps * 32 + cls + h * R];
+          if (e.y < 0) {
+            e = make_int4(off, b, cc, 0);
+            placed = true;
+          }
+        }
+      if (!placed) return false;
     }
-  if (cao < 8 && T < 32) {
-    cache[cao][T][wi][0] = bSR;
-    cache[cao][T][wi][1] = bSP;
-    have[cao][T][wi] = true;
-  }
-  *SRo = bSR;
-  *SPo = bSP;
+  return true;
 }
 
-// Lane table of the scatter: entry it*32 + lane = (tile offset a*SP + b*SR
-// + c, (a << 16) | (b << 8) | c) of the it-th stencil point of that lane,
-// or (0, -1).  Lane l takes the points whose offset is congruent to l modulo
-// the number of bank classes R (32 for 4-byte, 16 for 8-byte elements;
-// with 8-byte elements lanes l and l + 16 alternate over one class).
-inline void scatter_lane_table(int cao, int SR, int SP, int word_bytes, int2 *tab) {
-  const int R = 32 / (word_bytes / 4), nsplit = 32 / R, S = cao * cao * cao, IT = (S + 31) / 32;
-  int fill[32] = {0}, seen[32] = {0};
-  for (int e = 0; e < 32 * IT; e++) tab[e] = make_int2(0, -1);
-  for (int sp = 0; sp < S; sp++) {
-    const int a = sp / (cao * cao), b = (sp / cao) % cao, cc = sp % cao;
-    const int off = a * SP + b * SR + cc;
-    const int cls = off % R;
-    const int lane = cls + R * (seen[cls] % nsplit);
-    seen[cls]++;
-    if (fill[lane] < IT) tab[fill[lane]++ * 32 + lane] = make_int2(off, (a << 16) | (b << 8) | cc);
-  }
+// Smallest row pitch >= T with a conflict-free lane table (plane pitch
+// T * SR); searched once per shape.
+inline int scatter_row_pitch(int cao, int T, int word_bytes) {
+  static int cache[8][64][2];
+  const int wi = word_bytes == 8 ? 1 : 0;
+  if (cao < 8 && T < 64 && cache[cao][T][wi]) return cache[cao][T][wi];
+  int4 tab[64];
+  int sr = T;
+  while (sr < T + 64 && !scatter_lane_table(cao, sr, word_bytes, tab)) sr++;
+  if (cao < 8 && T < 64) cache[cao][T][wi] = sr;
+  return sr;
 }
 
 template <typename real, int CAO, int NMESH>
@@ -400,14 +386,14 @@ int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
   mark(c, EV_K2);
   if (!c->scatter_tab) {
     // built once per context, on its first (eager, uncaptured) step
-    const int IT = (CAO * CAO * CAO + 31) / 32;
-    int2 host[32 * 16];
-    scatter_lane_table(CAO, SR, SP, (int)sizeof(real), host);
-    P3MG_CUDA_TRY(cudaMalloc(&c->scatter_tab, sizeof(int2) * 32 * IT));
-    P3MG_CUDA_TRY(cudaMemcpy(c->scatter_tab, host, sizeof(int2) * 32 * IT, cudaMemcpyHostToDevice));
+    constexpr int NPASS = (CAO * CAO + 31) / 32;
+    int4 host[32 * NPASS];
+    if (!scatter_lane_table(CAO, SR, (int)sizeof(real), host)) return P3MG_ERR_MESH;
+    P3MG_CUDA_TRY(cudaMalloc(&c->scatter_tab, sizeof(int4) * 32 * NPASS));
+    P3MG_CUDA_TRY(cudaMemcpy(c->scatter_tab, host, sizeof(int4) * 32 * NPASS, cudaMemcpyHostToDevice));
   }
   kern<<<nbr, ASSIGN_THREADS, smem, c->stream>>>(c->sorted_xyzq, c->brick_start, c->mesh, c->brick, c->nbrick1, Hi,
-                                                shift, SR, SP, reinterpret_cast<const int2 *>(c->scatter_tab),
+                                                shift, SR, SP, reinterpret_cast<const int4 *>(c->scatter_tab),
                                                 reinterpret_cast<C *>(c->Q));
   c->launches++;
   mark(c, EV_K3);
@@ -419,8 +405,7 @@ template <typename real, int CAO>
 int dispatch_scatter(Ctx *c) {
   const int nmesh = method_interlaced(c->method) ? 2 : 1;
   const int T = brick_tile(c->brick, CAO, nmesh);
-  int SR, SP;
-  scatter_pitch(CAO, T, (int)sizeof(real), &SR, &SP);
+  const int SR = scatter_row_pitch(CAO, T, (int)sizeof(real)), SP = T * SR;
   const size_t tile = (size_t)nmesh * T * SP * sizeof(real);
   if (nmesh == 2) return launch_scatter<real, CAO, 2>(c, tile + scatter_stage_bytes<real, CAO, 2>(), SR, SP);
   return launch_scatter<real, CAO, 1>(c, tile + scatter_stage_bytes<real, CAO, 1>(), SR, SP);
