@@ -271,6 +271,43 @@ int p3mg_ewald_reference(p3mg_ctx *ctx, int nt, const int *targets, double *f_x,
 int p3mg_ewald_kspace_forces(p3mg_ctx *ctx, double alpha, int kmax, int nt, const int *targets, double *fk_x,
                              double *fk_y, double *fk_z);
 
+/* Inhomogeneous k-space error estimate of the context's particles
+ * (Generic_error_estimate_inhomo, p3m-common.c:437-719, the "inhomo_error"
+ * column of main.c:436-447), in FP64 on the GPU:
+ *   mesh, cao: the estimator's mesh and window order (main.c "inhomo_mesh",
+ *     "inhomo_cao"; mesh 4 .. 512 with prime factors 2, 3, 5, 7 only);
+ *   mc: alias range (main.c "inhomo_mc", 0 .. 10); with mc = 0 the kernel
+ *     is U2 G_opt - Ghat with an alias-free G_opt, which vanishes up to
+ *     rounding, as in the reference;
+ *   uniform: rho^2 = sum q^2 / mesh^3 instead of the assigned q_i^2
+ *     ("inhomo_uniform");
+ *   collect_mesh, collect_cao: mesh spacing L/collect_mesh, stencil shift
+ *     and stencil length of the final interpolation at the particles.  The
+ *     reference uses the force method's mesh and cao there
+ *     (charge-assign.c:1650-1705 called with the method's parameters);
+ *     pass the estimator's own values for a self-consistent estimate.
+ *     Window weights past the estimator's order count as 0 (the reference
+ *     reads past its table rows there).  Indices wrap modulo mesh (the
+ *     reference wraps once, which is the same whenever collect_mesh <
+ *     2 mesh and collect_cao <= mesh).
+ *   estimate: sqrt(sum_i rms_i / n);
+ *   mesh_out (host, 5 mesh^3 doubles, may be NULL): per mesh point
+ *     (index (i*mesh + j)*mesh + k) rho^2, Re and Im of the error density,
+ *     Re and Im of DFT(K^2): the columns of the reference's "inhomo_output"
+ *     file (p3m-common.c:683-696). */
+int p3mg_inhomo_error(p3mg_ctx *ctx, double alpha, int uniform, int mesh, int cao, int mc, int collect_mesh,
+                      int collect_cao, double *estimate, double *mesh_out);
+
+/* Error map (Error_map, p3m-common.c:402-435, main.c "error_map"): the
+ * squared k-space force error |ref - fk|^2 of each particle of the context
+ * assigned to a mesh of `mesh` points per side with the window of order
+ * cao (1 .. 7).  fk_* and ref_* are host arrays of n doubles; map (host,
+ * mesh^3 doubles, index (i*mesh + j)*mesh + k) receives the mesh;
+ * totals (may be NULL) = {sum of the particles' squared errors, sum over
+ * the mesh} (the reference prints both). */
+int p3mg_error_map(p3mg_ctx *ctx, int mesh, int cao, const double *fk_x, const double *fk_y, const double *fk_z,
+                   const double *ref_x, const double *ref_y, const double *ref_z, double *map, double totals[2]);
+
 /* Copy the FP64 influence function (mesh^3 doubles, full mesh, index
  * (i*mesh + j)*mesh + k as r_ind, p3m-common.h:25) and the 81 ad self-force
  * coefficients (zeros for other methods) to host memory; either may be NULL. */

@@ -60,6 +60,10 @@ def lib():
                                                                ctypes.c_double]
         L.oracle_kspace_error.restype = ctypes.c_double
         L.oracle_bspline.argtypes = [ctypes.c_int, ctypes.c_double, _dp, _dp]
+        L.oracle_inhomo_error.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double] * 2 + [ctypes.c_int] * 6 + [
+            _dp, _dp]
+        L.oracle_error_map.argtypes = [ctypes.c_int] + [_dp] * 3 + [ctypes.c_double, _dp, _dp, ctypes.c_int,
+                                                                   ctypes.c_int, _dp]
         _lib = L
     return _lib
 
@@ -88,6 +92,12 @@ def ref():
         R.ref_find_error.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         R.ref_find_error.restype = ctypes.c_double
         R.ref_realteil.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double] * 3 + [_dp, _dp]
+        R.ref_inhomo_error.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                                                    ctypes.c_double] + [ctypes.c_int] * 4 + [
+            ctypes.c_char_p]
+        R.ref_inhomo_error.restype = ctypes.c_double
+        R.ref_error_map.argtypes = [ctypes.c_int] + [_dp] * 3 + [ctypes.c_double, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                                                _dp]
         _ref = R
     return _ref
 
@@ -211,6 +221,31 @@ def realspace_error(n, q2, L, rcut, alpha):
     return lib().oracle_realspace_error(n, q2, L, rcut, alpha)
 
 
+def inhomo_error(x, y, z, q, L, alpha, uniform, mesh, cao, mc, collect_mesh, collect_cao, want_meshes=False):
+    """Inhomogeneous k-space error estimate; with want_meshes also the
+    (mesh^3, 5) columns rho2, Re E, Im E, Re K2(k), Im K2(k)."""
+    x, y, z, q = map(_arr, (x, y, z, q))
+    est = np.zeros(1)
+    out = np.zeros((mesh ** 3, 5)) if want_meshes else None
+    rc = lib().oracle_inhomo_error(len(x), _ptr(x), _ptr(y), _ptr(z), _ptr(q), L, alpha, int(uniform), mesh, cao, mc,
+                                   collect_mesh, collect_cao, _ptr(est), _ptr(out))
+    if rc:
+        raise ValueError("oracle_inhomo_error failed (%d)" % rc)
+    return (float(est[0]), out) if want_meshes else float(est[0])
+
+
+def error_map(x, y, z, L, fk, fk_ref, mesh, cao):
+    """Squared k-space force error per particle assigned to a mesh (mesh^3)."""
+    x, y, z = map(_arr, (x, y, z))
+    fk = _arr(np.asarray(fk).reshape(-1))
+    fk_ref = _arr(np.asarray(fk_ref).reshape(-1))
+    out = np.zeros(mesh ** 3)
+    rc = lib().oracle_error_map(len(x), _ptr(x), _ptr(y), _ptr(z), L, _ptr(fk), _ptr(fk_ref), mesh, cao, _ptr(out))
+    if rc:
+        raise ValueError("oracle_error_map failed (%d)" % rc)
+    return out
+
+
 # ------------------------------------------------------------ the reference
 
 def ref_forces(method, mesh, cao, mc, alpha, rcut, x, y, z, q, L, tuning=False, want_G=False):
@@ -267,6 +302,21 @@ def ref_error_estimates(method, mesh, cao, mc, alpha, rcut, q, L):
 
 def ref_find_error(alphaL, mesh, cao, method):
     return ref().ref_find_error(alphaL, mesh, cao, method)
+
+
+def ref_inhomo_error(x, y, z, q, L, method_mesh, method_cao, alpha, uniform, mesh, cao, mc, out_file=None):
+    x, y, z, q = map(_arr, (x, y, z, q))
+    return ref().ref_inhomo_error(len(x), _ptr(x), _ptr(y), _ptr(z), _ptr(q), L, method_mesh, method_cao, alpha,
+                                  int(uniform), mesh, cao, mc, out_file.encode() if out_file else None)
+
+
+def ref_error_map(x, y, z, L, fk, fk_ref, mesh, cao):
+    x, y, z = map(_arr, (x, y, z))
+    fk = _arr(np.asarray(fk).reshape(-1))
+    fk_ref = _arr(np.asarray(fk_ref).reshape(-1))
+    out = np.zeros(mesh ** 3)
+    ref().ref_error_map(len(x), _ptr(x), _ptr(y), _ptr(z), L, _ptr(fk), _ptr(fk_ref), mesh, cao, _ptr(out))
+    return out
 
 
 def estimate_table_mesh(mesh):

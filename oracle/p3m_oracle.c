@@ -790,3 +790,235 @@ double oracle_kspace_error(int method, int m, int cao, int mc_est, double alpha,
   }
   return 2.0 * q2 * sqrt(he / (double)n) / SQ(L);
 }
+
+/* ------------------------------------- inhomogeneous estimate and error map */
+
+/* signed index of a DFT bin: i - m for i >= m/2 (p3m-common.c:494-499) */
+static int half_signed(int i, int m) { return (i >= m / 2) ? i - m : i; }
+
+/* (sinc(a/m) sinc(b/m) sinc(c/m))^e (p3m-common.c:351-357, U and U2) */
+static double window_hat(int a, int b, int c, int m, int e) {
+  return pow(sinc_pi((double)a / m) * sinc_pi((double)b / m) * sinc_pi((double)c / m), e);
+}
+
+/* Influence function of the estimator: the B/A ratio of p3m-common.c:359-392
+ * with no alias images (mc = 0), B = U2 Ghat k^2, A = U2 (k^2 U2), together
+ * with Ghat = 4 pi/k^2 exp(-k^2/(4 alpha^2)) (p3m-common.c:310-313) and U2. */
+static double inhomo_gopt(int a, int b, int c, int m, int cao, double alpha, double L, double *ghat, double *u2) {
+  const double k2 = SQ(2.0 * ORC_PI / L) * (SQ((double)a) + SQ((double)b) + SQ((double)c));
+  const double g = (4 * ORC_PI / k2) * exp(-k2 / (4 * alpha * alpha));
+  const double w2 = window_hat(a, b, c, m, 2 * cao);
+  *ghat = g;
+  *u2 = w2;
+  return (w2 * g * k2) / (w2 * (k2 * w2));
+}
+
+/* B-spline weights of order tab_cao at the tabulated offset of one
+ * coordinate, read for `count` stencil points: entries past the table's
+ * order are 0 here (the reference reads past its table rows there,
+ * interpol.c:38-44). */
+static void inhomo_stencil(double xc, double Hi, double shift, int m, int tab_cao, int count, int *base, double *w) {
+  double pos = xc * Hi - shift;
+  int nmp = (int)floor(pos + 0.5);
+  int b = nmp % m;
+  *base = b < 0 ? b + m : b;
+  int arg = (int)floor((pos - nmp + 0.5) * 131072.0);
+  double wt[8] = {0};
+  oracle_bspline(tab_cao, (double)(arg - 65536) / 131072.0, wt, NULL);
+  for (int j = 0; j < count; j++) w[j] = (j < tab_cao) ? wt[j] : 0.0;
+}
+
+/* Generic_error_estimate_inhomo (p3m-common.c:437-719).
+ *
+ * Mesh `mesh`, window order `cao`:
+ *   rho2(r) = sum_i q_i^2 W(r - x_i)  (assign_charge_q2, charge-assign.c:1544-1590),
+ *             or sum q^2 / mesh^3 everywhere with `uniform`;
+ *   K_d(k) = -2 pi i k_d/L (U2 G_opt - Ghat)  (homogeneous part, :489-534);
+ *   for each alias vector a in [-mc, mc]^3 without 0 (:558-625):
+ *     K_d^a(k2) = -i (k2_d/L) 2 pi U(k2) U(-k2 - a m) G_opt(k2)
+ *                 * sum_{k != 0} (k_d/L) 2 pi U(k) U(k + a m) G_opt(k)
+ *     (the reference adds the product term by term over k for every k2; the
+ *      sum over k factors out and is formed once here);
+ *   K2(r) = sum_d Re(IDFT K_d)^2 + sum_a sum_d Re(IDFT K_d^a)^2;
+ *   E = IDFT[DFT(rho2) * DFT(K2)], the product taken component by component
+ *       (re*re, im*im) as at :664-672;
+ *   rms_i = q_i^2 sum_stencil W E  (collect_rms_nocf, charge-assign.c:1650-1705)
+ *           with the mesh spacing and stencil length of collect_mesh and
+ *           collect_cao (the reference passes its force-method parameters
+ *           there) and the window table of order cao;
+ *   estimate = sqrt(sum_i rms_i / n).
+ * DFTs unnormalised.  mesh_out (5 mesh^3 doubles, may be NULL) receives per
+ * mesh point rho2, Re E, Im E, Re DFT(K2), Im DFT(K2) (the columns of the
+ * reference's inhomo_output file, :688-692). */
+int oracle_inhomo_error(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                        double alpha, int uniform, int mesh, int cao, int mc, int collect_mesh, int collect_cao,
+                        double *estimate, double *mesh_out) {
+  if (mesh < 2 || cao < 1 || cao > 7 || collect_cao < 1 || collect_cao > 7 || collect_mesh < 1 || mc < 0 || n < 0)
+    return -1;
+  const int m = mesh;
+  const size_t M = (size_t)m * m * m;
+  double *rho2 = (double *)calloc(2 * M, sizeof(double));
+  double *E = (double *)calloc(2 * M, sizeof(double));
+  double *K2 = (double *)calloc(2 * M, sizeof(double));
+  double *Kd = (double *)calloc(6 * M, sizeof(double));
+  double *gopt = (double *)malloc(M * sizeof(double));
+  double *uw = (double *)malloc(M * sizeof(double));
+  int dims[3] = {m, m, m};
+  int base[3];
+  double w[3][8];
+
+  if (!uniform) {
+    const double Hi = (double)m / L, shift = (double)((cao - 1) / 2);
+    for (int i = 0; i < n; i++) {
+      const double c[3] = {x[i], y[i], z[i]};
+      for (int d = 0; d < 3; d++) inhomo_stencil(c[d], Hi, shift, m, cao, cao, &base[d], w[d]);
+      const double q2 = SQ(q[i]);
+      for (int a = 0; a < cao; a++) {
+        const int I = (base[0] + a) % m;
+        const double t0 = q2 * w[0][a];
+        for (int b = 0; b < cao; b++) {
+          const int J = (base[1] + b) % m;
+          const double t1 = t0 * w[1][b];
+          for (int cc = 0; cc < cao; cc++) rho2[cidx(I, J, (base[2] + cc) % m, m)] += t1 * w[2][cc];
+        }
+      }
+    }
+  } else {
+    double q2 = 0.0;
+    for (int i = 0; i < n; i++) q2 += SQ(q[i]);
+    for (size_t t = 0; t < M; t++) rho2[2 * t] = q2 / (double)M;
+  }
+
+  /* homogeneous kernel, and G_opt / U per bin for the alias terms */
+  for (int i = 0; i < m; i++)
+    for (int j = 0; j < m; j++)
+      for (int k = 0; k < m; k++) {
+        const size_t t = ((size_t)i * m + j) * m + k;
+        const int tn[3] = {half_signed(i, m), half_signed(j, m), half_signed(k, m)};
+        gopt[t] = 0.0;
+        uw[t] = window_hat(tn[0], tn[1], tn[2], m, cao);
+        if (tn[0] == 0 && tn[1] == 0 && tn[2] == 0) continue;
+        double ghat, u2;
+        const double g = inhomo_gopt(tn[0], tn[1], tn[2], m, cao, alpha, L, &ghat, &u2);
+        gopt[t] = g;
+        const double kv = u2 * g - ghat;
+        for (int d = 0; d < 3; d++) Kd[2 * (d * M + t) + 1] = -2 * ORC_PI * tn[d] / L * kv;
+      }
+  for (int d = 0; d < 3; d++) oracle_dft_nd(Kd + 2 * d * M, 3, dims, +1);
+  for (size_t t = 0; t < M; t++) {
+    double kr = 0.0;
+    for (int d = 0; d < 3; d++) kr += SQ(Kd[2 * (d * M + t)]);
+    K2[2 * t] = kr;
+  }
+
+  /* alias terms */
+  for (int ax = -mc; ax <= mc; ax++)
+    for (int ay = -mc; ay <= mc; ay++)
+      for (int az = -mc; az <= mc; az++) {
+        if (ax == 0 && ay == 0 && az == 0) continue;
+        double S[3] = {0, 0, 0};
+        for (int i = 0; i < m; i++)
+          for (int j = 0; j < m; j++)
+            for (int k = 0; k < m; k++) {
+              const size_t t = ((size_t)i * m + j) * m + k;
+              const int tn[3] = {half_signed(i, m), half_signed(j, m), half_signed(k, m)};
+              if (tn[0] == 0 && tn[1] == 0 && tn[2] == 0) continue;
+              const double k1 = 2 * ORC_PI * uw[t] *
+                                window_hat(tn[0] + ax * m, tn[1] + ay * m, tn[2] + az * m, m, cao) * gopt[t];
+              for (int d = 0; d < 3; d++) S[d] += (tn[d] / L) * k1;
+            }
+        memset(Kd, 0, 6 * M * sizeof(double));
+        for (int i = 0; i < m; i++)
+          for (int j = 0; j < m; j++)
+            for (int k = 0; k < m; k++) {
+              const size_t t = ((size_t)i * m + j) * m + k;
+              const int tn[3] = {half_signed(i, m), half_signed(j, m), half_signed(k, m)};
+              if (tn[0] == 0 && tn[1] == 0 && tn[2] == 0) continue;
+              const double k2 = 2 * ORC_PI * uw[t] *
+                                window_hat(-tn[0] - ax * m, -tn[1] - ay * m, -tn[2] - az * m, m, cao) * gopt[t];
+              for (int d = 0; d < 3; d++) Kd[2 * (d * M + t) + 1] = -(tn[d] / L) * k2 * S[d];
+            }
+        for (int d = 0; d < 3; d++) oracle_dft_nd(Kd + 2 * d * M, 3, dims, +1);
+        for (size_t t = 0; t < M; t++) {
+          double kr = 0.0;
+          for (int d = 0; d < 3; d++) kr += SQ(Kd[2 * (d * M + t)]);
+          K2[2 * t] += kr;
+        }
+      }
+
+  oracle_dft_nd(K2, 3, dims, -1);
+  memcpy(E, rho2, 2 * M * sizeof(double));
+  oracle_dft_nd(E, 3, dims, -1);
+  for (size_t t = 0; t < 2 * M; t++) E[t] *= K2[t];
+  oracle_dft_nd(E, 3, dims, +1);
+
+  /* collect at the particles */
+  double sum = 0.0;
+  {
+    const double Hi = (double)collect_mesh / L, shift = (double)((collect_cao - 1) / 2);
+    for (int i = 0; i < n; i++) {
+      const double c[3] = {x[i], y[i], z[i]};
+      for (int d = 0; d < 3; d++) inhomo_stencil(c[d], Hi, shift, m, cao, collect_cao, &base[d], w[d]);
+      const double q2 = SQ(q[i]);
+      double r = 0.0;
+      for (int a = 0; a < collect_cao; a++) {
+        const int I = (base[0] + a) % m;
+        const double t0 = q2 * w[0][a];
+        for (int b = 0; b < collect_cao; b++) {
+          const int J = (base[1] + b) % m;
+          const double t1 = t0 * w[1][b];
+          for (int cc = 0; cc < collect_cao; cc++) r += E[cidx(I, J, (base[2] + cc) % m, m)] * (t1 * w[2][cc]);
+        }
+      }
+      sum += r;
+    }
+  }
+  *estimate = sqrt(sum / n);
+  if (mesh_out)
+    for (size_t t = 0; t < M; t++) {
+      mesh_out[5 * t + 0] = rho2[2 * t];
+      mesh_out[5 * t + 1] = E[2 * t];
+      mesh_out[5 * t + 2] = E[2 * t + 1];
+      mesh_out[5 * t + 3] = K2[2 * t];
+      mesh_out[5 * t + 4] = K2[2 * t + 1];
+    }
+  free(rho2);
+  free(E);
+  free(K2);
+  free(Kd);
+  free(gopt);
+  free(uw);
+  return 0;
+}
+
+/* Error_map (p3m-common.c:402-435): the squared k-space force error of
+ * each particle, |fk_ref - fk|^2, assigned to a mesh of `mesh` points per
+ * side with the window of order cao (assign_charge_nocf,
+ * charge-assign.c:1592-1648).  fk and fk_ref are 3n arrays; map receives
+ * mesh^3 doubles (the real parts of the reference's complex mesh). */
+int oracle_error_map(int n, const double *x, const double *y, const double *z, double L, const double *fk,
+                     const double *fk_ref, int mesh, int cao, double *map) {
+  if (mesh < 1 || cao < 1 || cao > 7 || n < 0) return -1;
+  const int m = mesh;
+  const size_t M = (size_t)m * m * m;
+  memset(map, 0, M * sizeof(double));
+  const double Hi = (double)m / L, shift = (double)((cao - 1) / 2);
+  int base[3];
+  double w[3][8];
+  for (int i = 0; i < n; i++) {
+    double dF = 0.0;
+    for (int d = 0; d < 3; d++) dF += SQ(fk_ref[(size_t)d * n + i] - fk[(size_t)d * n + i]);
+    const double c[3] = {x[i], y[i], z[i]};
+    for (int d = 0; d < 3; d++) inhomo_stencil(c[d], Hi, shift, m, cao, cao, &base[d], w[d]);
+    for (int a = 0; a < cao; a++) {
+      const int I = (base[0] + a) % m;
+      const double t0 = dF * w[0][a];
+      for (int b = 0; b < cao; b++) {
+        const int J = (base[1] + b) % m;
+        const double t1 = t0 * w[1][b];
+        for (int cc = 0; cc < cao; cc++) map[((size_t)I * m + J) * m + (base[2] + cc) % m] += t1 * w[2][cc];
+      }
+    }
+  }
+  return 0;
+}

@@ -23,5 +23,10 @@ double oracle_rms_error(int n, const double *f, const double *ref);
 double oracle_realspace_error(int n, double q2, double L, double rcut, double alpha);
 int oracle_estimate_table_mesh(int mesh);
 double oracle_kspace_error(int method, int mesh, int cao, int mc_est, double alpha, int n, double q2, double L);
+int oracle_inhomo_error(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                        double alpha, int uniform, int mesh, int cao, int mc, int collect_mesh, int collect_cao,
+                        double *estimate, double *mesh_out);
+int oracle_error_map(int n, const double *x, const double *y, const double *z, double L, const double *fk,
+                     const double *fk_ref, int mesh, int cao, double *map);
 
 #endif

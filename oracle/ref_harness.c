@@ -227,3 +227,44 @@ int ref_realteil(int n, const double *x, const double *y, const double *z, const
   Free_system(s);
   return 0;
 }
+
+/* The reference's inhomogeneous estimate (p3m-common.c:437-719) as main.c
+ * calls it (main.c:436-440): `p` carries the force method's mesh, cao and
+ * alpha; mesh/cao/mc are the estimator's own. */
+double ref_inhomo_error(int n, const double *x, const double *y, const double *z, const double *q, double L,
+                        int method_mesh, int method_cao, double alpha, int uniform, int mesh, int cao, int mc,
+                        const char *out_file) {
+  system_t *s = make_system(n, x, y, z, q, L);
+  parameters_t p;
+  memset(&p, 0, sizeof(p));
+  p.mesh = method_mesh;
+  p.cao = method_cao;
+  p.cao3 = method_cao * method_cao * method_cao;
+  p.ip = method_cao - 1;
+  p.alpha = alpha;
+  const double r = Generic_error_estimate_inhomo(s, &p, uniform, mesh, cao, mc, (char *)out_file, NULL);
+  Free_system(s);
+  return r;
+}
+
+/* The reference's Error_map (p3m-common.c:402-435): fk, fk_ref 3n each;
+ * map receives the real parts of its mesh^3 complex mesh. */
+int ref_error_map(int n, const double *x, const double *y, const double *z, double L, const double *fk,
+                  const double *fk_ref, int mesh, int cao, double *map) {
+  double *zero = (double *)calloc((size_t)n + 1, sizeof(double));
+  system_t *s = make_system(n, x, y, z, zero, L);
+  forces_t *f = Init_forces(n), *fr = Init_forces(n);
+  for (int d = 0; d < 3; d++) {
+    memcpy(f->f_k->fields[d], fk + (size_t)d * n, sizeof(double) * n);
+    memcpy(fr->f_k->fields[d], fk_ref + (size_t)d * n, sizeof(double) * n);
+  }
+  double *em = Error_map(s, f, fr, mesh, cao);
+  const size_t M = (size_t)mesh * mesh * mesh;
+  for (size_t t = 0; t < M; t++) map[t] = em[2 * t];
+  FFTW_FREE(em);
+  Free_forces(f);
+  Free_forces(fr);
+  Free_system(s);
+  free(zero);
+  return 0;
+}

@@ -586,6 +586,21 @@ extern "C" int p3mg_estimate_errors(int method_id, int mesh, int cao, int mc_est
   return error_estimates(method_id, mesh, cao, n, L, q2, alpha, rcut, mc_est, cudaStreamPerThread, nullptr, est);
 }
 
+extern "C" int p3mg_inhomo_error(p3mg_ctx *h, double alpha, int uniform, int mesh, int cao, int mc,
+                                 int collect_mesh, int collect_cao, double *estimate, double *mesh_out) {
+  if (!h) return P3MG_ERR_ARG;
+  return inhomo_error(&h->c, alpha, uniform, mesh, cao, mc, collect_mesh, collect_cao, estimate, mesh_out);
+}
+
+extern "C" int p3mg_error_map(p3mg_ctx *h, int mesh, int cao, const double *fk_x, const double *fk_y,
+                              const double *fk_z, const double *ref_x, const double *ref_y, const double *ref_z,
+                              double *map, double totals[2]) {
+  if (!h) return P3MG_ERR_ARG;
+  const double *fk[3] = {fk_x, fk_y, fk_z};
+  const double *ref[3] = {ref_x, ref_y, ref_z};
+  return error_map(&h->c, mesh, cao, fk, ref, map, totals);
+}
+
 extern "C" int p3mg_alpha_range(double alphamin, double alphamax, double alphastep, int cap, double *alphas) {
   if (!(alphastep > 0.0) || !isfinite(alphamin) || !isfinite(alphamax) || cap < 0) return P3MG_ERR_ARG;
   // the reference's loop: alpha accumulated in double (main.c:375)

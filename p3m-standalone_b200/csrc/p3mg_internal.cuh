@@ -11,6 +11,8 @@
 #define P3MG_PI 3.14159265358979323846264338327950288
 #define P3MG_MAX_MESH 512
 #define P3MG_MAX_CAO 7
+// largest alias range of the inhomogeneous error estimate ((2 mc + 1)^3 - 1 alias vectors)
+#define P3MG_MAX_INHOMO_MC 10
 // tabulated in-cell offset resolution of the reference: 2*MaxInterpol
 // = 131072 bins per mesh spacing (interpol.h:149, charge-assign.c:156)
 #define P3MG_NINTERP 131072
@@ -170,6 +172,12 @@ int free_all(Ctx *c);
 int fft_plan_init(Ctx *c);
 void fft_plan_free(Ctx *c);
 int fft3d(Ctx *c, void *data, int nbatch, int sign);
+int fft_factor(int m, int *radix, int *npass);  // 0 when m factors into 2, 3, 4, 5, 7
+
+// inhomogeneous error estimate and error map (p3mg_inhomo.cu)
+int inhomo_error(Ctx *c, double alpha, int uniform, int mesh, int cao, int mc, int collect_mesh, int collect_cao,
+                 double *estimate, double *mesh_out);
+int error_map(Ctx *c, int mesh, int cao, const double *fk[3], const double *ref[3], double *map, double totals[2]);
 
 // influence (p3mg_influence.cu)
 int influence_compute(Ctx *c, double alpha);

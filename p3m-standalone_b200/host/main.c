@@ -17,9 +17,13 @@
  * forces); "tune" with "prec" picks mesh, cao (cao 0: any; otherwise that
  * cao) and alpha with the reference's tuning search (tuning.c:250-370,
  * which the reference's main parses but never runs) timed on the GPU, then
- * runs that single alpha.  Parameters the reference parses for its
- * analysis side paths (rdf, rdf_species, cdf, inhomo_error, error_map) are
- * accepted and reported as not provided here. */
+ * runs that single alpha.  "inhomo_error" (with inhomo_mesh, inhomo_cao,
+ * inhomo_mc, inhomo_uniform, inhomo_output) fills the err_inhomo column
+ * from the inhomogeneous estimate on the GPU (main.c:436-440), and
+ * "error_map" (with error_k, error_map_mesh, error_map_cao) writes
+ * error_map.dat and error_map_2d.dat (main.c:403-424).  Parameters the
+ * reference parses for its other analysis side paths (rdf, rdf_species,
+ * cdf) are accepted and reported as not provided here. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -70,6 +74,76 @@ static double min_distance(const system_t *s) {
       if (r2 < best) best = r2;
     }
   return sqrt(best);
+}
+
+/* Error map of the k-space forces against the Ewald k-space forces
+ * (main.c:403-424, Error_map p3m-common.c:402-435): error_map.dat holds every
+ * mesh point, error_map_2d.dat the plane nx = 0.5 mesh. */
+static void write_error_map(data_t *data, const forces_t *f, const forces_t *f_ref, int mesh, int cao) {
+  puts("Writing error map.");
+  const size_t M = (size_t)mesh * mesh * mesh;
+  double *map = (double *)malloc((M > 0 ? M : 1) * sizeof(double));
+  if (!map) {
+    fputs("out of memory\n", stderr);
+    exit(1);
+  }
+  double totals[2] = {0.0, 0.0};
+  const int st = p3mg_error_map(data->ctx, mesh, cao, f->f_k->x, f->f_k->y, f->f_k->z, f_ref->f_k->x, f_ref->f_k->y,
+                                f_ref->f_k->z, map, totals);
+  if (st != P3MG_OK) p3m_host_die(st, "p3mg_error_map");
+  printf("dF_total %e dF_total_mesh %e\n", totals[0], totals[1]);
+  FILE *out = fopen("error_map.dat", "w");
+  FILE *out2d = fopen("error_map_2d.dat", "w");
+  if (!out || !out2d) {
+    fputs("Could not open error_map.dat / error_map_2d.dat for writing.\n", stderr);
+    exit(127);
+  }
+  const int plane = (int)(0.5 * mesh);
+  printf("2d cut plane is nx = %d\n", plane);
+  for (int i = 0; i < mesh; i++)
+    for (int j = 0; j < mesh; j++)
+      for (int k = 0; k < mesh; k++) {
+        const double v = map[((size_t)i * mesh + j) * mesh + k];
+        fprintf(out, "%d %d %d %e\n", i, j, k, v);
+        if (i == plane) fprintf(out2d, "%d %d %e\n", j, k, v);
+      }
+  fclose(out);
+  fclose(out2d);
+  free(map);
+}
+
+/* Inhomogeneous error estimate as main.c:436-440 calls it: the estimator's
+ * mesh, cao and alias range, with the force method's mesh and cao for the
+ * final interpolation (collect_rms_nocf gets the method's parameters there).
+ * With out_file, one line per mesh point as p3m-common.c:683-692 writes. */
+static double inhomo_estimate(data_t *data, const parameters_t *p, int uniform, int mesh, int cao, int mc,
+                              const char *out_file) {
+  double est = 0.0;
+  double *cols = NULL;
+  const size_t M = (size_t)mesh * mesh * mesh;
+  if (out_file) {
+    cols = (double *)malloc(5 * (M > 0 ? M : 1) * sizeof(double));
+    if (!cols) {
+      fputs("out of memory\n", stderr);
+      exit(1);
+    }
+  }
+  const int st = p3mg_inhomo_error(data->ctx, p->alpha, uniform, mesh, cao, mc, p->mesh, p->cao, &est, cols);
+  if (st != P3MG_OK) p3m_host_die(st, "p3mg_inhomo_error");
+  if (out_file) {
+    FILE *f = fopen(out_file, "w");
+    if (f) {
+      for (int i = 0; i < mesh; i++)
+        for (int j = 0; j < mesh; j++)
+          for (int k = 0; k < mesh; k++) {
+            const double *c = cols + 5 * (((size_t)i * mesh + j) * mesh + k);
+            fprintf(f, "%d %d %d %e %e %e %e %e %e\n", i, j, k, c[0], c[1], c[2], c[3], c[4], c[1] * c[0]);
+          }
+      fclose(f);
+    }
+    free(cols);
+  }
+  return est;
 }
 
 int main(int argc, char **argv) {
@@ -164,7 +238,7 @@ int main(int argc, char **argv) {
     exit(1);
   }
 
-  static const char *const side_paths[] = {"rdf", "rdf_species", "cdf", "inhomo_error", "error_map"};
+  static const char *const side_paths[] = {"rdf", "rdf_species", "cdf"};
   for (size_t i = 0; i < sizeof side_paths / sizeof side_paths[0]; i++)
     if (param_isset(side_paths[i], &params))
       fprintf(stderr, "Note: '%s' is not provided by this program; ignored.\n", side_paths[i]);
@@ -312,6 +386,7 @@ int main(int argc, char **argv) {
           error_k += dv * dv;
         }
       error_k = sqrt(error_k) / sqrt((double)n);
+      if (param_isset("error_map", &params)) write_error_map(data, forces, forces_ewald, error_map_mesh, error_map_cao);
     }
 
     const double ewald_error_k_est = ewald_error_k_estimate(system, &parameters, parameters.alpha);
@@ -331,7 +406,10 @@ int main(int argc, char **argv) {
       estimate = method->Error(system, &parameters);
       error_k_est = method->Error_k(system, &parameters);
     }
-    const double err_inhomo = 0.0;
+    double err_inhomo = 0.0;
+    if (param_isset("inhomo_error", &params))
+      err_inhomo = inhomo_estimate(data, &parameters, param_isset("inhomo_uniform", &params), inhomo_mesh, inhomo_cao,
+                                   inhomo_mc, param_isset("inhomo_output", &params) ? inhomo_output : NULL);
     const double rs_error = Realspace_error(system, &parameters);
 
     printf("%8lf\t%8e\t%8e\t %8e %8e\t %8e sec\t %8e %8e\n", parameters.alpha, ef / sqrt((double)n), estimate,

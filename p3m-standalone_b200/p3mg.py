@@ -19,6 +19,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 OK = 0
+# status codes of include/p3mg.h
+ERR_ARG, ERR_METHOD, ERR_CAO, ERR_MESH, ERR_NOSYS = -1, -2, -3, -4, -5
+ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_PRECISION, ERR_NOBUF = -6, -7, -8, -9, -10
 FP64 = 0
 FP32_MIXED = 1
 
@@ -110,6 +113,8 @@ def load():
     L.p3mg_batch_destroy.restype = None
     L.p3mg_estimate_errors.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double] * 4 + [_dp]
     L.p3mg_error_estimate.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
+    L.p3mg_inhomo_error.argtypes = [vp, ctypes.c_double] + [ctypes.c_int] * 6 + [_dp, _dp]
+    L.p3mg_error_map.argtypes = [vp, ctypes.c_int, ctypes.c_int] + [_dp] * 8
     L.p3mg_kernel_times.argtypes = [vp, _dp]
     L.p3mg_set_graph.argtypes = [vp, ctypes.c_int]
     L.p3mg_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
@@ -327,6 +332,32 @@ class Context:
         _check(self._lib.p3mg_error_estimate(self._h, float(alpha), float(rcut), int(mc_est), _p(e)),
                "p3mg_error_estimate")
         return dict(total=e[0], kspace=e[1], realspace=e[2])
+
+    def inhomo_error(self, alpha, mesh=64, cao=5, mc=0, uniform=False, collect_mesh=None, collect_cao=None,
+                     want_meshes=False):
+        """Inhomogeneous k-space error estimate (p3mg_inhomo_error).  collect_mesh /
+        collect_cao default to the estimator's mesh and cao (the reference's CLI
+        passes the force method's).  With want_meshes also the (mesh^3, 5) columns
+        rho2, Re E, Im E, Re DFT(K2), Im DFT(K2)."""
+        cm = mesh if collect_mesh is None else collect_mesh
+        cc = cao if collect_cao is None else collect_cao
+        est = np.zeros(1)
+        out = np.zeros((mesh ** 3, 5)) if want_meshes else None
+        _check(self._lib.p3mg_inhomo_error(self._h, float(alpha), int(bool(uniform)), int(mesh), int(cao), int(mc),
+                                           int(cm), int(cc), _p(est), _p(out)), "p3mg_inhomo_error")
+        return (float(est[0]), out) if want_meshes else float(est[0])
+
+    def error_map(self, fk, ref, mesh=64, cao=1):
+        """Error map (p3mg_error_map): (mesh^3 doubles, totals (2,)) for k-space
+        forces fk and reference forces ref, both (3, n)."""
+        fk = np.ascontiguousarray(fk, dtype=np.float64).reshape(3, self.n)
+        ref = np.ascontiguousarray(ref, dtype=np.float64).reshape(3, self.n)
+        a = [np.ascontiguousarray(fk[d]) for d in range(3)] + [np.ascontiguousarray(ref[d]) for d in range(3)]
+        out = np.zeros(mesh ** 3)
+        tot = np.zeros(2)
+        _check(self._lib.p3mg_error_map(self._h, int(mesh), int(cao), *[_p(v) for v in a], _p(out), _p(tot)),
+               "p3mg_error_map")
+        return out, tot
 
     def kernel_times(self):
         t = np.zeros(3)

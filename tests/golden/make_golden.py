@@ -16,7 +16,13 @@ Outputs (numpy .npz, float64):
                 of the 0.1..2.5 step 0.05 sweep, and its Ewald forces.
   cli/*.dat  -- the out.dat tables of the reference program (oracle/_ref/p3m)
                 for the command lines in CLI_CASES, each with its own
-                generated system and Ewald reference forces.
+                generated system and Ewald reference forces; cli/*.inhomo,
+                *.map, *.map2d the inhomo_output and error map files the
+                program writes beside them.
+  inhomo.npz -- the reference's inhomogeneous error estimate and error map
+                (INHOMO_CASES, ERROR_MAP_CASES) on a seeded 200-particle
+                system.
+Single parts: --cli <case>... or --inhomo.
 The GPU box never runs this script; tests read the .npz files only.
 """
 import os
@@ -57,23 +63,83 @@ CLI_CASES = {
                 "alphamax 1.2 alphastep 0.2",
     "m2_type2": "particles 216 box 8 mesh 12 cao 7 rcut 2.5 method 2 system_type 2 alphamin 0.9 alphamax 1.3 "
                 "alphastep 0.2",
+    # inhomogeneous estimate (err_inhomo column, inhomo_output file) and error map files
+    "m2_inhomo": "particles 200 box 6 mesh 12 cao 5 rcut 2.5 method 2 alphamin 0.9 alphamax 1.1 alphastep 0.2 "
+                 "error_k inhomo_error inhomo_mesh 8 inhomo_cao 5 inhomo_mc 1 inhomo_output inhomo.txt "
+                 "error_map error_map_mesh 8 error_map_cao 3",
 }
 
+# files the program writes next to out.dat, kept as <case>.<suffix>
+CLI_EXTRA_FILES = {"inhomo.txt": "inhomo", "error_map.dat": "map", "error_map_2d.dat": "map2d"}
 
-def make_cli_goldens():
+
+def make_cli_goldens(names=None):
     import subprocess
     import tempfile
     exe = os.path.join(ROOT, "oracle", "_ref", "p3m")
     os.makedirs(os.path.join(HERE, "cli"), exist_ok=True)
     for name, args in CLI_CASES.items():
+        if names and name not in names:
+            continue
+        extra = {}
         with tempfile.TemporaryDirectory() as tmp:
             out = os.path.join(tmp, "out.dat")
             subprocess.run([exe] + args.split() + ["outfile", out], cwd=tmp, check=True, stdout=subprocess.DEVNULL,
                            stderr=subprocess.DEVNULL)
             with open(out) as f:
                 text = f.read()
+            for fname, suffix in CLI_EXTRA_FILES.items():
+                if os.path.exists(os.path.join(tmp, fname)):
+                    with open(os.path.join(tmp, fname)) as f:
+                        extra[suffix] = f.read()
         with open(os.path.join(HERE, "cli", name + ".dat"), "w") as f:
             f.write("# " + args + "\n" + text)
+        for suffix, body in extra.items():
+            with open(os.path.join(HERE, "cli", name + "." + suffix), "w") as f:
+                f.write(body)
+
+
+# (method mesh, method cao, alpha, uniform, mesh, cao, mc) of the inhomogeneous estimate
+INHOMO_CASES = [
+    (8, 3, 1.3, 0, 8, 3, 0),
+    (8, 3, 1.3, 0, 8, 3, 1),
+    (8, 3, 1.3, 0, 8, 5, 1),
+    (8, 4, 1.3, 1, 8, 4, 1),
+    (16, 2, 1.3, 0, 10, 3, 1),
+    (6, 2, 1.3, 0, 6, 2, 2),
+    (16, 5, 1.3, 0, 12, 5, 0),
+]
+# (mesh, cao) of the error map
+ERROR_MAP_CASES = [(8, 1), (16, 3), (10, 7), (7, 2)]
+
+
+def make_inhomo_golden():
+    """inhomo.npz: the reference's Generic_error_estimate_inhomo and Error_map
+    on a seeded 200-particle system (L = 5), plus the reference's inhomo_output
+    columns of case 1."""
+    import tempfile
+    x, y, z, q = O.uniform_system(200, 5.0, seed=7)
+    L = 5.0
+    out = dict(x=x, y=y, z=z, q=q, L=L, inhomo_cases=np.array(INHOMO_CASES, dtype=np.float64),
+               map_cases=np.array(ERROR_MAP_CASES, dtype=np.float64))
+    est = []
+    for k, (cm, cc, a, uni, m, c, mc) in enumerate(INHOMO_CASES):
+        if k == 1:
+            with tempfile.TemporaryDirectory() as tmp:
+                f = os.path.join(tmp, "inhomo.txt")
+                est.append(O.ref_inhomo_error(x, y, z, q, L, cm, cc, a, uni, m, c, mc, out_file=f))
+                out["inhomo_columns_1"] = np.loadtxt(f)
+        else:
+            est.append(O.ref_inhomo_error(x, y, z, q, L, cm, cc, a, uni, m, c, mc))
+    out["inhomo_estimates"] = np.array(est)
+    rng = np.random.default_rng(1)
+    fk = rng.normal(size=(3, 200))
+    fr = fk + 1e-3 * rng.normal(size=(3, 200))
+    out["fk"] = fk
+    out["fk_ref"] = fr
+    for k, (m, c) in enumerate(ERROR_MAP_CASES):
+        out["map_%d" % k] = O.ref_error_map(x, y, z, L, fk, fr, m, c)
+    np.savez_compressed(os.path.join(HERE, "inhomo.npz"), **out)
 
 
 def main(ref_dir):
@@ -109,8 +175,14 @@ def main(ref_dir):
     out["ewald_kmax"] = e["kmax"]
     np.savez_compressed(os.path.join(HERE, "sweep.npz"), **out)
     make_cli_goldens()
+    make_inhomo_golden()
     print("wrote", os.path.join(HERE, "wall.npz"), os.path.join(HERE, "sweep.npz"), os.path.join(HERE, "cli"))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 2 and sys.argv[1] == "--cli":
+        make_cli_goldens(sys.argv[2:])  # only these command-line cases
+    elif len(sys.argv) > 1 and sys.argv[1] == "--inhomo":
+        make_inhomo_golden()
+    else:
+        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
