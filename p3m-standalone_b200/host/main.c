@@ -78,7 +78,10 @@ static double min_distance(const system_t *s) {
 
 /* Error map of the k-space forces against the Ewald k-space forces
  * (main.c:403-424, Error_map p3m-common.c:402-435): error_map.dat holds every
- * mesh point, error_map_2d.dat the plane nx = 0.5 mesh. */
+ * mesh point, error_map_2d.dat the plane nx = 0.5 mesh.  Both are rewritten
+ * and closed at every alpha, so they hold the last alpha's map (the
+ * reference leaves its streams open, main.c:407-423, and with several alphas
+ * the earlier streams' buffers land in its files at exit). */
 static void write_error_map(data_t *data, const forces_t *f, const forces_t *f_ref, int mesh, int cao) {
   puts("Writing error map.");
   const size_t M = (size_t)mesh * mesh * mesh;

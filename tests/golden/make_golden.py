@@ -63,10 +63,15 @@ CLI_CASES = {
                 "alphamax 1.2 alphastep 0.2",
     "m2_type2": "particles 216 box 8 mesh 12 cao 7 rcut 2.5 method 2 system_type 2 alphamin 0.9 alphamax 1.3 "
                 "alphastep 0.2",
-    # inhomogeneous estimate (err_inhomo column, inhomo_output file) and error map files
+    # inhomogeneous estimate (err_inhomo column, inhomo_output file)
     "m2_inhomo": "particles 200 box 6 mesh 12 cao 5 rcut 2.5 method 2 alphamin 0.9 alphamax 1.1 alphastep 0.2 "
-                 "error_k inhomo_error inhomo_mesh 8 inhomo_cao 5 inhomo_mc 1 inhomo_output inhomo.txt "
-                 "error_map error_map_mesh 8 error_map_cao 3",
+                 "error_k inhomo_error inhomo_mesh 8 inhomo_cao 5 inhomo_mc 1 inhomo_output inhomo.txt",
+    # error map files.  A single alpha: the reference opens error_map.dat and
+    # error_map_2d.dat once per alpha and never closes them (main.c:407-423),
+    # so with several alphas the earlier streams' buffers are flushed over
+    # the last alpha's contents at exit.
+    "m2_errmap": "particles 200 box 6 mesh 12 cao 5 rcut 2.5 method 2 alphamin 1.1 alphamax 1.1 alphastep 0.2 "
+                 "error_k error_map error_map_mesh 8 error_map_cao 3",
 }
 
 # files the program writes next to out.dat, kept as <case>.<suffix>
