@@ -6,10 +6,20 @@
  *   forces out:  n lines "<i> fx fy fz fkx fky fkz" (io.c:159-177)
  *
  * Unreadable files exit 127 and malformed ones -1 (255), as in the
- * reference.  Two widenings: further "#" lines after the header (the
- * "# Mesh:" line of the Data/ReferenceDataVincent .dat files) are skipped,
- * and a forces file may have 4 or 7 columns per line (the reference reader
- * only parses 4, so it cannot read back its own 7-column output). */
+ * reference.  Widenings, for the reference's own data sets
+ * (Data/ReferenceDataVincent):
+ *   - further "#" lines after the header (the "# Mesh:", "# kmax:",
+ *     "# alpha:" ... lines of the Konfig_NN.dat files) are skipped;
+ *   - a positions file without the "#" header is read as the simulation
+ *     snapshots konfig_N: a line with the count, a line with the box
+ *     length, then "x y z q" with unwrapped coordinates, which are folded
+ *     into [0, L) here (the reference's mesh code wraps only once,
+ *     charge-assign.c:37-40);
+ *   - a forces file may have 4 or 7 columns per line (the reference reader
+ *     only parses 4, so it cannot read back its own 7-column output), and a
+ *     4-column line whose first field is not an integer is a Konfig_NN.exact
+ *     line "E fx fy fz" (total Coulomb energy, then the force). */
+#include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -97,11 +107,43 @@ static void bad_file(const char *filename, FILE *fp) {
   exit(-1);
 }
 
+/* x folded into [0, L) */
+static double fold(double x, double L) {
+  double r = x - L * floor(x / L);
+  return (r >= L || r < 0.0) ? 0.0 : r;
+}
+
+/* konfig_N snapshot: count line, length line, n lines "x y z q" */
+static system_t *read_konfig(const char *filename, FILE *fp) {
+  int n = -1;
+  double len = 0.0;
+  if (fscanf(fp, "%d", &n) != 1 || fscanf(fp, "%lf", &len) != 1 || n < 0 || !(len > 0.0)) bad_file(filename, fp);
+  system_t *s = Init_system(n);
+  s->length = len;
+  s->q2 = 0.0;
+  for (int i = 0; i < n; i++) {
+    double x, y, z;
+    if (fscanf(fp, "%lf %lf %lf %lf", &x, &y, &z, &s->q[i]) != 4) bad_file(filename, fp);
+    s->p->x[i] = fold(x, len);
+    s->p->y[i] = fold(y, len);
+    s->p->z[i] = fold(z, len);
+    s->q2 += s->q[i] * s->q[i];
+  }
+  fclose(fp);
+  return s;
+}
+
 system_t *Read_system(parameters_t *p, const char *filename) {
   (void)p;
   FILE *fp = open_or_die(filename, "r");
   int n = -1;
   double len = 0.0;
+  int first;
+  while ((first = fgetc(fp)) == ' ' || first == '\t' || first == '\n' || first == '\r') {
+  }
+  if (first == EOF) bad_file(filename, fp);
+  ungetc(first, fp);
+  if (first != '#') return read_konfig(filename, fp);
   if (fscanf(fp, " # Teilchenzahl: %d", &n) != 1 || fscanf(fp, " # Len: %lf", &len) != 1 || n < 0)
     bad_file(filename, fp);
   /* skip any further comment lines */
@@ -142,11 +184,15 @@ void Read_exact_forces(system_t *s, const char *filename) {
   char line[1024];
   int i = 0;
   while (i < s->nparticles && fgets(line, sizeof line, fp)) {
-    int idx;
-    double v[6];
-    const int got = sscanf(line, "%d %lf %lf %lf %lf %lf %lf", &idx, v, v + 1, v + 2, v + 3, v + 4, v + 5);
+    double v[7];
+    const int got = sscanf(line, "%lf %lf %lf %lf %lf %lf %lf", v + 6, v, v + 1, v + 2, v + 3, v + 4, v + 5);
     if (got == EOF || got == 0) continue; /* blank line */
-    if (got != 4 && got != 7) {
+    /* the first field: an index (reference layout) or, with 4 fields and a
+     * fraction or exponent in it, the energy of a .exact line */
+    const char *t = line + strspn(line, " \t");
+    const size_t tl = strcspn(t, " \t\r\n");
+    const int integer = memchr(t, '.', tl) == NULL && memchr(t, 'e', tl) == NULL && memchr(t, 'E', tl) == NULL;
+    if ((got != 4 && got != 7) || (got == 7 && !integer)) {
       fprintf(stderr, "Error while reading file '%s' (%d) (%d)\n", filename, got, i);
       fclose(fp);
       exit(-1);

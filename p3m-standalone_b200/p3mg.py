@@ -554,30 +554,67 @@ def generate_system(system_type, n, L, charge=1.0, seed=12345, sigma=None):
 
 def read_system(path):
     """Read_system (io.c:100-157): '# Teilchenzahl: N', '# Len: L', then
-    N lines 'x y z q'.  Extra '#' header lines (as in the Data/ fixtures'
-    '# Mesh:') are skipped."""
-    n = L = None
+    N lines 'x y z q'.  Extra '#' header lines (the '# Mesh:', '# kmax:',
+    '# alpha:' ... lines of the Data/ReferenceDataVincent Konfig_NN.dat
+    files, see read_system_header) are skipped.  A file without the '#'
+    header is a konfig_N simulation snapshot of the same data sets: a count
+    line, a box-length line, then 'x y z q' with unwrapped coordinates,
+    which are folded into [0, L)."""
+    with open(path) as fh:
+        lines = [l.strip() for l in fh]
+    lines = [l for l in lines if l]
+    if not lines:
+        raise ValueError("Error while reading file '%s'" % path)
+    if not lines[0].startswith("#"):
+        try:
+            n, L = int(lines[0].split()[0]), float(lines[1].split()[0])
+            a = np.array([[float(v) for v in l.split()[:4]] for l in lines[2:2 + n]], dtype=np.float64).reshape(-1, 4)
+        except (ValueError, IndexError):
+            raise ValueError("Error while reading file '%s'" % path)
+        if a.shape[0] != n or not L > 0:
+            raise ValueError("Error while reading file '%s': %d of %d particles" % (path, a.shape[0], n))
+        pos = a[:, :3] - L * np.floor(a[:, :3] / L)
+        pos[(pos >= L) | (pos < 0)] = 0.0
+        return pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy(), a[:, 3].copy(), L
+    hdr = read_system_header(path)
+    n, L = hdr.get("Teilchenzahl"), hdr.get("Len")
+    if n is None or L is None:
+        raise ValueError("Error while reading file '%s'" % path)
+    n = int(n)
     rows = []
+    for l in lines:
+        if l.startswith("#"):
+            continue
+        rows.append([float(v) for v in l.split()[:4]])
+        if len(rows) == n:
+            break
+    a = np.array(rows, dtype=np.float64).reshape(-1, 4)
+    if a.shape[0] != n:
+        raise ValueError("Error while reading file '%s': %d of %d particles" % (path, a.shape[0], n))
+    return a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy(), a[:, 3].copy(), float(L)
+
+
+def read_system_header(path):
+    """The '# key: value' header lines of a positions file as a dict of
+    numbers: Teilchenzahl and Len, and in the Konfig_NN.dat files of
+    Data/ReferenceDataVincent also Mesh, kmax, alpha, beta, ip (the window
+    order minus 1), rcut, Temp and Bjerrum."""
+    out = {}
     with open(path) as fh:
         for line in fh:
             s = line.strip()
             if not s:
                 continue
-            if s.startswith("#"):
-                if "Teilchenzahl" in s:
-                    n = int(s.split(":")[1])
-                elif "Len" in s:
-                    L = float(s.split(":")[1])
-                continue
-            rows.append([float(v) for v in s.split()[:4]])
-            if n is not None and len(rows) == n:
+            if not s.startswith("#"):
                 break
-    if n is None or L is None:
-        raise ValueError("Error while reading file '%s'" % path)
-    a = np.array(rows, dtype=np.float64).reshape(-1, 4)
-    if a.shape[0] != n:
-        raise ValueError("Error while reading file '%s': %d of %d particles" % (path, a.shape[0], n))
-    return a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy(), a[:, 3].copy(), L
+            key, _, val = s[1:].partition(":")
+            try:
+                v = float(val)
+            except ValueError:
+                continue
+            out[key.strip()] = int(v) if v.is_integer() and key.strip() in ("Teilchenzahl", "Mesh", "kmax", "ip") \
+                else v
+    return out
 
 
 def write_system(path, x, y, z, q, L):
@@ -589,24 +626,33 @@ def write_system(path, x, y, z, q, L):
             fh.write("%f\t%f\t%f\t%f\n" % (x[i], y[i], z[i], q[i]))
 
 
-def read_exact_forces(path, n):
+def read_exact_forces(path, n, with_energy=False):
     """Read_exact_forces (io.c:70-98): lines 'id fx fy fz'.  Also accepts the
     7-column 'id F(3) F_k(3)' layout Write_exact_forces writes (io.c:171-173),
-    taking the total force columns."""
+    taking the total force columns, and the Konfig_NN.exact lines
+    'E fx fy fz' of Data/ReferenceDataVincent (first field not an integer:
+    the total Coulomb energy).  with_energy: also return that energy (None
+    for the other layouts)."""
     f = np.zeros((3, n))
+    energy = None
     i = 0
     with open(path) as fh:
         for line in fh:
             s = line.split()
-            if len(s) < 4:
+            if not s:
                 continue
+            integer = not any(c in s[0] for c in ".eE")
+            if len(s) not in (4, 7) or (len(s) == 7 and not integer):
+                raise ValueError("Error while reading file '%s' (%d) (%d)" % (path, len(s), i))
+            if not integer:
+                energy = float(s[0])
             f[:, i] = [float(s[1]), float(s[2]), float(s[3])]
             i += 1
             if i == n:
                 break
     if i != n:
         raise ValueError("Error while reading file '%s' (%d)" % (path, i))
-    return f
+    return (f, energy) if with_energy else f
 
 
 def write_exact_forces(path, f, fk):

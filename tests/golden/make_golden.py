@@ -22,7 +22,10 @@ Outputs (numpy .npz, float64):
   inhomo.npz -- the reference's inhomogeneous error estimate and error map
                 (INHOMO_CASES, ERROR_MAP_CASES) on a seeded 200-particle
                 system.
-Single parts: --cli <case>... or --inhomo.
+  vincent.npz -- raw text of the reference's data sets
+                (Data/ReferenceDataVincent, VINCENT_FILES): NaCl snapshots
+                and a water box with their exact Ewald forces.
+Single parts: --cli <case>..., --inhomo or --vincent [reference_dir].
 The GPU box never runs this script; tests read the .npz files only.
 """
 import os
@@ -147,6 +150,33 @@ def make_inhomo_golden():
     np.savez_compressed(os.path.join(HERE, "inhomo.npz"), **out)
 
 
+# (key, zip archive, position file, exact-force file) from Data/ReferenceDataVincent
+VINCENT_FILES = [
+    ("nacl300_konfig", "NaCl_crystal_300K.zip", "NaCl_crystal_300K/konfig_0", None),
+    ("nacl300", "NaCl_crystal_300K.zip", "NaCl_crystal_300K/Konfig_01.dat", "NaCl_crystal_300K/Konfig_01.exact"),
+    ("melt_konfig", "NaCl_melt.zip", "NaCl_melt/konfig_0", None),
+    ("melt", "NaCl_melt.zip", "NaCl_melt/Konfig_01.dat", "NaCl_melt/Konfig_01.exact"),
+    ("water", "KONFIG_water.zip", "KONFIG_water/CONFIG_water", "KONFIG_water/CONFIG_water.exact"),
+]
+
+
+def make_vincent_golden(ref_dir):
+    """vincent.npz: the raw text (uint8 arrays) of the reference's own data
+    sets in Data/ReferenceDataVincent: 512-ion NaCl crystal (300 K) and melt
+    snapshots in both the konfig_N and the Konfig_NN.dat layout, and the
+    648-site water box, with their Konfig_NN.exact / CONFIG_water.exact
+    Ewald forces (made outside the reference, by its authors)."""
+    import zipfile
+    base = os.path.join(ref_dir, "Data", "ReferenceDataVincent")
+    out = {}
+    for key, arc, pos, exact in VINCENT_FILES:
+        with zipfile.ZipFile(os.path.join(base, arc)) as zf:
+            out[key + "_pos"] = np.frombuffer(zf.read(pos), dtype=np.uint8)
+            if exact:
+                out[key + "_exact"] = np.frombuffer(zf.read(exact), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "vincent.npz"), **out)
+
+
 def main(ref_dir):
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libp3mref.so missing: run sh oracle/build_ref.sh first")
@@ -181,6 +211,7 @@ def main(ref_dir):
     np.savez_compressed(os.path.join(HERE, "sweep.npz"), **out)
     make_cli_goldens()
     make_inhomo_golden()
+    make_vincent_golden(ref_dir)
     print("wrote", os.path.join(HERE, "wall.npz"), os.path.join(HERE, "sweep.npz"), os.path.join(HERE, "cli"))
 
 
@@ -189,5 +220,7 @@ if __name__ == "__main__":
         make_cli_goldens(sys.argv[2:])  # only these command-line cases
     elif len(sys.argv) > 1 and sys.argv[1] == "--inhomo":
         make_inhomo_golden()
+    elif len(sys.argv) > 1 and sys.argv[1] == "--vincent":
+        make_vincent_golden(sys.argv[2] if len(sys.argv) > 2 else "/root/reference")
     else:
         main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
