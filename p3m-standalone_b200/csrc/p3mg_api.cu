@@ -138,6 +138,11 @@ int free_all(Ctx *c) {
   if (c->ev_ok)
     for (int i = 0; i < 12; i++) cudaEventDestroy(c->ev[i]);
   c->ev_ok = false;
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  c->ev_fork = c->ev_join = nullptr;
+  if (c->stream2) cudaStreamDestroy(c->stream2);
+  c->stream2 = nullptr;
   if (c->stream) cudaStreamDestroy(c->stream);
   c->stream = nullptr;
   return P3MG_OK;
@@ -146,6 +151,25 @@ int free_all(Ctx *c) {
 // Enqueue one force evaluation on the context stream (Calculate_forces,
 // common.c:268-327): zero, real space (rcut != 0, common.c:290-294),
 // k-space with self-force, f += f_k + f_r.
+// The real-space pairs (instruction-issue bound) and the k-space chain
+// (shared-memory atomics, L1 and HBM bound) touch disjoint buffers, so the
+// pairs run on stream2 beside the k-space chain: forked after the forces
+// are zeroed, joined before they are combined.  Stage and kernel events
+// follow the stream their work runs on (t_r from the step start to the
+// pairs' end on stream2, t_c from the k-space start on the context stream).
+static int enqueue_pairs_on_stream2(Ctx *c, double rcut) {
+  P3MG_CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
+  P3MG_CUDA_TRY(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+  cudaStream_t main_stream = c->stream;
+  c->stream = c->stream2;
+  const int st = pairs_run(c, rcut, c->d_alpha, 1, c->fr, c->energy);
+  mark(c, EV_S1);
+  c->stream = main_stream;
+  // join even after an error, so no work is left outside the context stream
+  P3MG_CUDA_TRY(cudaEventRecord(c->ev_join, c->stream2));
+  return st;
+}
+
 static int enqueue_step(Ctx *c, double rcut) {
   P3MG_TRY(zero_forces(c));
   const bool timed = c->timing && c->ev_ok && c->n > 0;
@@ -153,13 +177,22 @@ static int enqueue_step(Ctx *c, double rcut) {
     // brackets of stages that may not run this step must still be recorded
     for (int s = EV_K0; s <= EV_K5; s++) cudaEventRecord(c->ev[s], c->stream);
   }
+  const bool overlap = rcut != 0.0 && c->n > 0 && c->stream2;
   mark(c, EV_S0);
-  if (rcut != 0.0) P3MG_TRY(pairs_run(c, rcut, c->d_alpha, 1, c->fr, c->energy));
-  mark(c, EV_S1);
-  if (c->n > 0) {
-    P3MG_TRY(kspace_prepare(c));
-    P3MG_TRY(kspace_run(c));
+  int st = P3MG_OK;
+  if (overlap) {
+    st = enqueue_pairs_on_stream2(c, rcut);
+  } else {
+    if (rcut != 0.0) st = pairs_run(c, rcut, c->d_alpha, 1, c->fr, c->energy);
+    mark(c, EV_S1);
   }
+  mark(c, EV_S1K);
+  if (st == P3MG_OK && c->n > 0) {
+    st = kspace_prepare(c);
+    if (st == P3MG_OK) st = kspace_run(c);
+  }
+  if (overlap) P3MG_CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+  P3MG_TRY(st);
   P3MG_TRY(combine_forces(c));
   c->stage_pending = timed;
   return P3MG_OK;
@@ -168,8 +201,9 @@ static int enqueue_step(Ctx *c, double rcut) {
 static void collect_stage_times(Ctx *c) {
   if (!c->stage_pending) return;
   cudaEventSynchronize(c->ev[EV_S4]);
+  cudaEventSynchronize(c->ev[EV_S1]);
   float t;
-  const int st[4][2] = {{EV_S1, EV_S2}, {EV_S2, EV_S3}, {EV_S3, EV_S4}, {EV_S0, EV_S1}};
+  const int st[4][2] = {{EV_S1K, EV_S2}, {EV_S2, EV_S3}, {EV_S3, EV_S4}, {EV_S0, EV_S1}};
   for (int i = 0; i < 4; i++)
     if (cudaEventElapsedTime(&t, c->ev[st[i][0]], c->ev[st[i][1]]) == cudaSuccess) c->stage_ms[i] = t;
   const int kt[3][2] = {{EV_K0, EV_K1}, {EV_K2, EV_K3}, {EV_K4, EV_K5}};
@@ -288,6 +322,9 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
       break;
     }
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
       record_cuda_error(e);
       st = P3MG_ERR_CUDA;

@@ -186,14 +186,16 @@ int scan_tmp_reserve(Ctx *c, int nb) {
   if (c->scan_tmp) cudaFree(c->scan_tmp);
   c->scan_tmp = nullptr;
   c->scan_cap = 0;
-  P3MG_CUDA_TRY(cudaMalloc(&c->scan_tmp, sizeof(int) * need));
+  P3MG_CUDA_TRY(cudaMalloc(&c->scan_tmp, sizeof(int) * 2 * need));
   c->scan_cap = need;
   return P3MG_OK;
 }
 
 // Exclusive scan of nb counts into start[0..nb] (start[nb] = total): one
 // CTA for short arrays, the tiled three-launch scan with the context's
-// scratch (scan_tmp_reserve, done before any graph capture) otherwise.
+// scratch (scan_tmp_reserve, done before any graph capture) otherwise --
+// its second slot when the scan is enqueued on stream2, so the two streams
+// of a step never share it.
 int exclusive_scan(Ctx *c, const int *counts, int *start, int nb) {
   if (nb <= 16 * SCAN_TILE) {
     scan_kernel<<<1, 1024, 0, c->stream>>>(counts, start, nb);
@@ -203,7 +205,8 @@ int exclusive_scan(Ctx *c, const int *counts, int *start, int nb) {
   }
   const int ntile = (nb + SCAN_TILE - 1) / SCAN_TILE;
   if (2 * (ntile + 1) > c->scan_cap) return P3MG_ERR_STATE;
-  int *tsum = c->scan_tmp, *tstart = c->scan_tmp + ntile + 1;
+  int *tmp = c->scan_tmp + ((c->stream2 && c->stream == c->stream2) ? c->scan_cap : 0);
+  int *tsum = tmp, *tstart = tmp + ntile + 1;
   scan_tile_sums_kernel<<<ntile, 1024, 0, c->stream>>>(counts, nb, tsum);
   scan_kernel<<<1, 1024, 0, c->stream>>>(tsum, tstart, ntile);
   scan_tiles_kernel<<<ntile, 1024, 0, c->stream>>>(counts, nb, tstart, start);

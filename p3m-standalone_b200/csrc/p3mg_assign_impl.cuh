@@ -36,6 +36,15 @@ __host__ __device__ constexpr size_t scatter_stage_bytes() {
 // so one instruction's shared-memory atomics neither collide nor conflict.
 // The tile is added to the global mesh at the end (periodic wrap, one
 // global atomic per non-zero tile point).
+//
+// FP32: the tile accumulates in 32-bit fixed point with the brick's own
+// scale S = 2^30 / sum |q| over the brick's particles -- shared-memory
+// integer adds are single native atomics where float adds are not, and
+// no tile point can overflow (every weight product is <= 1, so a point's
+// sum stays within 2^30 plus half a unit per contribution).  The resolution
+// sum |q| / 2^30 is below the FP32 rounding of the contributions for the
+// few hundred particles of a brick; integer sums also make the tile
+// independent of the order of the atomics.  FP64 accumulates doubles.
 template <typename real, int CAO, int NMESH>
 __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *__restrict__ sxyzq,
                                                                   const int *__restrict__ start, int m, int B, int nb,
@@ -43,17 +52,37 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
                                                                   const int4 *__restrict__ lanetab,
                                                                   typename cplx<real>::type *__restrict__ Q) {
   constexpr int NPASS = (CAO * CAO + 31) / 32;  // passes of 32 (b, c) columns
+  constexpr bool FIXED = std::is_same<real, float>::value;
+  typedef typename std::conditional<FIXED, int, real>::type acc_t;
+  static_assert(sizeof(acc_t) == sizeof(real), "tile layout");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int T = brick_tile(B, CAO, NMESH);
   const int T3 = T * SP;  // tile elements: T planes of pitch SP, rows of pitch SR
-  real *tile0 = reinterpret_cast<real *>(smem_raw);
-  real *tile1 = tile0 + T3;
-  real *sw = tile0 + NMESH * T3;                                   // [NMESH*CHUNK][3][CAO]
+  acc_t *tile0 = reinterpret_cast<acc_t *>(smem_raw);
+  acc_t *tile1 = tile0 + T3;
+  real *sw = reinterpret_cast<real *>(tile0 + NMESH * T3);         // [NMESH*CHUNK][3][CAO]
   int *soff = reinterpret_cast<int *>(sw + NMESH * SCATTER_CHUNK * 3 * CAO);  // tile offset of the stencil origin
   const int bid = blockIdx.x;
   const int p0 = start[bid * B * B * B], p1 = start[(bid + 1) * B * B * B];
   if (p0 == p1) return;
-  for (int t = threadIdx.x; t < NMESH * T3; t += blockDim.x) tile0[t] = (real)0;
+  for (int t = threadIdx.x; t < NMESH * T3; t += blockDim.x) tile0[t] = (acc_t)0;
+  // FP32: fixed-point scale of this brick from sum |q| (rounded up a little
+  // so the bound survives the summation's rounding)
+  real scale = (real)1, inv_scale = (real)1;
+  if (FIXED) {
+    __shared__ double qsum_w[ASSIGN_THREADS / 32];
+    double qs = 0.0;
+    for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) qs += fabs(sxyzq[p].w);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) qs += __shfl_xor_sync(0xffffffffu, qs, o);
+    if ((threadIdx.x & 31) == 0) qsum_w[threadIdx.x >> 5] = qs;
+    __syncthreads();
+    double R = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) R += qsum_w[w];
+    R *= 1.0 + 1e-6;
+    scale = R > 0.0 ? (real)(1073741824.0 / R) : (real)0;
+    inv_scale = (real)(R / 1073741824.0);
+  }
   const int bz = bid % nb, by = (bid / nb) % nb, bx = bid / (nb * nb);
   const int o0 = bx * B, o1 = by * B, o2 = bz * B;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
@@ -100,18 +129,23 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
     __syncthreads();
     for (int v = warp; v < cnt * NMESH; v += nwarp) {
       const real *wv = sw + (size_t)v * 3 * CAO;
-      real *tile = (NMESH == 2 && (v & 1)) ? tile1 : tile0;
-      real *org = tile + soff[v];
+      acc_t *tile = (NMESH == 2 && (v & 1)) ? tile1 : tile0;
+      acc_t *org = tile + soff[v];
       real wx[CAO];
 #pragma unroll
-      for (int a = 0; a < CAO; a++) wx[a] = wv[a];
+      for (int a = 0; a < CAO; a++) wx[a] = FIXED ? wv[a] * scale : wv[a];
 #pragma unroll
       for (int ps = 0; ps < NPASS; ps++) {
         if (lb[ps] >= 0) {
           const real wyz = wv[CAO + lb[ps]] * wv[2 * CAO + lc[ps]];
-          real *col = org + loff[ps];
+          acc_t *col = org + loff[ps];
 #pragma unroll
-          for (int a = 0; a < CAO; a++) atomicAdd(col + a * SP, wx[a] * wyz);
+          for (int a = 0; a < CAO; a++) {
+            if constexpr (FIXED)
+              atomicAdd(col + a * SP, __float2int_rn(wx[a] * wyz));
+            else
+              atomicAdd(col + a * SP, wx[a] * wyz);
+          }
         }
       }
     }
@@ -128,9 +162,9 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
     if (gj >= m) gj %= m;
     if (gk >= m) gk %= m;
     const size_t g = ((size_t)gi * m + gj) * m + gk;
-    const real v0 = tile0[e];
+    const real v0 = FIXED ? (real)tile0[e] * inv_scale : (real)tile0[e];
     if (NMESH == 2) {
-      const real v1 = tile1[e];
+      const real v1 = FIXED ? (real)tile1[e] * inv_scale : (real)tile1[e];
       if (v0 != (real)0) atomicAdd(&Q[g].x, v0);
       if (v1 != (real)0) atomicAdd(&Q[g].y, v1);
     } else {

@@ -100,14 +100,29 @@ __global__ void __launch_bounds__(EW_THREADS) ewald_sk_kernel(const double *__re
   }
 }
 
-// k-space force on each target from the half-space structure factors.
-// For k and -k the contributions are equal, so the half space counts twice
-// (the k_x = 0, k_y = 0 column holds both k_z and -k_z already).
+// S(k) *= 2 g(k) in place: the influence weight of each k vector (0 where
+// the cutoff drops it), doubled for the mirrored half space.  Applied once
+// here instead of once per target.
+__global__ void ewald_weight_kernel(const int2 *__restrict__ cols, int ncol, int kmax, bool shell, double fak1,
+                                    double fak2, double2 *__restrict__ S) {
+  const int nz = 2 * kmax + 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncol * nz) return;
+  const int2 col = cols[t / nz];
+  const int kz = t % nz - kmax;
+  const double g = 2.0 * ewald_ghat(abs(col.x), abs(col.y), abs(kz), kmax, shell, fak1, fak2);
+  const double2 s = S[t];
+  S[t] = make_double2(g * s.x, g * s.y);
+}
+
+// k-space force on each target from the weighted half-space structure
+// factors 2 g(k) S(k).  For k and -k the contributions are equal, so the
+// half space counts twice (the k_x = 0, k_y = 0 column holds both k_z and
+// -k_z already).
 __global__ void ewald_kforce_kernel(const double *__restrict__ x, const double *__restrict__ y,
                                     const double *__restrict__ z, const double *__restrict__ q,
                                     const int *__restrict__ tgt, int nt, double twopi_L, const int2 *__restrict__ cols,
-                                    int ncol, int kmax, bool shell, double fak1, double fak2,
-                                    const double2 *__restrict__ S, double *__restrict__ fk) {
+                                    int ncol, int kmax, const double2 *__restrict__ S, double *__restrict__ fk) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   const int i = tgt ? tgt[t] : t;
@@ -128,16 +143,13 @@ __global__ void ewald_kforce_kernel(const double *__restrict__ x, const double *
     sincos(twopi_L * (double)kz_lo * zi, &sz, &cz);
     double er = cxy * cz - s * sz, ei = s * cz + cxy * sz;
     for (int kz = kz_lo; kz <= kz_hi; kz++) {
-      const double g = ewald_ghat(abs(kx), abs(ky), abs(kz), kmax, shell, fak1, fak2);
-      if (g != 0.0) {
-        const double2 sk = S[(size_t)c * nz + (kz + kmax)];
-        // q_i g (rhohat_re sin(k.r_i) + rhohat_im cos(k.r_i)), rhohat = S (ewald.c:160-161);
-        // doubled for the mirrored half space
-        const double ff = 2.0 * qi * g * (ei * sk.x + er * sk.y);
-        fx += kx * ff;
-        fy += ky * ff;
-        fz += kz * ff;
-      }
+      const double2 sk = S[(size_t)c * nz + (kz + kmax)];
+      // q_i g (rhohat_re sin(k.r_i) + rhohat_im cos(k.r_i)), rhohat = S
+      // (ewald.c:160-161), with 2 g already in sk
+      const double ff = qi * (ei * sk.x + er * sk.y);
+      fx += kx * ff;
+      fy += ky * ff;
+      fz += kz * ff;
       const double nr = er * cz1 - ei * sz1;
       ei = ei * cz1 + er * sz1;
       er = nr;
@@ -285,9 +297,10 @@ int ewald_forces(Ctx *c, int nt, const int *d_tgt, double alpha, int kmax, bool 
     if (n > 0 && kout) {
       dim3 grid(ncol, (nz + EW_KZC - 1) / EW_KZC);
       ewald_sk_kernel<<<grid, EW_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, twopi_L, d_cols, kmax, d_S);
+      ewald_weight_kernel<<<(ncol * nz + 255) / 256, 256, 0, c->stream>>>(d_cols, ncol, kmax, shell, fak1, fak2, d_S);
       ewald_kforce_kernel<<<(nt + 127) / 128, 128, 0, c->stream>>>(c->x, c->y, c->z, c->q, d_tgt, nt, twopi_L, d_cols,
-                                                                   ncol, kmax, shell, fak1, fak2, d_S, kout);
-      c->launches += 2;
+                                                                   ncol, kmax, d_S, kout);
+      c->launches += 3;
       if (d_fk && d_out) e = cudaMemcpyAsync(d_out, d_fk, bytes, cudaMemcpyDeviceToDevice, c->stream);
       if (e == cudaSuccess) e = cudaGetLastError();
       if (e != cudaSuccess) break;

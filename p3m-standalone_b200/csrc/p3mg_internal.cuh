@@ -68,6 +68,10 @@ struct Ctx {
   int method = 0, mesh = 0, cao = 0, mc = 1, precision = P3MG_FP64;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream of a step: the real-space pairs run on it beside the
+  // k-space chain (fork / join events on the context stream)
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
   // particles
   int n = 0, cap = 0;
@@ -133,9 +137,10 @@ struct Ctx {
   int graph_n = -1;
   long long graph_launches = 0;  // kernels per replay
 
-  // scratch for a single-CTA scan
+  // scratch of the tiled scan: two slots of scan_cap ints, the second for
+  // scans enqueued on stream2
   int *scan_tmp = nullptr;
-  int scan_cap = 0;           // ints in scan_tmp
+  int scan_cap = 0;           // ints per slot
   void *sweep_ws = nullptr;  // workspace of p3mg_sweep, kept between calls
   // energy / adjoint buffers (allocated on first use): G and dG/dalpha at
   // alpha, the potential mesh, 8 reduction slots, the gradients (3 n + n)
@@ -148,7 +153,7 @@ struct Ctx {
 // event slots: stage markers and kernel brackets
 enum {
   EV_S0 = 0,   // step start
-  EV_S1 = 1,   // after real space
+  EV_S1 = 1,   // after real space (on the stream the pairs ran on)
   EV_S2 = 2,   // after binning + charge assignment
   EV_S3 = 3,   // after FFTs + convolution
   EV_S4 = 4,   // after back-interpolation + self-force
@@ -158,6 +163,7 @@ enum {
   EV_K3 = 8,
   EV_K4 = 9,   // gather kernel start / end
   EV_K5 = 10,
+  EV_S1K = 11,  // start of the k-space chain (after the pairs, or beside them on stream2)
 };
 
 inline void mark(Ctx *c, int slot) {
