@@ -321,6 +321,10 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
       st = P3MG_ERR_CUDA;
       break;
     }
+    // equal priorities: with the k-space stream ahead, its gather and the
+    // pair kernel share SMs and both slow down (they lean on the same L1 /
+    // shared-memory pipe), which measured slower than letting them follow
+    // the launch order
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
