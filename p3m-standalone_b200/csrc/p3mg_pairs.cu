@@ -24,7 +24,13 @@
 // forward columns, and the partner's force goes into a shared-memory
 // accumulator per staged candidate that is added to the global forces with
 // FP64 atomics at the end of the chunk (the particle's own force likewise).
-// About 90 M evaluations instead of 180 M at the headline workload.
+// About 90 M evaluations instead of 180 M at the headline workload.  The
+// partner accumulators are 32-bit fixed point (shared-memory integer adds
+// are single native atomics, float adds are not): with the chunk's scale
+// S = 2^20 / (max|q_i| max|q_j| max(alpha^2, 1/rcut^2)) a contribution below
+// 2^20 units is added there, a larger one (the closest pairs) goes straight
+// to the global FP64 force; a chunk adds at most 64 contributions per
+// partner, so no accumulator can overflow.
 //
 // FP64 keeps every ordered pair, each particle's force summed by one warp in
 // a fixed order (bit-reproducible from run to run): a conservative FP32
@@ -169,6 +175,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
   __shared__ double cell_off[27][3];
   __shared__ double ered[PAIR_WARPS];
+  __shared__ float qmax_i_w[PAIR_WARPS], qmax_j_w[PAIR_WARPS];  // FP32: |q| maxima of the i batch / staged chunk
+  int *sfji = reinterpret_cast<int *>(sfj);                        // FP32: fixed-point partner forces
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned short *q = queue + warp * PAIR_QCAP;
   const int cell = blockIdx.x;
@@ -231,20 +239,28 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   for (int ib = i0; ib < i1; ib += MAXI) {
     const int ni = min(MAXI, i1 - ib);
     __syncthreads();
+    float qmi = 0.0f;
     for (int t = tid; t < ni; t += PAIR_CTA) {
       if (DBL) {
         const double4 p = pos64[ib + t];
         spi[t] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz), (float)p.w);
       } else {
-        spi[t] = pos32[ib + t];
+        const float4 p = pos32[ib + t];
+        spi[t] = p;
+        qmi = fmaxf(qmi, fabsf(p.w));
       }
       sfi[3 * t] = sfi[3 * t + 1] = sfi[3 * t + 2] = (acc_t)0;
+    }
+    if (N3) {
+      qmi = __int_as_float(__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(qmi)));
+      if (lane == 0) qmax_i_w[warp] = qmi;
     }
     // all candidates in one chunk when they fit (pruned columns), else chunks
     // of the flat candidate order
     for (int k0 = 0; k0 < total; k0 += JCH) {
       const int kn = min(JCH, total - k0);
       __syncthreads();
+      float qmj = 0.0f;
 #pragma unroll 4
       for (int kk = tid; kk < kn; kk += PAIR_CTA) {
         const int k = k0 + kk;
@@ -256,7 +272,7 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         const int J0 = sg / 36, J1 = (sg / 6) % 6, J2 = sg % 6;
         const int cidx = ((J0 / 2) * 3 + J1 / 2) * 3 + J2 / 2;
         csrc[kk] = src;
-        if (N3) sfj[3 * kk] = sfj[3 * kk + 1] = sfj[3 * kk + 2] = 0.0f;
+        if (N3) sfji[3 * kk] = sfji[3 * kk + 1] = sfji[3 * kk + 2] = 0;
         if (DBL) {
           const double4 p = pos64[src];
           cf[kk] = make_float4((float)(p.x + cell_off[cidx][0] - ox), (float)(p.y + cell_off[cidx][1] - oy),
@@ -265,9 +281,29 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
           const float4 p = pos32[src];
           cf[kk] = make_float4(p.x + (float)cell_off[cidx][0], p.y + (float)cell_off[cidx][1],
                                p.z + (float)cell_off[cidx][2], p.w);
+          qmj = fmaxf(qmj, fabsf(p.w));
         }
       }
+      if (N3) {
+        qmj = __int_as_float(__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(qmj)));
+        if (lane == 0) qmax_j_w[warp] = qmj;
+      }
       __syncthreads();
+      // FP32: fixed-point scale of the partner accumulators for this chunk
+      float fxs = 0.0f, fxs_inv = 0.0f;
+      if (N3) {
+        float qi = 0.0f, qj = 0.0f;
+#pragma unroll
+        for (int w = 0; w < PAIR_WARPS; w++) {
+          qi = fmaxf(qi, qmax_i_w[w]);
+          qj = fmaxf(qj, qmax_j_w[w]);
+        }
+        const float fscale = qi * qj * fmaxf(alphaf * alphaf, 1.0f / ((float)rcut * (float)rcut));
+        if (fscale > 0.0f) {
+          fxs = 1048576.0f / fscale;
+          fxs_inv = fscale * (1.0f / 1048576.0f);
+        }
+      }
       for (int il = warp; il < ni; il += PAIR_WARPS) {
         const float4 pif = spi[il];
         double4 pid = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -315,9 +351,18 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               fy += fak * ey;
               fz += fak * ez;
               if (N3) {
-                atomicAdd(&sfj[3 * sl], -fak * ex);
-                atomicAdd(&sfj[3 * sl + 1], -fak * ey);
-                atomicAdd(&sfj[3 * sl + 2], -fak * ez);
+                const float gx = -fak * ex, gy = -fak * ey, gz = -fak * ez;
+                const float sx = gx * fxs, sy = gy * fxs, sz = gz * fxs;
+                if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < 1048576.0f) {
+                  atomicAdd(&sfji[3 * sl], __float2int_rn(sx));
+                  atomicAdd(&sfji[3 * sl + 1], __float2int_rn(sy));
+                  atomicAdd(&sfji[3 * sl + 2], __float2int_rn(sz));
+                } else {
+                  const int o = sidx[csrc[sl]];
+                  atomicAdd(&fr[o], (double)gx);
+                  atomicAdd(&fr[(size_t)n + o], (double)gy);
+                  atomicAdd(&fr[2 * (size_t)n + o], (double)gz);
+                }
               }
               const float term = (N3 ? 1.0f : 0.5f) * qq * ec * rinv - e_comp;
               const float tsum = e_sum + term;
@@ -414,8 +459,9 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         // the partners' forces of this chunk, added to the global forces
         __syncthreads();
         for (int kk = tid; kk < kn; kk += PAIR_CTA) {
-          const float gx = sfj[3 * kk], gy = sfj[3 * kk + 1], gz = sfj[3 * kk + 2];
-          if (gx != 0.0f || gy != 0.0f || gz != 0.0f) {
+          const int ix = sfji[3 * kk], iy = sfji[3 * kk + 1], iz = sfji[3 * kk + 2];
+          if (ix != 0 || iy != 0 || iz != 0) {
+            const float gx = (float)ix * fxs_inv, gy = (float)iy * fxs_inv, gz = (float)iz * fxs_inv;
             const int o = sidx[csrc[kk]];
             atomicAdd(&fr[o], (double)gx);
             atomicAdd(&fr[(size_t)n + o], (double)gy);
