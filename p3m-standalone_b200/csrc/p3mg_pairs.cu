@@ -28,9 +28,9 @@
 // partner accumulators are 32-bit fixed point (shared-memory integer adds
 // are single native atomics, float adds are not): with the chunk's scale
 // S = 2^20 / (max|q_i| max|q_j| max(alpha^2, 1/rcut^2)) a contribution below
-// 2^20 units is added there, a larger one (the closest pairs) goes straight
+// 2^24 units is added there, a larger one (the closest pairs) goes straight
 // to the global FP64 force; a chunk adds at most 64 contributions per
-// partner, so no accumulator can overflow.
+// partner, so no accumulator passes 2^30.
 //
 // FP64 keeps every ordered pair, each particle's force summed by one warp in
 // a fixed order (bit-reproducible from run to run): a conservative FP32
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               if (N3) {
                 const float gx = -fak * ex, gy = -fak * ey, gz = -fak * ez;
                 const float sx = gx * fxs, sy = gy * fxs, sz = gz * fxs;
-                if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < 1048576.0f) {
+                if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < 16777216.0f) {
                   atomicAdd(&sfji[3 * sl], __float2int_rn(sx));
                   atomicAdd(&sfji[3 * sl + 1], __float2int_rn(sy));
                   atomicAdd(&sfji[3 * sl + 2], __float2int_rn(sz));
