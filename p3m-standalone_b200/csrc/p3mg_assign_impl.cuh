@@ -38,13 +38,14 @@ __host__ __device__ constexpr size_t scatter_stage_bytes() {
 // global atomic per non-zero tile point).
 //
 // FP32: the tile accumulates in 32-bit fixed point with the brick's own
-// scale S = 2^30 / sum |q| over the brick's particles -- shared-memory
-// integer adds are single native atomics where float adds are not, and
-// no tile point can overflow (every weight product is <= 1, so a point's
-// sum stays within 2^30 plus half a unit per contribution).  The resolution
-// sum |q| / 2^30 is below the FP32 rounding of the contributions for the
-// few hundred particles of a brick; integer sums also make the tile
-// independent of the order of the atomics.  FP64 accumulates doubles.
+// scale S = (0.999 * 2^31 - n_brick / 2) / (sum |q| w_max^3) over the
+// brick's particles, w_max the largest weight of the order (0.511 for
+// cao 7) -- shared-memory integer adds are single native atomics where
+// float adds are not.  No tile point can overflow: its sum is at most
+// sum |q| w_max^3 plus half a unit of rounding per contribution.  The
+// resolution is below the FP32 rounding of the contributions for the few
+// hundred particles of a brick at density 1; integer sums also make the
+// tile independent of the order of the atomics.  FP64 accumulates doubles.
 template <typename real, int CAO, int NMESH>
 __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *__restrict__ sxyzq,
                                                                   const int *__restrict__ start, int m, int B, int nb,
@@ -67,9 +68,11 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
   if (p0 == p1) return;
   for (int t = threadIdx.x; t < NMESH * T3; t += blockDim.x) tile0[t] = (acc_t)0;
   // FP32: fixed-point scale of this brick from sum |q| (rounded up a little
-  // so the bound survives the summation's rounding)
+  // so the bound survives the summation's rounding) and the largest weight
   real scale = (real)1, inv_scale = (real)1;
   if (FIXED) {
+    // max over the in-cell offset of the order-CAO weights, rounded up
+    constexpr double wmax = CAO <= 2 ? 1.0 : CAO == 3 ? 0.75 : CAO == 4 ? 0.66667 : CAO == 5 ? 0.59896 : CAO == 6 ? 0.55001 : 0.51103;
     __shared__ double qsum_w[ASSIGN_THREADS / 32];
     double qs = 0.0;
     for (int p = p0 + (int)threadIdx.x; p < p1; p += blockDim.x) qs += fabs(sxyzq[p].w);
@@ -79,9 +82,10 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
     __syncthreads();
     double R = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); w++) R += qsum_w[w];
-    R *= 1.0 + 1e-6;
-    scale = R > 0.0 ? (real)(1073741824.0 / R) : (real)0;
-    inv_scale = (real)(R / 1073741824.0);
+    const double bound = R * (1.0 + 1e-6) * wmax * wmax * wmax;
+    const double units = 0.999 * 2147483648.0 - 0.5 * (double)(p1 - p0);
+    scale = bound > 0.0 ? (real)(units / bound) : (real)0;
+    inv_scale = bound > 0.0 ? (real)(bound / units) : (real)0;
   }
   const int bz = bid % nb, by = (bid / nb) % nb, bx = bid / (nb * nb);
   const int o0 = bx * B, o1 = by * B, o2 = bz * B;

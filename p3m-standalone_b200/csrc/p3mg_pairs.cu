@@ -26,11 +26,12 @@
 // FP64 atomics at the end of the chunk (the particle's own force likewise).
 // About 90 M evaluations instead of 180 M at the headline workload.  The
 // partner accumulators are 32-bit fixed point (shared-memory integer adds
-// are single native atomics, float adds are not): with the chunk's scale
-// S = 2^20 / (max|q_i| max|q_j| max(alpha^2, 1/rcut^2)) a contribution below
-// 2^24 units is added there, a larger one (the closest pairs) goes straight
-// to the global FP64 force; a chunk adds at most 64 contributions per
-// partner, so no accumulator passes 2^30.
+// are single native atomics, float adds are not): partner j's scale is
+// S_j = 2^20 / (|q_j| max|q_i| max(alpha^2, 1/rcut^2)) with the maximum over
+// the i batch, so its resolution follows its own charge; a contribution
+// below 2^24 units is added there, a larger one (the closest pairs) goes
+// straight to the global FP64 force; a chunk adds at most 64 contributions
+// per partner, so no accumulator passes 2^30.
 //
 // FP64 keeps every ordered pair, each particle's force summed by one warp in
 // a fixed order (bit-reproducible from run to run): a conservative FP32
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
   __shared__ double cell_off[27][3];
   __shared__ double ered[PAIR_WARPS];
-  __shared__ float qmax_i_w[PAIR_WARPS], qmax_j_w[PAIR_WARPS];  // FP32: |q| maxima of the i batch / staged chunk
+  __shared__ float qmax_i_w[PAIR_WARPS];                         // FP32: |q| maxima of the i batch
   int *sfji = reinterpret_cast<int *>(sfj);                        // FP32: fixed-point partner forces
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   unsigned short *q = queue + warp * PAIR_QCAP;
@@ -260,7 +261,6 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
     for (int k0 = 0; k0 < total; k0 += JCH) {
       const int kn = min(JCH, total - k0);
       __syncthreads();
-      float qmj = 0.0f;
 #pragma unroll 4
       for (int kk = tid; kk < kn; kk += PAIR_CTA) {
         const int k = k0 + kk;
@@ -281,24 +281,17 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
           const float4 p = pos32[src];
           cf[kk] = make_float4(p.x + (float)cell_off[cidx][0], p.y + (float)cell_off[cidx][1],
                                p.z + (float)cell_off[cidx][2], p.w);
-          qmj = fmaxf(qmj, fabsf(p.w));
         }
-      }
-      if (N3) {
-        qmj = __int_as_float(__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(qmj)));
-        if (lane == 0) qmax_j_w[warp] = qmj;
       }
       __syncthreads();
-      // FP32: fixed-point scale of the partner accumulators for this chunk
+      // FP32: fixed-point scale of the partner accumulators for this chunk,
+      // divided by |q_j| per partner
       float fxs = 0.0f, fxs_inv = 0.0f;
       if (N3) {
-        float qi = 0.0f, qj = 0.0f;
+        float qi = 0.0f;
 #pragma unroll
-        for (int w = 0; w < PAIR_WARPS; w++) {
-          qi = fmaxf(qi, qmax_i_w[w]);
-          qj = fmaxf(qj, qmax_j_w[w]);
-        }
-        const float fscale = qi * qj * fmaxf(alphaf * alphaf, 1.0f / ((float)rcut * (float)rcut));
+        for (int w = 0; w < PAIR_WARPS; w++) qi = fmaxf(qi, qmax_i_w[w]);
+        const float fscale = qi * fmaxf(alphaf * alphaf, 1.0f / ((float)rcut * (float)rcut));
         if (fscale > 0.0f) {
           fxs = 1048576.0f / fscale;
           fxs_inv = fscale * (1.0f / 1048576.0f);
@@ -352,7 +345,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               fz += fak * ez;
               if (N3) {
                 const float gx = -fak * ex, gy = -fak * ey, gz = -fak * ez;
-                const float sx = gx * fxs, sy = gy * fxs, sz = gz * fxs;
+                const float sj = (pj.w != 0.0f) ? __fdividef(fxs, fabsf(pj.w)) : 0.0f;
+                const float sx = gx * sj, sy = gy * sj, sz = gz * sj;
                 if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < 16777216.0f) {
                   atomicAdd(&sfji[3 * sl], __float2int_rn(sx));
                   atomicAdd(&sfji[3 * sl + 1], __float2int_rn(sy));
@@ -461,7 +455,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         for (int kk = tid; kk < kn; kk += PAIR_CTA) {
           const int ix = sfji[3 * kk], iy = sfji[3 * kk + 1], iz = sfji[3 * kk + 2];
           if (ix != 0 || iy != 0 || iz != 0) {
-            const float gx = (float)ix * fxs_inv, gy = (float)iy * fxs_inv, gz = (float)iz * fxs_inv;
+            const float inv = fxs_inv * fabsf(cf[kk].w);
+            const float gx = (float)ix * inv, gy = (float)iy * inv, gz = (float)iz * inv;
             const int o = sidx[csrc[kk]];
             atomicAdd(&fr[o], (double)gx);
             atomicAdd(&fr[(size_t)n + o], (double)gy);
