@@ -146,6 +146,26 @@ def profile_traffic(kernel):
     return None if v is None else float(v)
 
 
+# ------------------------------------------------------------- replicas
+
+def reduce_max(v, dist=None, device="cpu"):
+    """Max of v over the ranks of the process group (v itself without one).
+    NCCL needs a CUDA tensor (device = the rank's GPU); gloo a CPU one."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(ms_per_step_max, world):
+    """Whole-job steps/s of `world` independent replicas (one system per rank,
+    no collective on the data path) whose slowest rank takes ms_per_step_max
+    per step."""
+    return world * 1000.0 / ms_per_step_max
+
+
 # ------------------------------------------------------------- our arm
 
 def run_ours(args, rank, world, local_rank):
@@ -166,11 +186,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, dist, dev)
 
     W = WORKLOAD
     n = args.n or W["n"]
@@ -266,8 +282,8 @@ def run_ours(args, rank, world, local_rank):
                     "rms_error_fp32": _rms(r32["forces"]), "rms_error_fp64": _rms(r64["forces"]),
                     "rms_fp32_vs_fp64": float(np.sqrt(np.sum((r32["forces"][:, tg] - r64["forces"][:, tg]) ** 2)
                                                      / len(tg)))}
-    value = world * 1000.0 / r32["ms"]
-    e2e = world * 1000.0 / r32["e2e_ms"]
+    value = replica_throughput(r32["ms"], world)
+    e2e = replica_throughput(r32["e2e_ms"], world)
 
     out = None
     if rank == 0:
@@ -326,8 +342,9 @@ def run_ours(args, rank, world, local_rank):
                        "mesh": W["mesh"], "cao": W["cao"], "rcut": W["rcut"], "alpha": W["alpha"], "mc": W["mc"],
                        "parallelism": "replicas%d" % world if world > 1 else "single-gpu",
                        "l2": "flushed between timed steps (256 MB write, untimed)"},
-            "fp64": {"value": round(world * 1000.0 / r64["ms"], 3), "unit": "steps/s",
-                     "ms_per_step": round(r64["ms"], 4), "e2e_steps_per_s": round(world * 1000.0 / r64["e2e_ms"], 3)},
+            "fp64": {"value": round(replica_throughput(r64["ms"], world), 3), "unit": "steps/s",
+                     "ms_per_step": round(r64["ms"], 4),
+                     "e2e_steps_per_s": round(replica_throughput(r64["e2e_ms"], world), 3)},
             "fp32_over_fp64": round(r64["ms"] / r32["ms"], 3),
             "stages_ms": {"fp32": {k2: round(v, 4) for k2, v in r32["stages"].items()},
                           "fp64": {k2: round(v, 4) for k2, v in r64["stages"].items()}},
