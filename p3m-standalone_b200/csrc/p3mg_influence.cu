@@ -35,10 +35,134 @@ __device__ __forceinline__ double signed_freq(int i, int m) {
   return (double)i - round((double)i / (double)m) * (double)m;
 }
 
-// dG (may be NULL): dG/dalpha as well (each exp(-(pi/alpha)^2 |n|^2)
-// factor differentiated; the rest of the formula is linear in those sums).
+// G_opt at one mesh point (NX, NY, NZ) away from the zeroed ones, and with
+// want_dg dG/dalpha (each exp(-(pi/alpha)^2 |n|^2) factor differentiated; the
+// rest of the formula is linear in those sums).  MC >= 0: the alias range
+// mc == MC fixed at compile time, so the per-axis sinc powers and Gaussian
+// factors of the (2 MC + 1) aliases are tabulated once (3 (2MC+1) sin and
+// exp instead of (2MC+1)^3; the Gaussian of an alias is the product of its
+// three axis factors).  MC < 0: any mc, evaluated alias by alias.
+template <int MC>
+__device__ __forceinline__ void influence_point(int method, int m, int cao, int mc, double alpha, double L, int NX,
+                                                int NY, int NZ, bool want_dg, double *g_out, double *dg_out) {
+  const int half = m / 2;
+  const bool ad = method_ad(method);
+  const bool ik_sq = (method == 0 || method == 6);  // (sinc^cao)^2, else sinc^(2 cao)
+  const double Leni = 1.0 / L, fak1 = 1.0 / (double)m;
+  const double pa = P3MG_PI / alpha;
+  const double fak2 = pa * pa;
+  const double nx = signed_freq(NX, m), ny = signed_freq(NY, m), nz = signed_freq(NZ, m);
+  double Zx = 0.0, Zy = 0.0, Zz = 0.0, Z = 0.0, N1 = 0.0, N2 = 0.0, N3 = 0.0, N4 = 0.0;
+  double dZx = 0.0, dZy = 0.0, dZz = 0.0, dZ = 0.0;
+  const double dfac = 2.0 * fak2 / alpha;  // d/dalpha of -fak2 NM2 is dfac NM2
+  // one alias term: S3 the product of the sinc powers, NM* the shifted
+  // frequencies, TE the Gaussian, par the parity of MX + MY + MZ
+  auto term = [&](double S3, double NMX, double NMY, double NMZ, double NM2, double TE, bool even) {
+    const double dTE = want_dg ? TE * NM2 * dfac : 0.0;
+    N1 += S3;
+    if (ad) {
+      N2 += S3 * NM2;
+      N3 += even ? S3 : -S3;
+      N4 += even ? S3 * NM2 : -(S3 * NM2);
+      Z += S3 * TE;
+      dZ += S3 * dTE;
+    } else {
+      const double zwi = S3 * TE / NM2;
+      Zx += NMX * zwi * Leni;
+      Zy += NMY * zwi * Leni;
+      Zz += NMZ * zwi * Leni;
+      if (want_dg) {
+        const double dzwi = S3 * dTE / NM2;
+        dZx += NMX * dzwi * Leni;
+        dZy += NMY * dzwi * Leni;
+        dZz += NMZ * dzwi * Leni;
+      }
+      N2 += even ? S3 : -S3;
+    }
+  };
+  if constexpr (MC >= 0) {
+    constexpr int NA = 2 * MC + 1;
+    double Nx[NA], Ny[NA], Nz[NA], Sx[NA], Sy[NA], Sz[NA], Ex[NA], Ey[NA], Ez[NA];
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      const double shift = (double)(m * (i - MC));
+      Nx[i] = nx + shift;
+      Ny[i] = ny + shift;
+      Nz[i] = nz + shift;
+      const double sx = sinc_pi(fak1 * Nx[i]), sy = sinc_pi(fak1 * Ny[i]), sz = sinc_pi(fak1 * Nz[i]);
+      Sx[i] = ik_sq ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
+      Sy[i] = ik_sq ? ipow_d(ipow_d(sy, cao), 2) : ipow_d(sy, 2 * cao);
+      Sz[i] = ik_sq ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao);
+      const double a = Nx[i] * Leni, b = Ny[i] * Leni, c = Nz[i] * Leni;
+      Ex[i] = exp(-fak2 * (a * a));
+      Ey[i] = exp(-fak2 * (b * b));
+      Ez[i] = exp(-fak2 * (c * c));
+    }
+#pragma unroll
+    for (int i = 0; i < NA; i++)
+#pragma unroll
+      for (int j = 0; j < NA; j++) {
+        const double S2 = Sx[i] * Sy[j];
+        const double Exy = Ex[i] * Ey[j];
+#pragma unroll
+        for (int k = 0; k < NA; k++) {
+          const double a = Nx[i] * Leni, b = Ny[j] * Leni, cc = Nz[k] * Leni;
+          const double NM2 = a * a + b * b + cc * cc;
+          term(S2 * Sz[k], Nx[i], Ny[j], Nz[k], NM2, Exy * Ez[k], ((i + j + k - 3 * MC) % 2) == 0);
+        }
+      }
+  } else {
+    for (int MX = -mc; MX <= mc; MX++) {
+      const double NMX = nx + (double)(m * MX);
+      const double sx = sinc_pi(fak1 * NMX);
+      const double S1 = ik_sq ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
+      for (int MY = -mc; MY <= mc; MY++) {
+        const double NMY = ny + (double)(m * MY);
+        const double sy = sinc_pi(fak1 * NMY);
+        const double S2 = S1 * (ik_sq ? ipow_d(ipow_d(sy, cao), 2) : ipow_d(sy, 2 * cao));
+        for (int MZ = -mc; MZ <= mc; MZ++) {
+          const double NMZ = nz + (double)(m * MZ);
+          const double sz = sinc_pi(fak1 * NMZ);
+          const double S3 = S2 * (ik_sq ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao));
+          const double a = NMX * Leni, b = NMY * Leni, cc = NMZ * Leni;
+          const double NM2 = a * a + b * b + cc * cc;
+          term(S3, NMX, NMY, NMZ, NM2, exp(-fak2 * NM2), ((MX + MY + MZ) % 2) == 0);
+        }
+      }
+    }
+  }
+  double g, dg = 0.0;
+  if (ad) {
+    const double den = (method == 3) ? (0.5 * P3MG_PI * (N1 * N2 + N3 * N4)) : (P3MG_PI * N1 * N2);
+    g = Z / den;
+    if (want_dg) dg = dZ / den;
+  } else {
+    const double Dx = (NX == half) ? 0.0 : nx, Dy = (NY == half) ? 0.0 : ny, Dz = (NZ == half) ? 0.0 : nz;
+    double num = Dx * Zx * Leni + Dy * Zy * Leni + Dz * Zz * Leni;
+    double dnum = Dx * dZx * Leni + Dy * dZy * Leni + Dz * dZz * Leni;
+    const double dxl = Dx * Leni, dyl = Dy * Leni, dzl = Dz * Leni;
+    const double d2 = dxl * dxl + dyl * dyl + dzl * dzl;
+    if (method == 1) {
+      num /= d2;
+      num /= 0.5 * (N1 * N1 + N2 * N2);
+      dnum /= d2;
+      dnum /= 0.5 * (N1 * N1 + N2 * N2);
+    } else {
+      num /= d2 * (N1 * N1);
+      dnum /= d2 * (N1 * N1);
+    }
+    g = 2.0 * num / P3MG_PI;
+    dg = 2.0 * dnum / P3MG_PI;
+  }
+  *g_out = g;
+  *dg_out = dg;
+}
+
+// dG (may be NULL): dG/dalpha as well.  MC: see influence_point (launch
+// through launch_influence, which picks it from mc).
+template <int MC>
 __global__ void influence_kernel(double *__restrict__ G, int method, int m, int cao, int mc, double alpha_v,
-                                 const double *__restrict__ alphas, double L, double *__restrict__ dG = nullptr) {
+                                 const double *__restrict__ alphas, double L, double *__restrict__ dG) {
   const size_t M = (size_t)m * m * m;
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ind >= M) return;
@@ -65,78 +189,22 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
     if (dG) dG[ind] = 0.0;
     return;
   }
-  const double Leni = 1.0 / L, fak1 = 1.0 / (double)m;
-  const double pa = P3MG_PI / alpha;
-  const double fak2 = pa * pa;
-  const double nx = signed_freq(NX, m), ny = signed_freq(NY, m), nz = signed_freq(NZ, m);
-  double Zx = 0.0, Zy = 0.0, Zz = 0.0, Z = 0.0, N1 = 0.0, N2 = 0.0, N3 = 0.0, N4 = 0.0;
-  double dZx = 0.0, dZy = 0.0, dZz = 0.0, dZ = 0.0;
-  const double dfac = 2.0 * fak2 / alpha;  // d/dalpha of -fak2 NM2 is dfac NM2
-  for (int MX = -mc; MX <= mc; MX++) {
-    const double NMX = nx + (double)(m * MX);
-    const double sx = sinc_pi(fak1 * NMX);
-    const double S1 = (method == 0 || method == 6) ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
-    for (int MY = -mc; MY <= mc; MY++) {
-      const double NMY = ny + (double)(m * MY);
-      const double sy = sinc_pi(fak1 * NMY);
-      const double S2 = S1 * ((method == 0 || method == 6) ? ipow_d(ipow_d(sy, cao), 2) : ipow_d(sy, 2 * cao));
-      for (int MZ = -mc; MZ <= mc; MZ++) {
-        const double NMZ = nz + (double)(m * MZ);
-        const double sz = sinc_pi(fak1 * NMZ);
-        const double S3 = S2 * ((method == 0 || method == 6) ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao));
-        const double a = NMX * Leni, b = NMY * Leni, cc = NMZ * Leni;
-        const double NM2 = a * a + b * b + cc * cc;
-        const double TE = exp(-fak2 * NM2);
-        const double dTE = dG ? TE * NM2 * dfac : 0.0;
-        const bool even = ((MX + MY + MZ) % 2) == 0;
-        N1 += S3;
-        if (ad) {
-          N2 += S3 * NM2;
-          N3 += even ? S3 : -S3;
-          N4 += even ? S3 * NM2 : -(S3 * NM2);
-          Z += S3 * TE;
-          dZ += S3 * dTE;
-        } else {
-          const double zwi = S3 * TE / NM2;
-          Zx += NMX * zwi * Leni;
-          Zy += NMY * zwi * Leni;
-          Zz += NMZ * zwi * Leni;
-          if (dG) {
-            const double dzwi = S3 * dTE / NM2;
-            dZx += NMX * dzwi * Leni;
-            dZy += NMY * dzwi * Leni;
-            dZz += NMZ * dzwi * Leni;
-          }
-          N2 += even ? S3 : -S3;
-        }
-      }
-    }
-  }
-  double g, dg = 0.0;
-  if (ad) {
-    const double den = (method == 3) ? (0.5 * P3MG_PI * (N1 * N2 + N3 * N4)) : (P3MG_PI * N1 * N2);
-    g = Z / den;
-    if (dG) dg = dZ / den;
-  } else {
-    const double Dx = (NX == half) ? 0.0 : nx, Dy = (NY == half) ? 0.0 : ny, Dz = (NZ == half) ? 0.0 : nz;
-    double num = Dx * Zx * Leni + Dy * Zy * Leni + Dz * Zz * Leni;
-    double dnum = Dx * dZx * Leni + Dy * dZy * Leni + Dz * dZz * Leni;
-    const double dxl = Dx * Leni, dyl = Dy * Leni, dzl = Dz * Leni;
-    const double d2 = dxl * dxl + dyl * dyl + dzl * dzl;
-    if (method == 1) {
-      num /= d2;
-      num /= 0.5 * (N1 * N1 + N2 * N2);
-      dnum /= d2;
-      dnum /= 0.5 * (N1 * N1 + N2 * N2);
-    } else {
-      num /= d2 * (N1 * N1);
-      dnum /= d2 * (N1 * N1);
-    }
-    g = 2.0 * num / P3MG_PI;
-    dg = 2.0 * dnum / P3MG_PI;
-  }
+  double g, dg;
+  influence_point<MC>(method, m, cao, mc, alpha, L, NX, NY, NZ, dG != nullptr, &g, &dg);
   G[ind] = g;
   if (dG) dG[ind] = dg;
+}
+
+// G (and dG) for grid (blocks, na) on the stream
+void launch_influence(double *G, int method, int m, int cao, int mc, double alpha, const double *alphas, double L,
+                      double *dG, unsigned blocks, int na, int threads, cudaStream_t st) {
+  const dim3 grid(blocks, na);
+  switch (mc) {
+    case 0: influence_kernel<0><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
+    case 1: influence_kernel<1><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
+    case 2: influence_kernel<2><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
+    default: influence_kernel<-1><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
+  }
 }
 
 // ad self-force sums S(m') for the 26 non-zero m' in {-1,0,1}^3
@@ -245,8 +313,7 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
-  influence_kernel<<<dim3(blocks, na), threads, 0, c->stream>>>(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas,
-                                                                 c->L);
+  launch_influence(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas, c->L, nullptr, blocks, na, threads, c->stream);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   if (method_self_force(c->method)) {
@@ -266,8 +333,8 @@ int influence_with_derivative(Ctx *c, double *G_out, double *dG_out) {
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
-  influence_kernel<<<blocks, threads, 0, c->stream>>>(G_out, c->method, c->mesh, c->cao, c->mc, c->alpha, nullptr,
-                                                       c->L, dG_out);
+  launch_influence(G_out, c->method, c->mesh, c->cao, c->mc, c->alpha, nullptr, c->L, dG_out, blocks, 1, threads,
+                   c->stream);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
@@ -278,7 +345,7 @@ int influence_compute(Ctx *c, double alpha) {
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
-  influence_kernel<<<blocks, threads, 0, c->stream>>>(c->G, c->method, m, c->cao, c->mc, alpha, nullptr, c->L);
+  launch_influence(c->G, c->method, m, c->cao, c->mc, alpha, nullptr, c->L, nullptr, blocks, 1, threads, c->stream);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   if (c->precision != P3MG_FP64) {
