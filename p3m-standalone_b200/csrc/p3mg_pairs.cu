@@ -123,16 +123,24 @@ constexpr int PAIR_MAXI32 = 64;  // FP32 (cells hold about 46 at density 1)
 constexpr int PAIR_QCAP = 64;    // circular queue per warp (power of two)
 constexpr int PAIR_NSEG = 216;   // 6x6x6 half-cells around the cell
 
-__host__ __device__ constexpr int pair_jch(bool dbl) { return dbl ? PAIR_JCH : PAIR_JCH32; }
+// Newton's third law: FP32 with one alpha per CTA (see pairs_cell_kernel)
+__host__ __device__ constexpr bool pair_n3(bool dbl, int na) { return !dbl && na == 1; }
+__host__ __device__ constexpr int pair_jch(bool dbl, int na) { return pair_n3(dbl, na) ? PAIR_JCH32 : PAIR_JCH; }
 __host__ __device__ constexpr int pair_maxi(bool dbl) { return dbl ? PAIR_MAXI : PAIR_MAXI32; }
 
-// staged positions, sorted slots, (FP32) partner-force accumulators, the
-// i batch and its forces, the warp queues
-__host__ __device__ constexpr size_t pair_smem_bytes(bool dbl) {
-  return (size_t)pair_jch(dbl) * (sizeof(float4) + sizeof(int) + (dbl ? 0 : 3 * sizeof(float))) +
-         (size_t)pair_maxi(dbl) * sizeof(float4) + (size_t)pair_maxi(dbl) * 3 * (dbl ? sizeof(double) : sizeof(float)) +
+// staged positions, sorted slots, (Newton-3) partner-force accumulators,
+// the i batch and its forces per alpha of the group, the warp queues
+__host__ __device__ constexpr size_t pair_smem_bytes(bool dbl, int na) {
+  return (size_t)pair_jch(dbl, na) * (sizeof(float4) + sizeof(int) + (pair_n3(dbl, na) ? 3 * sizeof(float) : 0)) +
+         (size_t)pair_maxi(dbl) * sizeof(float4) +
+         (size_t)pair_maxi(dbl) * 3 * na * (dbl ? sizeof(double) : sizeof(float)) +
          (size_t)PAIR_WARPS * PAIR_QCAP * sizeof(unsigned short);
 }
+
+// alphas per CTA in an alpha batch: the candidate search is shared by the
+// group, each pair is evaluated for every alpha of it
+constexpr int PAIR_NA32 = 8;
+constexpr int PAIR_NA64 = 4;
 
 template <bool DBL>
 struct PairAcc {
@@ -143,27 +151,33 @@ struct PairAcc<true> {
   typedef double type;
 };
 
-template <bool DBL>
+template <bool DBL, int NA>
 __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__restrict__ posv,
                                                                const int *__restrict__ sidx,
                                                                const int *__restrict__ start, int nc, double L,
                                                                double rcut, double alpha_v,
-                                                               const double *__restrict__ alphas,
+                                                               const double *__restrict__ alphas, int nalpha,
                                                                double *__restrict__ fr, int n,
                                                                double *__restrict__ energy) {
   typedef typename PairAcc<DBL>::type acc_t;
-  // alpha batch: grid.y = alpha index (alphas on the device), outputs per
-  // alpha at fr + 3 n y and energy + y; without alphas the scalar alpha_v
-  const double alpha = alphas ? alphas[blockIdx.y] : alpha_v;
-  fr += (size_t)blockIdx.y * 3 * (size_t)n;
-  energy += blockIdx.y;
-  // FP32: Newton's third law -- each pair once, by the CTA of the particle
-  // that comes first in the staged (J0, J1, J2, slot) order, with the
-  // partner's force accumulated in shared memory and added atomically.
-  // FP64 keeps every ordered pair (the reference's loop, reproducible bit
-  // for bit from run to run).
-  constexpr bool N3 = !DBL;
-  constexpr int JCH = pair_jch(DBL);
+  // alpha batch: grid.y = group of NA alphas (alphas on the device), outputs
+  // per alpha k at fr + 3 n k and energy + k; without alphas the scalar alpha_v
+  const int a0 = blockIdx.y * NA;
+  const int nag = alphas ? min(NA, nalpha - a0) : 1;
+  double alpha_g[NA];
+#pragma unroll
+  for (int a = 0; a < NA; a++) alpha_g[a] = alphas ? (a < nag ? alphas[a0 + a] : 0.0) : alpha_v;
+  const double alpha = alpha_g[0];
+  fr += (size_t)a0 * 3 * (size_t)n;
+  energy += a0;
+  // FP32 with one alpha per CTA: Newton's third law -- each pair once, by
+  // the CTA of the particle that comes first in the staged (J0, J1, J2,
+  // slot) order, with the partner's force accumulated in shared memory and
+  // added atomically.  FP64 keeps every ordered pair (the reference's loop,
+  // reproducible bit for bit from run to run), and so does an alpha group,
+  // whose per-alpha partner accumulators would not fit.
+  constexpr bool N3 = pair_n3(DBL, NA);
+  constexpr int JCH = pair_jch(DBL, NA);
   extern __shared__ __align__(16) unsigned char pair_smem[];
   float4 *cf = reinterpret_cast<float4 *>(pair_smem);
   int *csrc = reinterpret_cast<int *>(cf + JCH);  // sorted slot of each staged candidate
@@ -171,11 +185,11 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   float4 *spi = reinterpret_cast<float4 *>(N3 ? reinterpret_cast<unsigned char *>(sfj + 3 * JCH)
                                               : reinterpret_cast<unsigned char *>(csrc + JCH));
   constexpr int MAXI = pair_maxi(DBL);
-  acc_t *sfi = reinterpret_cast<acc_t *>(spi + MAXI);
-  unsigned short *queue = reinterpret_cast<unsigned short *>(sfi + 3 * MAXI);
+  acc_t *sfi = reinterpret_cast<acc_t *>(spi + MAXI);  // [MAXI][NA][3]
+  unsigned short *queue = reinterpret_cast<unsigned short *>(sfi + 3 * NA * MAXI);
   __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
   __shared__ double cell_off[27][3];
-  __shared__ double ered[PAIR_WARPS];
+  __shared__ double ered[PAIR_WARPS][NA];
   __shared__ float qmax_i_w[PAIR_WARPS];                         // FP32: |q| maxima of the i batch
   int *sfji = reinterpret_cast<int *>(sfj);                        // FP32: fixed-point partner forces
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -228,14 +242,26 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   const double Li = 1.0 / L;
   const double wupi = 1.77245385090551602729816748334;
   const float rc2f = DBL ? (float)(rcut * rcut * (1.0 + 1e-4)) : (float)rcut * (float)rcut;
-  const float alphaf = (float)alpha, preff = (float)(2.0 * alpha / wupi);
+  const float alphaf = (float)alpha;
+  float alphaf_g[NA], preff_g[NA];
+  double prefd_g[NA];
+#pragma unroll
+  for (int a = 0; a < NA; a++) {
+    alphaf_g[a] = (float)alpha_g[a];
+    preff_g[a] = (float)(2.0 * alpha_g[a] / wupi);
+    prefd_g[a] = 2.0 * alpha_g[a] / wupi;
+  }
   const float hf = (float)(0.5 * cs), hinvf = (float)(2.0 / cs);
   const float prune_r2 = (float)(rcut * rcut * (1.0 + 1e-4));
-  const double prefd = 2.0 * alpha / wupi;
   const float4 *pos32 = reinterpret_cast<const float4 *>(posv);
   const double4 *pos64 = reinterpret_cast<const double4 *>(posv);
-  double e_d = 0.0;
-  float e_sum = 0.0f, e_comp = 0.0f;  // compensated FP32 energy sum (Kahan)
+  double e_d[NA];
+  float e_sum[NA], e_comp[NA];  // compensated FP32 energy sums (Kahan)
+#pragma unroll
+  for (int a = 0; a < NA; a++) {
+    e_d[a] = 0.0;
+    e_sum[a] = e_comp[a] = 0.0f;
+  }
 
   for (int ib = i0; ib < i1; ib += MAXI) {
     const int ni = min(MAXI, i1 - ib);
@@ -250,7 +276,7 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         spi[t] = p;
         qmi = fmaxf(qmi, fabsf(p.w));
       }
-      sfi[3 * t] = sfi[3 * t + 1] = sfi[3 * t + 2] = (acc_t)0;
+      for (int a = 0; a < 3 * NA; a++) sfi[3 * NA * t + a] = (acc_t)0;
     }
     if (N3) {
       qmi = __int_as_float(__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(qmi)));
@@ -308,7 +334,9 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         for (int v = 1; v < 8; v++)
           if (isorted >= own_start[v]) u = v;
         const int kself = own_seg[u] + (isorted - own_start[u]) - k0;
-        acc_t fx = 0, fy = 0, fz = 0;
+        acc_t fx[NA], fy[NA], fz[NA];
+#pragma unroll
+        for (int a = 0; a < NA; a++) fx[a] = fy[a] = fz[a] = (acc_t)0;
         unsigned head = 0, tail = 0;
         // evaluate `take` queued interactions (one per lane) and pop them
         auto process = [&](int take) {
@@ -322,27 +350,35 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               const double ddz = min_image(__dadd_rn(pid.z, -pj.z), Li, L);
               const double rr = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)));
               if (rr <= rcut) {
-                const double ar = alpha * rr;
-                const double ec = erfc(ar);
-                const double fak = pid.w * pj.w * (ec / rr + prefd * exp(-ar * ar)) / (rr * rr);
-                fx += fak * ddx;
-                fy += fak * ddy;
-                fz += fak * ddz;
-                e_d += 0.5 * pid.w * pj.w * ec / rr;
+#pragma unroll
+                for (int a = 0; a < NA; a++) {
+                  if (a < nag) {
+                    const double ar = alpha_g[a] * rr;
+                    const double ec = erfc(ar);
+                    const double fak = pid.w * pj.w * (ec / rr + prefd_g[a] * exp(-ar * ar)) / (rr * rr);
+                    fx[a] += fak * ddx;
+                    fy[a] += fak * ddy;
+                    fz[a] += fak * ddz;
+                    e_d[a] += 0.5 * pid.w * pj.w * ec / rr;
+                  }
+                }
               }
             } else {
               const float4 pj = cf[sl];
               const float ex = pif.x - pj.x, ey = pif.y - pj.y, ez = pif.z - pj.z;
               const float rr2 = ex * ex + ey * ey + ez * ez;
               const float rinv = rsqrtf(rr2);
-              const float ar = alphaf * (rr2 * rinv);
+              const float qq = pif.w * pj.w;
+#pragma unroll
+              for (int a = 0; a < NA; a++) {
+                if (a >= nag) break;
+              const float ar = alphaf_g[a] * (rr2 * rinv);
               const float gs = __expf(-ar * ar);
               const float ec = erfc_fit(ar, gs);
-              const float qq = pif.w * pj.w;
-              const float fak = qq * (ec * rinv + preff * gs) * (rinv * rinv);
-              fx += fak * ex;
-              fy += fak * ey;
-              fz += fak * ez;
+              const float fak = qq * (ec * rinv + preff_g[a] * gs) * (rinv * rinv);
+              fx[a] += fak * ex;
+              fy[a] += fak * ey;
+              fz[a] += fak * ez;
               if (N3) {
                 const float gx = -fak * ex, gy = -fak * ey, gz = -fak * ez;
                 const float sj = (pj.w != 0.0f) ? __fdividef(fxs, fabsf(pj.w)) : 0.0f;
@@ -358,10 +394,11 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
                   atomicAdd(&fr[2 * (size_t)n + o], (double)gz);
                 }
               }
-              const float term = (N3 ? 1.0f : 0.5f) * qq * ec * rinv - e_comp;
-              const float tsum = e_sum + term;
-              e_comp = (tsum - e_sum) - term;
-              e_sum = tsum;
+              const float term = (N3 ? 1.0f : 0.5f) * qq * ec * rinv - e_comp[a];
+              const float tsum = e_sum[a] + term;
+              e_comp[a] = (tsum - e_sum[a]) - term;
+              e_sum[a] = tsum;
+              }
             }
           }
           head += take;
@@ -438,15 +475,19 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         }
         if (tail != head) process((int)(tail - head));
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          fx += __shfl_xor_sync(0xffffffffu, fx, o);
-          fy += __shfl_xor_sync(0xffffffffu, fy, o);
-          fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        }
-        if (lane == 0) {
-          sfi[3 * il] += fx;
-          sfi[3 * il + 1] += fy;
-          sfi[3 * il + 2] += fz;
+        for (int a = 0; a < NA; a++) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            fx[a] += __shfl_xor_sync(0xffffffffu, fx[a], o);
+            fy[a] += __shfl_xor_sync(0xffffffffu, fy[a], o);
+            fz[a] += __shfl_xor_sync(0xffffffffu, fz[a], o);
+          }
+          if (lane == 0) {
+            acc_t *si = sfi + 3 * (NA * il + a);
+            si[0] += fx[a];
+            si[1] += fy[a];
+            si[2] += fz[a];
+          }
         }
       }
       if (N3) {
@@ -473,43 +514,62 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         atomicAdd(&fr[(size_t)n + o], (double)sfi[3 * t + 1]);
         atomicAdd(&fr[2 * (size_t)n + o], (double)sfi[3 * t + 2]);
       } else {
-        fr[o] += (double)sfi[3 * t];
-        fr[(size_t)n + o] += (double)sfi[3 * t + 1];
-        fr[2 * (size_t)n + o] += (double)sfi[3 * t + 2];
+        for (int a = 0; a < nag; a++) {
+          double *fa = fr + (size_t)a * 3 * (size_t)n;
+          const acc_t *si = sfi + 3 * (NA * t + a);
+          fa[o] += (double)si[0];
+          fa[(size_t)n + o] += (double)si[1];
+          fa[2 * (size_t)n + o] += (double)si[2];
+        }
       }
     }
   }
-  double e_loc = DBL ? e_d : ((double)e_sum - (double)e_comp);
-  for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
-  if (lane == 0) ered[warp] = e_loc;
+#pragma unroll
+  for (int a = 0; a < NA; a++) {
+    double e_loc = DBL ? e_d[a] : ((double)e_sum[a] - (double)e_comp[a]);
+    for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
+    if (lane == 0) ered[warp][a] = e_loc;
+  }
   __syncthreads();
-  if (tid == 0) {
+  if (tid < nag) {
     double s = 0.0;
-    for (int w = 0; w < PAIR_WARPS; w++) s += ered[w];
-    if (s != 0.0) atomicAdd(energy, s);
+    for (int w = 0; w < PAIR_WARPS; w++) s += ered[w][tid];
+    if (s != 0.0) atomicAdd(energy + tid, s);
   }
 }
 
 // Launch the cell kernel (FP64 or FP32 positions, already half-cell sorted).
+// An alpha batch (alphas with nalpha > 1) runs in groups of PAIR_NA32 /
+// PAIR_NA64 alphas per CTA.
+template <bool DBL, int NA>
+int launch_cells_na(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
+                    const double *alphas, int nalpha, double *fr, int n, double *energy, cudaStream_t s) {
+  static bool attr_set = false;
+  const size_t smem = pair_smem_bytes(DBL, NA);
+  if (!attr_set) {
+    P3MG_CUDA_TRY(
+        cudaFuncSetAttribute(pairs_cell_kernel<DBL, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  const int groups = alphas ? (nalpha + NA - 1) / NA : 1;
+  const dim3 grid(nc * nc * nc, groups);
+  pairs_cell_kernel<DBL, NA><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr,
+                                                         n, energy);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
 int launch_pairs_cells(bool dbl, const void *pos, const int *sidx, const int *start, int nc, double L, double rcut,
                        double alpha, const double *alphas, int nalpha, double *fr, int n, double *energy,
                        cudaStream_t s) {
-  static bool attr_set[2] = {false, false};
-  const size_t smem = pair_smem_bytes(dbl);
-  if (!attr_set[dbl]) {
-    if (dbl)
-      P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    else
-      P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set[dbl] = true;
-  }
-  const dim3 grid(nc * nc * nc, nalpha);
+  const bool group = alphas != nullptr && nalpha > 1;
   if (dbl)
-    pairs_cell_kernel<true><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, fr, n, energy);
-  else
-    pairs_cell_kernel<false><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, fr, n, energy);
-  P3MG_CUDA_TRY(cudaGetLastError());
-  return P3MG_OK;
+    return group ? launch_cells_na<true, PAIR_NA64>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr, n,
+                                                     energy, s)
+                 : launch_cells_na<true, 1>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr, n, energy, s);
+  return group ? launch_cells_na<false, PAIR_NA32>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr, n,
+                                                    energy, s)
+               : launch_cells_na<false, 1>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr, n, energy, s);
 }
 
 // All-pairs fallback (fewer than 3 cells per side): the reference's loop
