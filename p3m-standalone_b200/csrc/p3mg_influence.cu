@@ -195,6 +195,127 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
   if (dG) dG[ind] = dg;
 }
 
+// G_opt for a group of AB alphas per thread (alpha batches, mc <= 2):
+// everything but the Gaussian factors is independent of alpha, so the
+// per-axis sinc powers, the alias sums N1..N4 and 1/|n_m|^2 are formed once
+// per mesh point and only the per-axis Gaussians and their products are
+// evaluated per alpha.  Same zeroing and final formula as influence_point.
+template <int MC, int AB>
+__global__ void influence_group_kernel(double *__restrict__ G, int method, int m, int cao,
+                                       const double *__restrict__ alphas, int na, double L) {
+  const size_t M = (size_t)m * m * m;
+  const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ind >= M) return;
+  const int a0 = blockIdx.y * AB;
+  const int nag = min(AB, na - a0);
+  const int NZ = (int)(ind % m);
+  const int NY = (int)((ind / m) % m);
+  const int NX = (int)(ind / ((size_t)m * m));
+  const int half = m / 2;
+  const bool ad = method_ad(method);
+  const bool zero_all = ((NX | NY | NZ) == 0) || (!ad && (NX % half == 0) && (NY % half == 0) && (NZ % half == 0));
+  if (zero_all) {
+    for (int a = 0; a < nag; a++) G[(size_t)(a0 + a) * M + ind] = 0.0;
+    return;
+  }
+  const bool ik_sq = (method == 0 || method == 6);
+  const double Leni = 1.0 / L, fak1 = 1.0 / (double)m;
+  const double nx = signed_freq(NX, m), ny = signed_freq(NY, m), nz = signed_freq(NZ, m);
+  constexpr int NA = 2 * MC + 1;
+  double Nx[NA], Ny[NA], Nz[NA], Sx[NA], Sy[NA], Sz[NA];
+#pragma unroll
+  for (int i = 0; i < NA; i++) {
+    const double shift = (double)(m * (i - MC));
+    Nx[i] = nx + shift;
+    Ny[i] = ny + shift;
+    Nz[i] = nz + shift;
+    const double sx = sinc_pi(fak1 * Nx[i]), sy = sinc_pi(fak1 * Ny[i]), sz = sinc_pi(fak1 * Nz[i]);
+    Sx[i] = ik_sq ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
+    Sy[i] = ik_sq ? ipow_d(ipow_d(sy, cao), 2) : ipow_d(sy, 2 * cao);
+    Sz[i] = ik_sq ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao);
+  }
+  double fak2[AB];
+  double Ex[AB][NA], Ey[AB][NA], Ez[AB][NA];
+#pragma unroll
+  for (int a = 0; a < AB; a++) {
+    const double alpha = a < nag ? alphas[a0 + a] : 1.0;
+    const double pa = P3MG_PI / alpha;
+    fak2[a] = pa * pa;
+#pragma unroll
+    for (int i = 0; i < NA; i++) {
+      const double x = Nx[i] * Leni, y = Ny[i] * Leni, z = Nz[i] * Leni;
+      Ex[a][i] = exp(-fak2[a] * (x * x));
+      Ey[a][i] = exp(-fak2[a] * (y * y));
+      Ez[a][i] = exp(-fak2[a] * (z * z));
+    }
+  }
+  double N1 = 0.0, N2 = 0.0, N3 = 0.0, N4 = 0.0;
+  double Zx[AB], Zy[AB], Zz[AB], Z[AB];
+#pragma unroll
+  for (int a = 0; a < AB; a++) Zx[a] = Zy[a] = Zz[a] = Z[a] = 0.0;
+#pragma unroll
+  for (int i = 0; i < NA; i++)
+#pragma unroll
+    for (int j = 0; j < NA; j++) {
+      const double S2 = Sx[i] * Sy[j];
+#pragma unroll
+      for (int k = 0; k < NA; k++) {
+        const double S3 = S2 * Sz[k];
+        const double a_ = Nx[i] * Leni, b_ = Ny[j] * Leni, c_ = Nz[k] * Leni;
+        const double NM2 = a_ * a_ + b_ * b_ + c_ * c_;
+        const bool even = ((i + j + k - 3 * MC) % 2) == 0;
+        N1 += S3;
+        if (ad) {
+          N2 += S3 * NM2;
+          N3 += even ? S3 : -S3;
+          N4 += even ? S3 * NM2 : -(S3 * NM2);
+#pragma unroll
+          for (int a = 0; a < AB; a++) Z[a] += S3 * (Ex[a][i] * Ey[a][j] * Ez[a][k]);
+        } else {
+          N2 += even ? S3 : -S3;
+          const double w = S3 / NM2;
+#pragma unroll
+          for (int a = 0; a < AB; a++) {
+            const double zwi = w * (Ex[a][i] * Ey[a][j] * Ez[a][k]);
+            Zx[a] += Nx[i] * zwi * Leni;
+            Zy[a] += Ny[j] * zwi * Leni;
+            Zz[a] += Nz[k] * zwi * Leni;
+          }
+        }
+      }
+    }
+#pragma unroll
+  for (int a = 0; a < AB; a++) {
+    if (a >= nag) break;
+    const double alpha = alphas[a0 + a];
+    double g;
+    if (ad) {
+      if (alpha == 0.0) {
+        g = 0.0;
+      } else {
+        const double den = (method == 3) ? (0.5 * P3MG_PI * (N1 * N2 + N3 * N4)) : (P3MG_PI * N1 * N2);
+        g = Z[a] / den;
+      }
+    } else {
+      const double Dx = (NX == half) ? 0.0 : nx, Dy = (NY == half) ? 0.0 : ny, Dz = (NZ == half) ? 0.0 : nz;
+      double num = Dx * Zx[a] * Leni + Dy * Zy[a] * Leni + Dz * Zz[a] * Leni;
+      const double dxl = Dx * Leni, dyl = Dy * Leni, dzl = Dz * Leni;
+      const double d2 = dxl * dxl + dyl * dyl + dzl * dzl;
+      if (method == 1) {
+        num /= d2;
+        num /= 0.5 * (N1 * N1 + N2 * N2);
+      } else {
+        num /= d2 * (N1 * N1);
+      }
+      g = 2.0 * num / P3MG_PI;
+    }
+    G[(size_t)(a0 + a) * M + ind] = g;
+  }
+}
+
+// alphas per thread of influence_group_kernel (registers: 2 at mc = 2)
+constexpr int influence_ab(int mc) { return mc >= 2 ? 2 : 4; }
+
 // G (and dG) for grid (blocks, na) on the stream
 void launch_influence(double *G, int method, int m, int cao, int mc, double alpha, const double *alphas, double L,
                       double *dG, unsigned blocks, int na, int threads, cudaStream_t st) {
@@ -306,14 +427,31 @@ __global__ void self_coeff_kernel(const double *__restrict__ S26, const double *
 
 // G_opt (and for methods 2 and 7 the self-force coefficients) for na alphas
 // at once: G_all holds na meshes, b81_all 81 coefficients per alpha, S26
-// is 26 na doubles of scratch.  Same kernels and arithmetic as
-// influence_compute, so each alpha's G is the one a single call gives.
+// is 26 na doubles of scratch.  For mc <= 2 groups of alphas share the
+// alpha-independent alias sums (influence_group_kernel: each alpha's G
+// equals a single call's to rounding); otherwise the single-alpha kernel
+// over grid.y.
 int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, double *S26, double *b81_all) {
   const int m = c->mesh;
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
-  launch_influence(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas, c->L, nullptr, blocks, na, threads, c->stream);
+  if (na > 1 && c->mc <= 2) {
+    const int ab = influence_ab(c->mc);
+    const dim3 grid(blocks, (na + ab - 1) / ab);
+    if (c->mc == 0)
+      influence_group_kernel<0, influence_ab(0)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
+                                                                                 d_alphas, na, c->L);
+    else if (c->mc == 1)
+      influence_group_kernel<1, influence_ab(1)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
+                                                                                 d_alphas, na, c->L);
+    else
+      influence_group_kernel<2, influence_ab(2)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
+                                                                                 d_alphas, na, c->L);
+  } else {
+    launch_influence(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas, c->L, nullptr, blocks, na, threads,
+                     c->stream);
+  }
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   if (method_self_force(c->method)) {
