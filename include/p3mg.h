@@ -159,17 +159,31 @@ int p3mg_alpha_range(double alphamin, double alphamax, double alphastep, int cap
  * charge assignment and forward FFT run once; G, pairs, convolution,
  * backward FFTs, gather and self forces run batched over the alphas.  Each
  * alpha's forces are the ones the single calls give.
+ * With max_batch 0, at least 24 alphas and max alpha <= 2.5 min alpha, the
+ * forces are instead evaluated at 12 (FP32) / 16 (FP64) Chebyshev nodes in
+ * 1/alpha^2 and interpolated to every alpha, provided two of the requested
+ * alphas, also evaluated, agree with the interpolation to 1e-6 (FP32) /
+ * 1e-12 (FP64) of their RMS force; otherwise every alpha is evaluated.
+ * p3mg_sweep_nodes reports which happened.
  *   ref_x/y/z (host, n each, may all be NULL): reference forces; then
  *   rms_out (host, nalpha, may be NULL) receives sqrt(sum |f - ref|^2) /
  *   sqrt(n) per alpha (Calculate_errors, error.c:21-34, main.c:446).
  *   f_out (host, 3 n nalpha doubles, may be NULL): total forces, alpha k
  *   component d particle i at f_out[(k * 3 + d) * n + i].
  *   max_batch: most alphas per batched pass (0: as many as half the free
- *   device memory holds, at most 16 GiB of buffers).
+ *   device memory holds, at most 16 GiB of buffers); a positive value also
+ *   has every alpha evaluated.
  * The context's own influence function and forces are left as they were
  * (its charge mesh is overwritten). */
 int p3mg_sweep(p3mg_ctx *ctx, double rcut, int nalpha, const double *alphas, const double *ref_x,
                const double *ref_y, const double *ref_z, double *rms_out, double *f_out, int max_batch);
+
+/* Interpolation nodes the context's last p3mg_sweep used (0: every alpha
+ * was evaluated) and, in check (may be NULL), the larger relative RMS
+ * difference between interpolated and evaluated forces at its two check
+ * alphas (-1 when no interpolation was tried).  No counterpart in the
+ * reference. */
+int p3mg_sweep_nodes(p3mg_ctx *ctx, int *nodes, double *check);
 
 /* Electrostatic energy of the P3M approximation (no counterpart in the
  * reference, which computes no P3M energy): parts = {total, k space, real

@@ -684,7 +684,14 @@ extern "C" int p3mg_sweep(p3mg_ctx *h, double rcut, int nalpha, const double *al
     const size_t b = (size_t)max_batch * sweep_bytes_per_alpha(c);
     if (b < budget) budget = b;
   }
-  return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref.data() : nullptr, rms_out, f_out, budget);
+  return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref.data() : nullptr, rms_out, f_out, budget, max_batch > 0);
+}
+
+extern "C" int p3mg_sweep_nodes(p3mg_ctx *h, int *nodes, double *check) {
+  if (!h || !nodes) return P3MG_ERR_ARG;
+  *nodes = h->c.sweep_nodes;
+  if (check) *check = h->c.sweep_check;
+  return P3MG_OK;
 }
 
 extern "C" int p3mg_backward(p3mg_ctx *h, double rcut, double grad_E, double *grad_x, double *grad_y,

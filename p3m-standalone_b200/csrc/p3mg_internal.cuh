@@ -142,6 +142,8 @@ struct Ctx {
   int *scan_tmp = nullptr;
   int scan_cap = 0;           // ints per slot
   void *sweep_ws = nullptr;  // workspace of p3mg_sweep, kept between calls
+  int sweep_nodes = 0;       // last p3mg_sweep: interpolation nodes used (0: every alpha evaluated)
+  double sweep_check = -1.0; // its check: RMS(interpolated - evaluated) / RMS(evaluated), -1: none
   // energy / adjoint buffers (allocated on first use): G and dG/dalpha at
   // alpha, the potential mesh, 8 reduction slots, the gradients (3 n + n)
   double *adj_G = nullptr, *adj_dG = nullptr, *adj_sums = nullptr, *adj_grad = nullptr;
@@ -230,7 +232,7 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
 int g_to_f32_n(Ctx *c, const double *G, float *G32, size_t count);
 size_t sweep_bytes_per_alpha(const Ctx *c);
 int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
-              size_t budget);
+              size_t budget, bool exact);
 
 // misc kernels (p3mg_api.cu)
 int zero_forces(Ctx *c);

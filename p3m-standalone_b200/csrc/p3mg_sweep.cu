@@ -12,9 +12,21 @@
 // sum |f - f_ref|^2 per alpha.  The kernels are the single-step kernels
 // with an alpha index, so each alpha's forces are the ones
 // p3mg_influence + p3mg_calculate_forces give.
+//
+// Many alphas over a narrow range (>= 24 alphas, max/min <= 2.5, no batch
+// limit given): the forces are smooth functions of t = 1/alpha^2 -- G_opt
+// is a sum of exp(-c t) terms and the pair force of erfc and Gaussian terms
+// in alpha = t^{-1/2} -- so they are evaluated exactly as above at R
+// Chebyshev nodes in t (12 FP32, 16 FP64) and interpolated to every
+// requested alpha.  Two of the requested alphas are evaluated exactly as
+// well; the interpolation is used only if it reproduces their forces to
+// 1e-6 (FP32) / 1e-12 (FP64) of the RMS force, else every alpha is evaluated.
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+
+#include <algorithm>
+#include <vector>
 
 #include "p3mg_internal.cuh"
 
@@ -48,6 +60,70 @@ __global__ void combine_batch_kernel(double *__restrict__ f, const double *__res
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < count) f[t] += fk[t] + fr[t];
 }
+
+// out[y n3 + t] = sum_r W[y R + r] fn[r n3 + t] (interpolation from the nodes)
+__global__ void interp_kernel(double *__restrict__ out, const double *__restrict__ fn, const double *__restrict__ W,
+                              int R, size_t n3) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n3) return;
+  const double *w = W + (size_t)blockIdx.y * R;
+  double v = 0.0;
+  for (int r = 0; r < R; r++) v += w[r] * fn[(size_t)r * n3 + t];
+  out[(size_t)blockIdx.y * n3 + t] = v;
+}
+
+// acc[2 y] += sum_t (a - b)^2, acc[2 y + 1] += sum_t b^2 over entry y
+__global__ void diff_norm_kernel(const double *__restrict__ a, const double *__restrict__ b, size_t n3,
+                                 double *__restrict__ acc) {
+  __shared__ double red[2][8];
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double d2 = 0.0, b2 = 0.0;
+  if (t < n3) {
+    const double bv = b[(size_t)blockIdx.y * n3 + t];
+    const double d = a[(size_t)blockIdx.y * n3 + t] - bv;
+    d2 = d * d;
+    b2 = bv * bv;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+    b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = d2;
+    red[1][threadIdx.x >> 5] = b2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      s0 += red[0][w];
+      s1 += red[1][w];
+    }
+    atomicAdd(&acc[2 * blockIdx.y], s0);
+    atomicAdd(&acc[2 * blockIdx.y + 1], s1);
+  }
+}
+
+// Lagrange weights of the nodes tn[0..R) at t
+void lagrange_weights(const double *tn, int R, double t, double *w) {
+  for (int i = 0; i < R; i++) {
+    double v = 1.0;
+    for (int j = 0; j < R; j++)
+      if (j != i) v *= (t - tn[j]) / (tn[i] - tn[j]);
+    w[i] = v;
+  }
+}
+
+// Device allocation released on scope exit.
+struct SweepBuf {
+  void *p = nullptr;
+  ~SweepBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+constexpr int SWEEP_INTERP_NOT_USED = 1;  // internal: fall back to the exact sweep
 
 // Sub-buffers of the sweep, carved from one workspace that the context
 // keeps between calls (grown when a call needs more).
@@ -106,8 +182,12 @@ size_t sweep_bytes_per_alpha(const Ctx *c) {
   return b;
 }
 
-int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
-              size_t budget) {
+namespace {
+
+// Every alpha evaluated.  f_dev (device, na 3n doubles, may be NULL)
+// receives the total forces as well.
+int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
+                size_t budget, double *f_dev) {
   const size_t n3 = 3 * (size_t)c->n;
   const size_t per = sweep_bytes_per_alpha(c);
   int chunk = (int)(budget / per);
@@ -188,6 +268,10 @@ int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *r
         e = cudaMemcpyAsync(f_out + (size_t)a0 * n3, w.f, fb, cudaMemcpyDeviceToHost, c->stream);
         if (e != cudaSuccess) break;
       }
+      if (f_dev) {
+        e = cudaMemcpyAsync(f_dev + (size_t)a0 * n3, w.f, fb, cudaMemcpyDeviceToDevice, c->stream);
+        if (e != cudaSuccess) break;
+      }
     }
     if (st != P3MG_OK || e != cudaSuccess) break;
     if (rms_out && ref) {
@@ -205,6 +289,110 @@ int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *r
   }
   cudaStreamSynchronize(c->stream);
   return st;
+}
+
+// Interpolation in t = 1/alpha^2 from exact evaluations at Chebyshev nodes
+// (see the file comment); SWEEP_INTERP_NOT_USED when it does not apply or
+// does not reproduce the check alphas.
+int sweep_interpolated(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out,
+                       double *f_out, size_t budget) {
+  if (na < 24 || c->n == 0) return SWEEP_INTERP_NOT_USED;
+  double amin = alphas[0], amax = alphas[0];
+  for (int k = 1; k < na; k++) {
+    amin = alphas[k] < amin ? alphas[k] : amin;
+    amax = alphas[k] > amax ? alphas[k] : amax;
+  }
+  if (!(amin > 0.0) || amax > 2.5 * amin) return SWEEP_INTERP_NOT_USED;
+  const bool dbl = c->precision == P3MG_FP64;
+  const int R = dbl ? 16 : 12;
+  if (R + 2 > na / 2) return SWEEP_INTERP_NOT_USED;
+  const double tol = dbl ? 1e-12 : 1e-6;
+  const size_t n3 = 3 * (size_t)c->n;
+  // nodes in t, then two requested alphas (a third and two thirds up the sorted list) as checks
+  std::vector<double> ex(R + 2), tn(R);
+  const double lo = 1.0 / (amax * amax), hi = 1.0 / (amin * amin);
+  for (int r = 0; r < R; r++) {
+    tn[r] = 0.5 * (lo + hi) + 0.5 * (hi - lo) * cos((2 * r + 1) * P3MG_PI / (2.0 * R));
+    ex[r] = 1.0 / sqrt(tn[r]);
+  }
+  std::vector<double> sorted(alphas, alphas + na);
+  std::sort(sorted.begin(), sorted.end());
+  ex[R] = sorted[na / 3];
+  ex[R + 1] = sorted[(2 * na) / 3];
+  // device: node + check forces, one chunk of interpolated forces, ref,
+  // weights, squared errors and check sums
+  const int chunk = 16;
+  SweepBuf buf;
+  const size_t nf = (size_t)(R + 2) * n3, nb = (size_t)chunk * n3;
+  const size_t total = (nf + nb + (ref ? n3 : 0) + (size_t)na * R + (size_t)na + 8) * sizeof(double);
+  P3MG_CUDA_TRY(cudaMalloc(&buf.p, total));
+  double *fnode = (double *)buf.p, *fb = fnode + nf, *dref = fb + nb;
+  double *dW = dref + (ref ? n3 : 0), *rms2 = dW + (size_t)na * R, *sums = rms2 + na;
+  P3MG_TRY(sweep_exact(c, rcut, R + 2, ex.data(), nullptr, nullptr, nullptr, budget, fnode));
+  // the checks: interpolate and compare with their exact forces
+  std::vector<double> W((size_t)na * R);
+  lagrange_weights(tn.data(), R, 1.0 / (ex[R] * ex[R]), W.data());
+  lagrange_weights(tn.data(), R, 1.0 / (ex[R + 1] * ex[R + 1]), W.data() + R);
+  cudaStream_t st = c->stream;
+  P3MG_CUDA_TRY(cudaMemcpyAsync(dW, W.data(), 2 * (size_t)R * sizeof(double), cudaMemcpyHostToDevice, st));
+  P3MG_CUDA_TRY(cudaMemsetAsync(sums, 0, 4 * sizeof(double), st));
+  const unsigned gx = (unsigned)((n3 + 255) / 256);
+  interp_kernel<<<dim3(gx, 2), 256, 0, st>>>(fb, fnode, dW, R, n3);
+  diff_norm_kernel<<<dim3(gx, 2), 256, 0, st>>>(fb, fnode + (size_t)R * n3, n3, sums);
+  c->launches += 2;
+  P3MG_CUDA_TRY(cudaGetLastError());
+  double hs[4];
+  P3MG_CUDA_TRY(cudaMemcpyAsync(hs, sums, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  P3MG_CUDA_TRY(cudaStreamSynchronize(st));
+  c->sweep_check = 0.0;
+  for (int j = 0; j < 2; j++) {
+    const double rel = hs[2 * j + 1] > 0.0 ? sqrt(hs[2 * j] / hs[2 * j + 1]) : (hs[2 * j] > 0.0 ? INFINITY : 0.0);
+    c->sweep_check = rel > c->sweep_check ? rel : c->sweep_check;
+  }
+  if (!(c->sweep_check <= tol)) return SWEEP_INTERP_NOT_USED;
+  // every alpha, chunk by chunk
+  for (int k = 0; k < na; k++)
+    lagrange_weights(tn.data(), R, 1.0 / (alphas[k] * alphas[k]), W.data() + (size_t)k * R);
+  P3MG_CUDA_TRY(cudaMemcpyAsync(dW, W.data(), (size_t)na * R * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (ref) {
+    P3MG_CUDA_TRY(cudaMemcpyAsync(dref, ref, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
+    P3MG_CUDA_TRY(cudaMemsetAsync(rms2, 0, (size_t)na * sizeof(double), st));
+  }
+  for (int a0 = 0; a0 < na; a0 += chunk) {
+    const int nch = (na - a0 < chunk) ? na - a0 : chunk;
+    interp_kernel<<<dim3(gx, nch), 256, 0, st>>>(fb, fnode, dW + (size_t)a0 * R, R, n3);
+    c->launches++;
+    if (ref) {
+      sq_err_kernel<<<dim3(gx, nch), 256, 0, st>>>(fb, dref, n3, rms2 + a0);
+      c->launches++;
+    }
+    P3MG_CUDA_TRY(cudaGetLastError());
+    if (f_out)
+      P3MG_CUDA_TRY(cudaMemcpyAsync(f_out + (size_t)a0 * n3, fb, (size_t)nch * n3 * sizeof(double),
+                                    cudaMemcpyDeviceToHost, st));
+  }
+  if (rms_out && ref)
+    P3MG_CUDA_TRY(cudaMemcpyAsync(rms_out, rms2, (size_t)na * sizeof(double), cudaMemcpyDeviceToHost, st));
+  P3MG_CUDA_TRY(cudaStreamSynchronize(st));
+  if (rms_out && ref)
+    for (int k = 0; k < na; k++) rms_out[k] = sqrt(rms_out[k]) / sqrt((double)c->n);
+  return P3MG_OK;
+}
+
+}  // namespace
+
+int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
+              size_t budget, bool exact) {
+  c->sweep_nodes = 0;
+  c->sweep_check = -1.0;
+  if (!exact) {
+    const int st = sweep_interpolated(c, rcut, na, alphas, ref, rms_out, f_out, budget);
+    if (st != SWEEP_INTERP_NOT_USED) {
+      if (st == P3MG_OK) c->sweep_nodes = (c->precision == P3MG_FP64) ? 16 : 12;
+      return st;
+    }
+  }
+  return sweep_exact(c, rcut, na, alphas, ref, rms_out, f_out, budget, nullptr);
 }
 
 }  // namespace p3mg

@@ -99,6 +99,7 @@ def load():
                                            ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp]
     L.p3mg_alpha_range.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, _dp]
     L.p3mg_sweep.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
+    L.p3mg_sweep_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_int), _dp]
     L.p3mg_energy.argtypes = [vp, ctypes.c_double, _dp]
     L.p3mg_backward.argtypes = [vp, ctypes.c_double, ctypes.c_double] + [_dp] * 7
     L.p3mg_set_tiles.argtypes = [vp, ctypes.c_int, ctypes.c_int]
@@ -296,7 +297,10 @@ class Context:
             rx = ry = rz = None
         _check(self._lib.p3mg_sweep(self._h, float(rcut), na, _p(al), _p(rx), _p(ry), _p(rz), _p(rms), _p(f),
                                     int(max_batch)), "p3mg_sweep")
-        return dict(rms=rms, forces=f)
+        nodes = ctypes.c_int(0)
+        check = np.zeros(1)
+        _check(self._lib.p3mg_sweep_nodes(self._h, ctypes.byref(nodes), _p(check)), "p3mg_sweep_nodes")
+        return dict(rms=rms, forces=f, nodes=nodes.value, check=float(check[0]))
 
     def energy(self, rcut):
         """P3M energy parts (p3mg_energy): dict total, kspace, realspace, self, neutral."""

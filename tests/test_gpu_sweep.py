@@ -91,3 +91,41 @@ def test_graph_replay_follows_box_changes(gpu):
             got = ctx.calculate_forces(3.0)["f"]
             want = ref.calculate_forces(3.0)["f"]
             assert O.rel_rms(got.ravel(), want.ravel()) <= 1e-14, L
+
+
+@pytest.mark.parametrize("method", [1, 7])
+@pytest.mark.parametrize("precision,lo,hi,na,nodes,tol", [
+    (p3mg.FP32_MIXED, 0.7, 1.4, 32, 12, 2e-6),   # interpolated: FP32 noise level
+    (p3mg.FP64, 0.8, 1.2, 48, 16, 1e-12),        # interpolated: checked to 1e-12
+    (p3mg.FP64, 0.7, 1.4, 48, 0, 1e-13),         # check ~1e-9 > 1e-12: every alpha evaluated
+])
+def test_interpolated_sweep_matches_single_alpha_steps(gpu, method, precision, lo, hi, na, nodes, tol):
+    # many alphas over a narrow range: forces interpolated in 1/alpha^2 from
+    # exact evaluations at Chebyshev nodes when two check alphas confirm it;
+    # every alpha's forces must still match its own single-alpha step
+    x, y, z, q = p3mg.generate_system(0, 3000, 14.4, seed=54)
+    alphas = np.linspace(lo, hi, na)
+    ref = np.zeros((3, len(x)))
+    with p3mg.Context(method, 32, 7, 1, precision) as ctx:
+        ctx.set_system(x, y, z, q, 14.4)
+        r = ctx.sweep(3.0, alphas, ref=ref, want_forces=True)
+        assert r["nodes"] == nodes, r["check"]
+        assert r["check"] >= 0.0  # the interpolation was tried
+        if nodes == 0:
+            assert r["check"] > 1e-12
+        ex = ctx.sweep(3.0, alphas[:5], want_forces=True, max_batch=32)
+        assert ex["nodes"] == 0 and ex["check"] == -1.0  # a batch limit: every alpha evaluated
+        for k in range(0, len(alphas), 5):
+            ctx.influence(alphas[k])
+            single = ctx.calculate_forces(3.0)["f"]
+            assert O.rel_rms(r["forces"][k].ravel(), single.ravel()) <= tol, k
+            # rms against the (zero) reference is the RMS force itself
+            assert abs(r["rms"][k] - np.sqrt(np.sum(r["forces"][k] ** 2) / len(x))) <= 1e-12 * r["rms"][k]
+
+
+def test_wide_alpha_range_is_evaluated_alpha_by_alpha(gpu):
+    x, y, z, q = p3mg.generate_system(0, 1000, 10.0, seed=55)
+    with p3mg.Context(7, 16, 7, 2) as ctx:
+        ctx.set_system(x, y, z, q, 10.0)
+        r = ctx.sweep(3.0, p3mg.alpha_range(0.1, 2.5, 0.05))
+        assert r["nodes"] == 0
