@@ -412,28 +412,38 @@ def secondary_workloads(dev):
         return torch.cuda.ExternalStream(ctx.stream(), device=dev)
 
     # alpha sweep: the reference's example (method 7, 1000 particles, box 10,
-    # mesh 16, cao 7, mc 2, rcut 3, alpha 0.1..2.5 step 0.05: 49 alphas), FP64
+    # mesh 16, cao 7, mc 2, rcut 3, alpha 0.1..2.5 step 0.05: 49 alphas), FP64;
+    # each sweep returns the RMS force error per alpha against the Ewald forces
     x, y, z, q = p3mg.generate_system(0, 1000, 10.0, seed=12345)
     with p3mg.Context(7, 16, 7, 2, p3mg.FP64) as ctx:
         ctx.set_system(x, y, z, q, 10.0)
         st = stream_of(ctx)
+        ref = ctx.ewald_forces()["f"]
         al = p3mg.alpha_range(0.1, 2.5, 0.05)
         ctx.influence(1.0)
         ctx.set_graph(True)
         step = _timed(st, lambda: ctx.compute(3.0), reps=7)
         loop = _timed(st, lambda: [(ctx.influence(a), ctx.compute(3.0)) for a in al])
-        sweep = _timed(st, lambda: ctx.sweep(3.0, al))
+        sweep = _timed(st, lambda: ctx.sweep(3.0, al, ref=ref))
         a64 = np.linspace(0.1, 2.5, 64)
-        sweep64 = _timed(st, lambda: ctx.sweep(3.0, a64))
+        sweep64 = _timed(st, lambda: ctx.sweep(3.0, a64, ref=ref))
     out["alpha_sweep_1000"] = {
-        "workload": "method 7, 1000 particles, box 10, mesh 16, cao 7, mc 2, rcut 3, FP64",
+        "workload": "method 7, 1000 particles, box 10, mesh 16, cao 7, mc 2, rcut 3, FP64, "
+                    "RMS error per alpha against the Ewald forces",
         "step_ms": round(step, 4), "alphas": len(al), "sweep_ms": round(sweep, 3),
         "per_alpha_loop_ms": round(loop, 3), "sweep_64_alphas_ms": round(sweep64, 3),
         "sweep_64_over_step": round(sweep64 / step, 2)}
 
-    # the same 64-alpha sweep at the headline size (method 1, 1M, mesh 128), FP32
+    # the same 64-alpha sweep at the headline size (method 1, 1M, mesh 128),
+    # FP32, RMS error per alpha against the FP64 P3M forces at the headline
+    # alpha (host rows, uploaded inside the timed call)
     W = WORKLOAD
     x, y, z, q = p3mg.generate_system(0, W["n"], W["box"], seed=W["seed"])
+    with p3mg.Context(W["method"], W["mesh"], W["cao"], W["mc"], p3mg.FP64) as ctx:
+        ctx.set_system(x, y, z, q, W["box"])
+        ctx.influence(W["alpha"])
+        ctx.compute(W["rcut"])
+        ref = ctx.get_forces()["f"]
     with p3mg.Context(W["method"], W["mesh"], W["cao"], W["mc"], p3mg.FP32_MIXED) as ctx:
         ctx.set_system(x, y, z, q, W["box"])
         st = stream_of(ctx)
@@ -441,8 +451,9 @@ def secondary_workloads(dev):
         ctx.set_graph(True)
         step = _timed(st, lambda: ctx.compute(W["rcut"]), reps=5)
         a64 = np.linspace(0.6, 1.2, 64)
-        sweep64 = _timed(st, lambda: ctx.sweep(W["rcut"], a64), reps=1)
-    out["alpha_sweep_1m"] = {"workload": W["workload"] + ", FP32, 64 alphas 0.6..1.2",
+        sweep64 = _timed(st, lambda: ctx.sweep(W["rcut"], a64, ref=ref), reps=3)
+    out["alpha_sweep_1m"] = {"workload": W["workload"] + ", FP32, 64 alphas 0.6..1.2, RMS error per alpha "
+                                                        "against FP64 P3M forces",
                              "step_ms": round(step, 4), "sweep_64_alphas_ms": round(sweep64, 2),
                              "sweep_64_over_step": round(sweep64 / step, 2)}
 

@@ -160,14 +160,15 @@ int p3mg_alpha_range(double alphamin, double alphamax, double alphastep, int cap
  * backward FFTs, gather and self forces run batched over the alphas.  Each
  * alpha's forces are the ones the single calls give.
  * With max_batch 0, at least 24 alphas and max alpha <= 2.5 min alpha, the
- * forces are instead evaluated at 12 (FP32) / 16 (FP64) Chebyshev nodes in
+ * forces are instead evaluated at 10 (FP32) / 16 (FP64) Chebyshev nodes in
  * 1/alpha^2 and interpolated to every alpha, provided two of the requested
  * alphas, also evaluated, agree with the interpolation to 1e-6 (FP32) /
  * 1e-12 (FP64) of their RMS force; otherwise every alpha is evaluated.
  * p3mg_sweep_nodes reports which happened.
  *   ref_x/y/z (host, n each, may all be NULL): reference forces; then
  *   rms_out (host, nalpha, may be NULL) receives sqrt(sum |f - ref|^2) /
- *   sqrt(n) per alpha (Calculate_errors, error.c:21-34, main.c:446).
+ *   sqrt(n) per alpha (Calculate_errors, error.c:21-34, main.c:446).  The
+ *   rows are read while the sweep runs, not copied first.
  *   f_out (host, 3 n nalpha doubles, may be NULL): total forces, alpha k
  *   component d particle i at f_out[(k * 3 + d) * n + i].
  *   max_batch: most alphas per batched pass (0: as many as half the free

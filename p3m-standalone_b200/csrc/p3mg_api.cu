@@ -126,6 +126,9 @@ int free_all(Ctx *c) {
   if (c->sweep_ws) cudaFree(c->sweep_ws);
   c->sweep_ws = nullptr;
   c->sweep_cap = 0;
+  if (c->interp_ws) cudaFree(c->interp_ws);
+  c->interp_ws = nullptr;
+  c->interp_cap = 0;
   dfree(c->adj_G);
   dfree(c->adj_dG);
   dfree(c->adj_sums);
@@ -667,14 +670,7 @@ extern "C" int p3mg_sweep(p3mg_ctx *h, double rcut, int nalpha, const double *al
     if (!isfinite(alphas[k]) || alphas[k] < 0.0) return P3MG_ERR_ARG;
   if (nalpha == 0) return P3MG_OK;
   cudaSetDevice(c->device);
-  const size_t n = (size_t)c->n;
-  std::vector<double> ref;
-  if (want_ref) {
-    ref.resize(3 * n + 1);
-    memcpy(ref.data(), ref_x, n * sizeof(double));
-    memcpy(ref.data() + n, ref_y, n * sizeof(double));
-    memcpy(ref.data() + 2 * n, ref_z, n * sizeof(double));
-  }
+  const double *const ref[3] = {ref_x, ref_y, ref_z};
   size_t free_b = 0, total_b = 0;
   P3MG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
   size_t budget = free_b / 2;
@@ -684,7 +680,7 @@ extern "C" int p3mg_sweep(p3mg_ctx *h, double rcut, int nalpha, const double *al
     const size_t b = (size_t)max_batch * sweep_bytes_per_alpha(c);
     if (b < budget) budget = b;
   }
-  return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref.data() : nullptr, rms_out, f_out, budget, max_batch > 0);
+  return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref : nullptr, rms_out, f_out, budget, max_batch > 0);
 }
 
 extern "C" int p3mg_sweep_nodes(p3mg_ctx *h, int *nodes, double *check) {

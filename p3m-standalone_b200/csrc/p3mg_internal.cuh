@@ -143,6 +143,8 @@ struct Ctx {
   int scan_cap = 0;           // ints per slot
   void *sweep_ws = nullptr;  // workspace of p3mg_sweep, kept between calls
   int sweep_nodes = 0;       // last p3mg_sweep: interpolation nodes used (0: every alpha evaluated)
+  void *interp_ws = nullptr;  // buffers of the interpolated sweep, kept between calls
+  size_t interp_cap = 0;
   double sweep_check = -1.0; // its check: RMS(interpolated - evaluated) / RMS(evaluated), -1: none
   // energy / adjoint buffers (allocated on first use): G and dG/dalpha at
   // alpha, the potential mesh, 8 reduction slots, the gradients (3 n + n)
@@ -231,8 +233,9 @@ int kspace_batch(Ctx *c, const KspaceBatch &b);
 int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, double *S26, double *b81_all);
 int g_to_f32_n(Ctx *c, const double *G, float *G32, size_t count);
 size_t sweep_bytes_per_alpha(const Ctx *c);
-int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
-              size_t budget, bool exact);
+// ref: host reference rows x, y, z (n doubles each), or NULL
+int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *const *ref, double *rms_out,
+              double *f_out, size_t budget, bool exact);
 
 // misc kernels (p3mg_api.cu)
 int zero_forces(Ctx *c);

@@ -17,10 +17,17 @@
 // limit given): the forces are smooth functions of t = 1/alpha^2 -- G_opt
 // is a sum of exp(-c t) terms and the pair force of erfc and Gaussian terms
 // in alpha = t^{-1/2} -- so they are evaluated exactly as above at R
-// Chebyshev nodes in t (12 FP32, 16 FP64) and interpolated to every
+// Chebyshev nodes in t (10 FP32, 16 FP64) and interpolated to every
 // requested alpha.  Two of the requested alphas are evaluated exactly as
 // well; the interpolation is used only if it reproduces their forces to
 // 1e-6 (FP32) / 1e-12 (FP64) of the RMS force, else every alpha is evaluated.
+// Without a force output the interpolation goes straight into the squared
+// errors (one kernel reading the node forces once), so an RMS-only sweep
+// writes no per-alpha forces.
+//
+// Reference forces arrive as three host rows; they are uploaded on the
+// context's second stream once work is queued on the first, so that a
+// pageable copy overlaps the evaluation instead of preceding it.
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -105,6 +112,83 @@ __global__ void diff_norm_kernel(const double *__restrict__ a, const double *__r
   }
 }
 
+// Interpolation straight into squared errors:
+// rms2[a] += sum_t (sum_r W[a R + r] fn[r n3 + t] - ref[t])^2 for IE_AB
+// alphas per block.  grid.x = alpha blocks (fastest, so the blocks of one t
+// tile run together and share its node reads through L2), grid.y = t tiles
+// of blockDim.x * IE_ITEMS entries.  RN >= R is the register count for the
+// node values.
+constexpr int IE_AB = 16;
+constexpr int IE_ITEMS = 8;
+constexpr int IE_THREADS = 256;
+
+template <int RN>
+__global__ void __launch_bounds__(IE_THREADS) interp_err_kernel(const double *__restrict__ fn,
+                                                                const double *__restrict__ W, int R, int na,
+                                                                const double *__restrict__ ref, size_t n3,
+                                                                double *__restrict__ rms2) {
+  __shared__ double ws[IE_AB][RN];
+  __shared__ double red[IE_THREADS / 32][IE_AB];
+  const int a0 = blockIdx.x * IE_AB;
+  for (int i = threadIdx.x; i < IE_AB * RN; i += blockDim.x) {
+    const int a = i / RN, r = i % RN;
+    ws[a][r] = (a0 + a < na && r < R) ? W[(size_t)(a0 + a) * R + r] : 0.0;
+  }
+  __syncthreads();
+  double acc[IE_AB];
+#pragma unroll
+  for (int a = 0; a < IE_AB; a++) acc[a] = 0.0;
+  const size_t base = (size_t)blockIdx.y * blockDim.x * IE_ITEMS + threadIdx.x;
+#pragma unroll 1
+  for (int it = 0; it < IE_ITEMS; it++) {
+    const size_t t = base + (size_t)it * blockDim.x;
+    if (t >= n3) break;
+    // keeps the weight loads inside the loop (hoisted, they would take
+    // IE_AB * RN registers)
+    asm volatile("" ::: "memory");
+    double f[RN];
+#pragma unroll
+    for (int r = 0; r < RN; r++) f[r] = (r < R) ? fn[(size_t)r * n3 + t] : 0.0;
+    const double rv = ref[t];
+#pragma unroll
+    for (int a = 0; a < IE_AB; a++) {
+      double v = 0.0;
+#pragma unroll
+      for (int r = 0; r < RN; r++) v = fma(ws[a][r], f[r], v);
+      const double d = v - rv;
+      acc[a] = fma(d, d, acc[a]);
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < IE_AB; a++) {
+    double v = acc[a];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][a] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < IE_AB && a0 + (int)threadIdx.x < na) {
+    double s = 0.0;
+    for (int w = 0; w < IE_THREADS / 32; w++) s += red[w][threadIdx.x];
+    if (s != 0.0) atomicAdd(&rms2[a0 + threadIdx.x], s);
+  }
+}
+
+// Host reference rows (x, y, z; n doubles each) to dst (3n doubles) on the
+// second stream; the context stream waits for them before its next launch.
+cudaError_t upload_ref(Ctx *c, const double *const *ref, double *dst) {
+  const size_t n = (size_t)c->n;
+  cudaStream_t s = c->stream2 ? c->stream2 : c->stream;
+  for (int d = 0; d < 3; d++) {
+    const cudaError_t e = cudaMemcpyAsync(dst + d * n, ref[d], n * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+  }
+  if (s == c->stream) return cudaSuccess;
+  const cudaError_t e = cudaEventRecord(c->ev_join, s);
+  return e != cudaSuccess ? e : cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+}
+
 // Lagrange weights of the nodes tn[0..R) at t
 void lagrange_weights(const double *tn, int R, double t, double *w) {
   for (int i = 0; i < R; i++) {
@@ -115,20 +199,12 @@ void lagrange_weights(const double *tn, int R, double t, double *w) {
   }
 }
 
-// Device allocation released on scope exit.
-struct SweepBuf {
-  void *p = nullptr;
-  ~SweepBuf() {
-    if (p) cudaFree(p);
-  }
-};
-
 constexpr int SWEEP_INTERP_NOT_USED = 1;  // internal: fall back to the exact sweep
 
-// interpolation nodes: 12 (FP32: the checks measure ~2e-7, the FP32
-// rounding of the forces; 8 nodes measured up to 1.8e-6 over max/min = 2),
-// 16 (FP64)
-constexpr int sweep_interp_nodes(bool dbl) { return dbl ? 16 : 12; }
+// interpolation nodes: 10 (FP32: the checks measure ~2e-7, the FP32
+// rounding of the forces, up to max/min = 2; 8 nodes measured up to 1.8e-6
+// there), 16 (FP64)
+constexpr int sweep_interp_nodes(bool dbl) { return dbl ? 16 : 10; }
 
 // Sub-buffers of the sweep, carved from one workspace that the context
 // keeps between calls (grown when a call needs more).
@@ -189,10 +265,13 @@ size_t sweep_bytes_per_alpha(const Ctx *c) {
 
 namespace {
 
-// Every alpha evaluated.  f_dev (device, na 3n doubles, may be NULL)
-// receives the total forces as well.
-int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
-                size_t budget, double *f_dev) {
+// Every alpha evaluated.  ref: host reference rows x, y, z (or NULL).
+// f_dev (device, na 3n doubles, may be NULL) receives the total forces as
+// well.  late_ref (host rows, may be NULL) is uploaded to late_dst once the
+// evaluation is queued, for the caller's use after it.
+int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double *const *ref, double *rms_out,
+                double *f_out, size_t budget, double *f_dev, const double *const *late_ref = nullptr,
+                double *late_dst = nullptr) {
   const size_t n3 = 3 * (size_t)c->n;
   const size_t per = sweep_bytes_per_alpha(c);
   int chunk = (int)(budget / per);
@@ -217,7 +296,6 @@ int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double 
   sweep_layout(c, na, chunk, ref != nullptr, reinterpret_cast<unsigned char *>(c->sweep_ws), &w);
   do {
     e = cudaMemcpyAsync(w.alphas, alphas, (size_t)na * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess && ref) e = cudaMemcpyAsync(w.ref, ref, n3 * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.rms2, 0, (size_t)na * sizeof(double), c->stream);
     if (e != cudaSuccess) break;
     if (rcut != 0.0) {
@@ -262,6 +340,8 @@ int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double 
         const size_t cnt = (size_t)nch * n3;
         combine_batch_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, c->stream>>>(w.f, w.fk, w.fr, cnt);
         c->launches++;
+        if (ref && a0 == 0) e = upload_ref(c, ref, w.ref);
+        if (e != cudaSuccess) break;
         if (ref) {
           sq_err_kernel<<<dim3((unsigned)((n3 + 255) / 256), nch), 256, 0, c->stream>>>(w.f, w.ref, n3, w.rms2 + a0);
           c->launches++;
@@ -279,6 +359,10 @@ int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double 
       }
     }
     if (st != P3MG_OK || e != cudaSuccess) break;
+    if (late_ref) {
+      e = upload_ref(c, late_ref, late_dst);
+      if (e != cudaSuccess) break;
+    }
     if (rms_out && ref) {
       e = cudaMemcpyAsync(rms_out, w.rms2, (size_t)na * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
       if (e != cudaSuccess) break;
@@ -299,8 +383,8 @@ int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double 
 // Interpolation in t = 1/alpha^2 from exact evaluations at Chebyshev nodes
 // (see the file comment); SWEEP_INTERP_NOT_USED when it does not apply or
 // does not reproduce the check alphas.
-int sweep_interpolated(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out,
-                       double *f_out, size_t budget) {
+int sweep_interpolated(Ctx *c, double rcut, int na, const double *alphas, const double *const *ref,
+                       double *rms_out, double *f_out, size_t budget) {
   if (na < 24 || c->n == 0) return SWEEP_INTERP_NOT_USED;
   double amin = alphas[0], amax = alphas[0];
   for (int k = 1; k < na; k++) {
@@ -324,16 +408,22 @@ int sweep_interpolated(Ctx *c, double rcut, int na, const double *alphas, const 
   std::sort(sorted.begin(), sorted.end());
   ex[R] = sorted[na / 3];
   ex[R + 1] = sorted[(2 * na) / 3];
-  // device: node + check forces, one chunk of interpolated forces, ref,
-  // weights, squared errors and check sums
-  const int chunk = 16;
-  SweepBuf buf;
+  // device: node + check forces, interpolated forces (one chunk of alphas
+  // with a force output, else the two checks), ref, weights, squared
+  // errors and check sums
+  const int chunk = f_out ? 16 : 2;
   const size_t nf = (size_t)(R + 2) * n3, nb = (size_t)chunk * n3;
   const size_t total = (nf + nb + (ref ? n3 : 0) + (size_t)na * R + (size_t)na + 8) * sizeof(double);
-  P3MG_CUDA_TRY(cudaMalloc(&buf.p, total));
-  double *fnode = (double *)buf.p, *fb = fnode + nf, *dref = fb + nb;
+  if (total > c->interp_cap) {
+    if (c->interp_ws) cudaFree(c->interp_ws);
+    c->interp_ws = nullptr;
+    c->interp_cap = 0;
+    P3MG_CUDA_TRY(cudaMalloc(&c->interp_ws, total));
+    c->interp_cap = total;
+  }
+  double *fnode = (double *)c->interp_ws, *fb = fnode + nf, *dref = fb + nb;
   double *dW = dref + (ref ? n3 : 0), *rms2 = dW + (size_t)na * R, *sums = rms2 + na;
-  P3MG_TRY(sweep_exact(c, rcut, R + 2, ex.data(), nullptr, nullptr, nullptr, budget, fnode));
+  P3MG_TRY(sweep_exact(c, rcut, R + 2, ex.data(), nullptr, nullptr, nullptr, budget, fnode, ref, dref));
   // the checks: interpolate and compare with their exact forces
   std::vector<double> W((size_t)na * R);
   lagrange_weights(tn.data(), R, 1.0 / (ex[R] * ex[R]), W.data());
@@ -355,26 +445,34 @@ int sweep_interpolated(Ctx *c, double rcut, int na, const double *alphas, const 
     c->sweep_check = rel > c->sweep_check ? rel : c->sweep_check;
   }
   if (!(c->sweep_check <= tol)) return SWEEP_INTERP_NOT_USED;
-  // every alpha, chunk by chunk
+  // every alpha: with a force output chunk by chunk, else straight into the
+  // squared errors
   for (int k = 0; k < na; k++)
     lagrange_weights(tn.data(), R, 1.0 / (alphas[k] * alphas[k]), W.data() + (size_t)k * R);
   P3MG_CUDA_TRY(cudaMemcpyAsync(dW, W.data(), (size_t)na * R * sizeof(double), cudaMemcpyHostToDevice, st));
-  if (ref) {
-    P3MG_CUDA_TRY(cudaMemcpyAsync(dref, ref, n3 * sizeof(double), cudaMemcpyHostToDevice, st));
-    P3MG_CUDA_TRY(cudaMemsetAsync(rms2, 0, (size_t)na * sizeof(double), st));
-  }
-  for (int a0 = 0; a0 < na; a0 += chunk) {
-    const int nch = (na - a0 < chunk) ? na - a0 : chunk;
-    interp_kernel<<<dim3(gx, nch), 256, 0, st>>>(fb, fnode, dW + (size_t)a0 * R, R, n3);
-    c->launches++;
-    if (ref) {
-      sq_err_kernel<<<dim3(gx, nch), 256, 0, st>>>(fb, dref, n3, rms2 + a0);
+  if (ref) P3MG_CUDA_TRY(cudaMemsetAsync(rms2, 0, (size_t)na * sizeof(double), st));
+  if (f_out) {
+    for (int a0 = 0; a0 < na; a0 += chunk) {
+      const int nch = (na - a0 < chunk) ? na - a0 : chunk;
+      interp_kernel<<<dim3(gx, nch), 256, 0, st>>>(fb, fnode, dW + (size_t)a0 * R, R, n3);
       c->launches++;
-    }
-    P3MG_CUDA_TRY(cudaGetLastError());
-    if (f_out)
+      if (ref) {
+        sq_err_kernel<<<dim3(gx, nch), 256, 0, st>>>(fb, dref, n3, rms2 + a0);
+        c->launches++;
+      }
+      P3MG_CUDA_TRY(cudaGetLastError());
       P3MG_CUDA_TRY(cudaMemcpyAsync(f_out + (size_t)a0 * n3, fb, (size_t)nch * n3 * sizeof(double),
                                     cudaMemcpyDeviceToHost, st));
+    }
+  } else if (ref) {
+    const dim3 grid((unsigned)((na + IE_AB - 1) / IE_AB),
+                    (unsigned)((n3 + (size_t)IE_THREADS * IE_ITEMS - 1) / ((size_t)IE_THREADS * IE_ITEMS)));
+    if (R <= 10)
+      interp_err_kernel<10><<<grid, IE_THREADS, 0, st>>>(fnode, dW, R, na, dref, n3, rms2);
+    else
+      interp_err_kernel<16><<<grid, IE_THREADS, 0, st>>>(fnode, dW, R, na, dref, n3, rms2);
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
   }
   if (rms_out && ref)
     P3MG_CUDA_TRY(cudaMemcpyAsync(rms_out, rms2, (size_t)na * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -386,8 +484,8 @@ int sweep_interpolated(Ctx *c, double rcut, int na, const double *alphas, const 
 
 }  // namespace
 
-int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *ref, double *rms_out, double *f_out,
-              size_t budget, bool exact) {
+int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *const *ref, double *rms_out,
+              double *f_out, size_t budget, bool exact) {
   c->sweep_nodes = 0;
   c->sweep_check = -1.0;
   if (!exact) {

@@ -95,7 +95,7 @@ def test_graph_replay_follows_box_changes(gpu):
 
 @pytest.mark.parametrize("method", [1, 7])
 @pytest.mark.parametrize("precision,lo,hi,na,nodes,tol", [
-    (p3mg.FP32_MIXED, 0.7, 1.4, 32, 12, 2e-6),   # interpolated: FP32 noise level
+    (p3mg.FP32_MIXED, 0.7, 1.4, 32, 10, 2e-6),   # interpolated: FP32 noise level
     (p3mg.FP64, 0.8, 1.2, 48, 16, 1e-12),        # interpolated: checked to 1e-12
     (p3mg.FP64, 0.7, 1.4, 48, 0, 1e-13),         # check ~1e-9 > 1e-12: every alpha evaluated
 ])
@@ -121,6 +121,31 @@ def test_interpolated_sweep_matches_single_alpha_steps(gpu, method, precision, l
             assert O.rel_rms(r["forces"][k].ravel(), single.ravel()) <= tol, k
             # rms against the (zero) reference is the RMS force itself
             assert abs(r["rms"][k] - np.sqrt(np.sum(r["forces"][k] ** 2) / len(x))) <= 1e-12 * r["rms"][k]
+
+
+@pytest.mark.parametrize("precision,nodes,rtol", [
+    (p3mg.FP32_MIXED, 10, 2e-6),   # two sweeps: FP32 sums in atomic binning order differ at ~1e-7
+    (p3mg.FP64, 16, 1e-9),
+])
+def test_rms_only_interpolated_sweep_matches_forces_sweep(gpu, precision, nodes, rtol):
+    # without a force output the interpolation goes straight into the squared
+    # errors (one kernel); the RMS must equal the one of the interpolated
+    # forces against the same (host) reference rows
+    x, y, z, q = p3mg.generate_system(0, 3000, 14.4, seed=56)
+    alphas = np.linspace(0.8, 1.2, 40)
+    with p3mg.Context(1, 32, 7, 1, precision) as ctx:
+        ctx.set_system(x, y, z, q, 14.4)
+        ctx.influence(1.0)
+        f1 = ctx.calculate_forces(3.0)["f"]
+        rng = np.random.default_rng(7)
+        ref = f1 + 0.01 * np.sqrt(np.mean(f1 ** 2)) * rng.standard_normal(f1.shape)
+        a = ctx.sweep(3.0, alphas, ref=ref)
+        b = ctx.sweep(3.0, alphas, ref=ref, want_forces=True)
+        assert a["nodes"] == b["nodes"] == nodes, (a["check"], b["check"])
+        assert a["forces"] is None
+        direct = np.sqrt(np.sum((b["forces"] - ref[None]) ** 2, axis=(1, 2)) / len(x))
+        np.testing.assert_allclose(a["rms"], direct, rtol=rtol)
+        np.testing.assert_allclose(b["rms"], direct, rtol=1e-9)
 
 
 def test_wide_alpha_range_is_evaluated_alpha_by_alpha(gpu):
