@@ -213,13 +213,16 @@ int p3mg_backward(p3mg_ctx *ctx, double rcut, double grad_E, double *grad_x, dou
 
 /* Tile shapes (no counterpart in the reference): brick edge of the
  * charge-assignment tiles (4 or 8 mesh points; the default is 8 for meshes
- * of 64 and more, else 4) and pencils per FFT tile (4, 8 or 16; 0 for the
- * default, 16 in FP32 and 8 in FP64).  Results differ only by the order of
- * floating-point additions. */
+ * of 64 and more, else 4) and the FFT kernel: 0 (the default) for the
+ * register-tiled pencil kernels on FP32 meshes of 32, 64 and 128 points
+ * (with the ik convolution folded into the first backward pass) and the
+ * shared-memory Stockham kernel with 16 (FP32) / 8 (FP64) pencils per tile
+ * otherwise; 4, 8 or 16 for the Stockham kernel with that many pencils.
+ * Results differ only by the rounding of the floating-point operations. */
 int p3mg_set_tiles(p3mg_ctx *ctx, int brick, int fft_w);
 
 /* Tile autotuner (no counterpart in the reference): times the context's
- * force evaluation with rcut for every brick edge and FFT tile width, keeps
+ * force evaluation with rcut for every brick edge and FFT kernel, keeps
  * the fastest and returns it with its mean time in ms (outputs may be
  * NULL).  Needs p3mg_influence first. */
 int p3mg_autotune(p3mg_ctx *ctx, double rcut, int *brick, int *fft_w, double *ms);

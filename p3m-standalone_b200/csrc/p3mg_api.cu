@@ -729,7 +729,9 @@ extern "C" int p3mg_energy(p3mg_ctx *h, double rcut, double parts[5]) {
   return p3mg_backward(h, rcut, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, parts);
 }
 
-// Brick edge of the charge-assignment tiles and pencils per FFT tile.
+// Brick edge of the charge-assignment tiles and the FFT kernel (0: pencil
+// kernels where they apply, else Stockham with the default width; 4, 8, 16:
+// Stockham with that many pencils per tile).
 static int set_tiles(Ctx *c, int brick, int fft_w) {
   if (brick != 4 && brick != 8) return P3MG_ERR_ARG;
   if (fft_w != 0 && fft_w != 4 && fft_w != 8 && fft_w != 16) return P3MG_ERR_ARG;
@@ -790,12 +792,14 @@ extern "C" int p3mg_autotune(p3mg_ctx *h, double rcut, int *brick_out, int *fft_
   const bool timing = c->timing;
   c->timing = false;
   P3MG_TRY(pairs_reserve(c, rcut));
-  const int bricks[2] = {4, 8}, ws[3] = {4, 8, 16};
+  // FFT: 0 = automatic (the pencil kernels where they apply), then the
+  // Stockham tile widths
+  const int bricks[2] = {4, 8}, ws[4] = {0, 4, 8, 16};
   int bb = c->brick, bw = c->fft_w;
   double best = 1e300;
   int st = P3MG_OK;
   for (int ib = 0; ib < 2 && st == P3MG_OK; ib++)
-    for (int iw = 0; iw < 3 && st == P3MG_OK; iw++) {
+    for (int iw = 0; iw < 4 && st == P3MG_OK; iw++) {
       if (bricks[ib] > c->mesh) continue;
       st = set_tiles(c, bricks[ib], ws[iw]);
       double ms = 0.0;

@@ -537,24 +537,31 @@ int run_kspace(Ctx *c) {
     P3MG_TRY(fft3d(c, c->Q, 1, +1));
   } else {
     const double s = 2.0 * P3MG_PI / c->L;
-    if (c->precision == P3MG_FP64)
-      conv_ik_kernel<real, double><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), c->G,
-                                                                       c->mesh, s, M, reinterpret_cast<C *>(c->F));
-    else
-      conv_ik_kernel<real, float><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), c->G32,
-                                                                      c->mesh, s, M, reinterpret_cast<C *>(c->F));
-    c->launches++;
-    P3MG_CUDA_TRY(cudaGetLastError());
-    P3MG_TRY(fft3d(c, c->F, 3, +1));
-    typedef typename cplx<real>::vec4 V;
-    if (method_interlaced(c->method))
-      pack_ik_kernel<real, 2><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->F), M,
-                                                                  reinterpret_cast<V *>(c->P));
-    else
-      pack_ik_kernel<real, 1><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->F), M,
-                                                                  reinterpret_cast<V *>(c->P));
-    c->launches++;
-    P3MG_CUDA_TRY(cudaGetLastError());
+    // FP32 pencil FFTs: the convolution folded into the first backward
+    // pass, the packing into the last
+    const bool fused = c->precision != P3MG_FP64 && c->fft_w == 0 && fft_pencil_ok(c);
+    if (fused) {
+      P3MG_TRY(ik_conv_inverse_pencil(c, c->Q, c->G32, s, c->F, 1, c->P));
+    } else {
+      if (c->precision == P3MG_FP64)
+        conv_ik_kernel<real, double><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), c->G,
+                                                                         c->mesh, s, M, reinterpret_cast<C *>(c->F));
+      else
+        conv_ik_kernel<real, float><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), c->G32,
+                                                                        c->mesh, s, M, reinterpret_cast<C *>(c->F));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+      P3MG_TRY(fft3d(c, c->F, 3, +1));
+      typedef typename cplx<real>::vec4 V;
+      if (method_interlaced(c->method))
+        pack_ik_kernel<real, 2><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->F), M,
+                                                                    reinterpret_cast<V *>(c->P));
+      else
+        pack_ik_kernel<real, 1><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->F), M,
+                                                                    reinterpret_cast<V *>(c->P));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+    }
   }
   mark(c, EV_S3);
   // back-interpolation
@@ -597,6 +604,12 @@ int run_kspace_batch(Ctx *c, const KspaceBatch &b) {
     P3MG_CUDA_TRY(cudaGetLastError());
     P3MG_TRY(fft3d(c, b.F, na, +1));
     P3MG_TRY(gather_any<real>(c, b.F, b.fk, na));
+  } else if (sizeof(real) == 4 && c->fft_w == 0 && fft_pencil_ok(c)) {
+    // FP32 pencil FFTs: the convolution folded into the first backward
+    // pass, the packing into the last
+    P3MG_TRY(ik_conv_inverse_pencil(c, c->Q, reinterpret_cast<const float *>(b.G), 2.0 * P3MG_PI / c->L, b.F, na,
+                                    b.P));
+    P3MG_TRY(gather_any<real>(c, b.P, b.fk, na));
   } else {
     conv_ik_kernel<real, Gt><<<mgrid, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), G, c->mesh,
                                                                2.0 * P3MG_PI / c->L, M, reinterpret_cast<C *>(b.F));

@@ -327,10 +327,12 @@ int fft_plan_init(Ctx *c) {
   e = cudaMemcpy(c->plan.tw, host, bytes, cudaMemcpyHostToDevice);
   free(host);
   P3MG_CUDA_TRY(e);
-  if (dbl)
+  if (dbl) {
     P3MG_TRY(set_smem_limits<double>());
-  else
+  } else {
     P3MG_TRY(set_smem_limits<float>());
+    P3MG_TRY(fft_pencil_init());
+  }
   return P3MG_OK;
 }
 
@@ -340,6 +342,7 @@ void fft_plan_free(Ctx *c) {
 }
 
 int fft3d(Ctx *c, void *data, int nbatch, int sign) {
+  if (c->fft_w == 0 && fft_pencil_ok(c)) return fft_pencil(c, data, nbatch, sign);
   if (c->precision == P3MG_FP64) return launch_fft3d<double>(c, data, nbatch, sign);
   return launch_fft3d<float>(c, data, nbatch, sign);
 }

@@ -85,7 +85,7 @@ struct Ctx {
 
   // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
   int brick = 8;
-  int fft_w = 0;    // pencils per FFT tile (0: 16 for FP32, 8 for FP64)
+  int fft_w = 0;    // FFT: 0 automatic (pencil kernels where they apply), 4/8/16 Stockham tile width
   int nbrick1 = 0;  // bricks per dimension
   // particle counts / starts per sort key: brick, then mesh point in the
   // brick (B^3 keys per brick); the range of brick b is
@@ -182,6 +182,15 @@ int free_all(Ctx *c);
 int fft_plan_init(Ctx *c);
 void fft_plan_free(Ctx *c);
 int fft3d(Ctx *c, void *data, int nbatch, int sign);
+// register-tiled pencil passes (p3mg_fft_pencil.cu): FP32, m = 32, 64, 128
+bool fft_pencil_ok(const Ctx *c);
+int fft_pencil(Ctx *c, void *data, int nbatch, int sign);
+// ik convolution of Q^ with the G of na alphas (FP32, na M), the backward
+// FFTs of their field meshes (F: 3 na M complex work space) and the packing
+// for the gather (P: NMESH na M float4), the convolution fused into the
+// first pass and the packing into the last
+int fft_pencil_init();
+int ik_conv_inverse_pencil(Ctx *c, const void *Qh, const float *G32, double s, void *F, int na, void *P);
 int fft_factor(int m, int *radix, int *npass);  // 0 when m factors into 2, 3, 4, 5, 7
 
 // inhomogeneous error estimate and error map (p3mg_inhomo.cu)
