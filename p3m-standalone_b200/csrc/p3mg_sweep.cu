@@ -15,8 +15,11 @@
 //
 // Many alphas over a narrow range (>= 24 alphas, max/min <= 2.5, no batch
 // limit given): the forces are smooth functions of t = 1/alpha^2 -- G_opt
-// is a sum of exp(-c t) terms and the pair force of erfc and Gaussian terms
-// in alpha = t^{-1/2} -- so they are evaluated exactly as above at R
+// is a sum of exp(-k^2 t / 4) terms, whose fast high-|k| ones reach the
+// forces only through the charge-assignment filter twice, and the pair
+// force is made of erfc and Gaussian terms in alpha = t^{-1/2} (G itself
+// does not interpolate to the same accuracy: the checks below are on
+// forces) -- so they are evaluated exactly as above at R
 // Chebyshev nodes in t (10 FP32, 16 FP64) and interpolated to every
 // requested alpha.  Two of the requested alphas are evaluated exactly as
 // well; the interpolation is used only if it reproduces their forces to
