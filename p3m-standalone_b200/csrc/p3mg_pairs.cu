@@ -375,23 +375,26 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               const float ar = alphaf_g[a] * (rr2 * rinv);
               const float gs = __expf(-ar * ar);
               const float ec = erfc_fit(ar, gs);
-              const float fak = qq * (ec * rinv + preff_g[a] * gs) * (rinv * rinv);
+              const float kf = (ec * rinv + preff_g[a] * gs) * (rinv * rinv);  // force / (q_i q_j r)
+              const float fak = qq * kf;
               fx[a] += fak * ex;
               fy[a] += fak * ey;
               fz[a] += fak * ez;
               if (N3) {
-                const float gx = -fak * ex, gy = -fak * ey, gz = -fak * ez;
-                const float sj = (pj.w != 0.0f) ? __fdividef(fxs, fabsf(pj.w)) : 0.0f;
-                const float sx = gx * sj, sy = gy * sj, sz = gz * sj;
+                // the partner's force -fak d in its units S_j = fxs / |q_j|:
+                // -q_i q_j kf d fxs / |q_j| = -(q_i copysign(fxs, q_j)) kf d,
+                // no division (q_j = 0: units that the flush scales by |q_j| = 0)
+                const float sk = -(pif.w * copysignf(fxs, pj.w)) * kf;
+                const float sx = sk * ex, sy = sk * ey, sz = sk * ez;
                 if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < 16777216.0f) {
                   atomicAdd(&sfji[3 * sl], __float2int_rn(sx));
                   atomicAdd(&sfji[3 * sl + 1], __float2int_rn(sy));
                   atomicAdd(&sfji[3 * sl + 2], __float2int_rn(sz));
                 } else {
                   const int o = sidx[csrc[sl]];
-                  atomicAdd(&fr[o], (double)gx);
-                  atomicAdd(&fr[(size_t)n + o], (double)gy);
-                  atomicAdd(&fr[2 * (size_t)n + o], (double)gz);
+                  atomicAdd(&fr[o], (double)(-fak * ex));
+                  atomicAdd(&fr[(size_t)n + o], (double)(-fak * ey));
+                  atomicAdd(&fr[2 * (size_t)n + o], (double)(-fak * ez));
                 }
               }
               const float term = (N3 ? 1.0f : 0.5f) * qq * ec * rinv - e_comp[a];
