@@ -32,6 +32,13 @@ sys.path.insert(0, os.path.join(ROOT, "p3m-standalone_b200"))
 WORKLOAD = dict(workload="p3m-ik-i 1M particles, box 100, mesh 128^3, cao 7, rcut 3.5, alpha 0.9",
                 method=1, n=1_000_000, box=100.0, mesh=128, cao=7, mc=1, rcut=3.5, alpha=0.9,
                 system_type=0, seed=12345)
+# The headline's parameters on 20,000 particles at density 1: small enough
+# for the reference's own full step (its O(N^2) Realteil included) to be
+# timed on the host instead of extrapolated, so both arms report one
+# measured, same-configuration step time beside the headline.
+SAME_CONFIG = dict(workload="p3m-ik-i 20,000 particles at density 1 (box 27.14), mesh 128^3, cao 7, rcut 3.5, "
+                            "alpha 0.9", method=1, n=20000, box=20000 ** (1.0 / 3.0), mesh=128, cao=7, mc=1,
+                   rcut=3.5, alpha=0.9, system_type=0, seed=12345)
 METRIC = "P3M steps/s at 1e-4 RMS force error: FP32-mixed vs FP64 plain, same B200"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
@@ -131,14 +138,38 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+# the sources that define each profiled kernel: a committed ncu count is
+# only used while these files are byte-identical to the ones it measured
+KERNEL_SOURCES = {
+    "pairs_cell_kernel": ["p3mg_pairs.cu", "p3mg_internal.cuh"],
+    "scatter_kernel": ["p3mg_assign_impl.cuh", "p3mg_internal.cuh"],
+    "gather_kernel": ["p3mg_assign_impl.cuh", "p3mg_internal.cuh"],
+}
+
+
+def kernel_source_digest(kernel):
+    """sha256 (first 16 hex digits) of the source files of `kernel`."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in KERNEL_SOURCES[kernel]:
+        with open(os.path.join(ROOT, "p3m-standalone_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
 def profile_counters(kernel):
     """DRAM bytes and warp instructions per launch of `kernel` at the headline
-    workload from the committed ncu summary (profiles/traffic.json), or {}."""
+    workload from the committed ncu summary (profiles/traffic.json), or {}
+    when there is none or it was captured from other sources than the
+    current ones (its source_digest differs)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
-            return json.load(fh).get(kernel, {})
+            d = json.load(fh).get(kernel, {})
     except Exception:
         return {}
+    if d.get("source_digest") != kernel_source_digest(kernel):
+        return {}
+    return d
 
 
 def profile_traffic(kernel):
@@ -324,7 +355,8 @@ def run_ours(args, rank, world, local_rank):
                         "hbm_frac": round(achieved / peak, 4),
                         "pairs_per_s": round(pairs_unique / (k["pairs"] * 1e-3), 1),
                         "unique_pairs_within_rcut": int(pairs_unique),
-                        "instructions_source": "profiles/traffic.json (ncu smsp__inst_executed.sum)"}
+                        "instructions_source": "profiles/traffic.json (ncu smsp__inst_executed.sum of these "
+                                               "sources, digest %s)" % kernel_source_digest("pairs_cell_kernel")}
         out = {
             "metric": METRIC,
             "value": round(value, 3),
@@ -365,6 +397,36 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clocks,
         }
     return out, results
+
+
+# ------------------------------------------------- same-config point
+
+def same_config_ours(dev, steps=20):
+    """Device time of one step (CUDA events, median of `steps`) and of one
+    step end to end through the C ABI (host buffers in, total forces out)
+    at SAME_CONFIG, FP32-mixed and FP64."""
+    import torch
+    import p3mg
+    S = SAME_CONFIG
+    x, y, z, q = p3mg.generate_system(S["system_type"], S["n"], S["box"], seed=S["seed"])
+    out = {"workload": S["workload"]}
+    for prec, tag in ((p3mg.FP32_MIXED, "fp32"), (p3mg.FP64, "fp64")):
+        with p3mg.Context(S["method"], S["mesh"], S["cao"], S["mc"], prec) as ctx:
+            ctx.set_system(x, y, z, q, S["box"])
+            ctx.influence(S["alpha"])
+            st = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+            step = _timed(st, lambda: ctx.compute(S["rcut"]), reps=steps)
+            hx = [torch.from_numpy(a).pin_memory() for a in (x, y, z, q)]
+            hf = [torch.empty(S["n"], dtype=torch.float64).pin_memory() for _ in range(3)]
+
+            def e2e():
+                ctx.set_system_ptr(S["n"], *[t.data_ptr() for t in hx], S["box"])
+                ctx.compute(S["rcut"])
+                ctx.get_total_forces_ptr(*[t.data_ptr() for t in hf])
+            e2e_ms = _timed(st, e2e, reps=steps)
+        out[tag] = {"ms_per_step": round(step, 4), "steps_per_s": round(1000.0 / step, 2),
+                    "e2e_ms_per_step": round(e2e_ms, 4), "e2e_steps_per_s": round(1000.0 / e2e_ms, 2)}
+    return out
 
 
 # ------------------------------------------------- secondary workloads
@@ -456,6 +518,31 @@ def secondary_workloads(dev):
                                                         "against FP64 P3M forces",
                              "step_ms": round(step, 4), "sweep_64_alphas_ms": round(sweep64, 2),
                              "sweep_64_over_step": round(sweep64 / step, 2)}
+
+    # the metric's accuracy point: the headline system (1M, box 100, method 1,
+    # rcut 3.5) with mesh, cao and alpha chosen by the reference's Tune search
+    # (p3mg_tune, FP32 candidates timed) for a 1e-4 RMS force error estimate;
+    # FP32-mixed and FP64 steps at those parameters and their RMS errors
+    # against the FP64 Ewald forces on 2000 seeded targets
+    x, y, z, q = p3mg.generate_system(0, W["n"], W["box"], seed=W["seed"])
+    tuned = p3mg.tune(W["method"], x, y, z, q, W["box"], W["rcut"], 1e-4, precision=p3mg.FP32_MIXED)
+    tg = np.sort(np.random.default_rng(2024).choice(W["n"], 2000, replace=False))
+    acc = {"workload": "p3m-ik-i 1M particles, box 100, rcut 3.5, (mesh, cao, alpha) from p3mg_tune for a 1e-4 "
+                       "RMS force error estimate", "tuned": tuned}
+    with p3mg.Context(W["method"], tuned["mesh"], tuned["cao"], W["mc"], p3mg.FP64) as ectx:
+        ectx.set_system(x, y, z, q, W["box"])
+        fe = ectx.ewald_forces(tg)["f"]
+    for prec, tag in ((p3mg.FP32_MIXED, "fp32"), (p3mg.FP64, "fp64")):
+        with p3mg.Context(W["method"], tuned["mesh"], tuned["cao"], W["mc"], prec) as ctx:
+            ctx.set_system(x, y, z, q, W["box"])
+            ctx.influence(tuned["alpha"])
+            st = stream_of(ctx)
+            ms = _timed(st, lambda: ctx.compute(W["rcut"]), reps=5)
+            f = ctx.get_forces()["f"]
+        acc[tag] = {"ms_per_step": round(ms, 4), "steps_per_s": round(1000.0 / ms, 2),
+                    "rms_error_vs_ewald": float(np.sqrt(np.sum((f[:, tg] - fe) ** 2) / len(tg)))}
+    acc["fp32_over_fp64"] = round(acc["fp64"]["ms_per_step"] / acc["fp32"]["ms_per_step"], 3)
+    out["accuracy_1e-4_1m"] = acc
 
     # adjoint: 50,000 separated dipoles, box 46.4, method 2, mesh 64, cao 5,
     # rcut 3, alpha 1, FP32; -dE/dx against FP64 Ewald forces on 2000 targets
@@ -597,10 +684,34 @@ def reference_sample(n_k=20000, n_r=5000):
     else:
         O.realspace(xr, yr, zr, qr, Lr, W["rcut"], W["alpha"], cells=False)
     t_r = (time.perf_counter() - t0) * (N / n_r) ** 2
-    desc = ("k-space on %d of the 1M particles (stage times t_c+t_f scaled x%d, t_g as is) + real-space "
-            "N^2 loop on %d particles at density 1 scaled x%d; FFT is the oracle's DFT standing in for FFTW"
-            % (n_k, N // n_k, n_r, (N // n_r) ** 2))
+    desc = ("extrapolated: k-space on %d of the 1M particles (stage times t_c+t_f scaled x%d, t_g as is) + "
+            "real-space N^2 loop on %d particles at density 1 scaled x%d; FFT is the oracle's DFT standing in for "
+            "FFTW" % (n_k, N // n_k, n_r, (N // n_r) ** 2))
     return t_k + t_r, desc, kind, dict(t_c=tc, t_g=tg, t_f=tf, t_real_sample=t_r / (N / n_r) ** 2)
+
+
+def same_config_reference():
+    """One measured step of the reference's own code at SAME_CONFIG: the
+    whole Calculate_forces (common.c:268-327), its timed region
+    (main.c:382-386), single-threaded -- not extrapolated."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import p3mg
+    S = SAME_CONFIG
+    x, y, z, q = p3mg.generate_system(S["system_type"], S["n"], S["box"], seed=S["seed"])
+    if O.ref_available():
+        t = O.ref_step_seconds(S["method"], S["mesh"], S["cao"], S["mc"], S["alpha"], S["rcut"], x, y, z, q,
+                               S["box"], reps=1)
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        O.forces(S["method"], S["mesh"], S["cao"], S["mc"], S["alpha"], S["rcut"], x, y, z, q, S["box"],
+                 G=np.ones(S["mesh"] ** 3), cells=False)
+        t = time.perf_counter() - t0
+        kind = "port"
+    return {"workload": S["workload"], "kind": kind, "extrapolated": False, "seconds_per_step": round(t, 4),
+            "steps_per_s": 1.0 / t, "cores": 1,
+            "note": "one full Calculate_forces (real space N^2 loop + k-space with the oracle's DFT for FFTW)"}
 
 
 def run_reference(args, rank, world):
@@ -636,9 +747,10 @@ def run_reference(args, rank, world):
         "data": "synthetic: seeded uniform system (system_type 0), +-1 charges alternating",
         "config": {"workload": WORKLOAD["workload"], "parallelism": "cpu, 1 thread"},
         "cpu_baseline": {"value": v, "unit": "steps/s", "cores": 1, "kind": kind, "sample": desc,
-                         "last_sample_parts_s": parts, "scipy_fft_128cube_1thread_s": fft_proxy,
-                         "cpu": _cpu_model()},
+                         "extrapolated": True, "last_sample_parts_s": parts,
+                         "scipy_fft_128cube_1thread_s": fft_proxy, "cpu": _cpu_model()},
         "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "same_config_measured": same_config_reference(),
     }
 
 
@@ -674,14 +786,16 @@ def main():
             print(json.dumps(out))
         return
     out, _ = run_ours(args, rank, world, local_rank)
-    if rank == 0 and world == 1 and not args.no_workloads:
+    if rank == 0 and world == 1:
         import torch
-        out["workloads"] = secondary_workloads(torch.device("cuda", local_rank))
+        out["same_config_measured"] = same_config_ours(torch.device("cuda", local_rank))
+        if not args.no_workloads:
+            out["workloads"] = secondary_workloads(torch.device("cuda", local_rank))
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             t, desc, kind, parts = reference_sample()
             out["cpu_baseline"] = {"value": 1.0 / t, "unit": "steps/s", "cores": 1, "kind": kind, "sample": desc,
-                                   "cpu": _cpu_model()}
+                                   "extrapolated": True, "cpu": _cpu_model()}
         print(json.dumps(out))
     if world > 1:
         import torch.distributed as dist

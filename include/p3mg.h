@@ -343,8 +343,7 @@ int p3mg_kernel_times(p3mg_ctx *ctx, double t[3]);
 int p3mg_set_graph(p3mg_ctx *ctx, int on);
 
 /* Real-space erfc pair forces that allocate no device memory.
- * No counterpart in the reference (its Realteil, realpart.c:124-167, is the
- * computation; this entry point only changes who owns the memory).
+ * No counterpart in the reference.
  * For callers that cannot let a library allocate GPU memory: an engine
  * whose allocator owns all device memory (a library cudaMalloc would
  * synchronise the device and fragment its pool), or a stepping loop that

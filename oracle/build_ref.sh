@@ -6,9 +6,10 @@
 # FFTW3 and GSL are absent from this image; the FFTW/GSL API subsets the
 # reference calls come from oracle/shim (the oracle's own DFT restatement and
 # a published MT19937).  Flags follow the reference Makefile:1-4, plus -fPIC.
-# Usage: sh oracle/build_ref.sh [reference_dir]
+# Usage: sh oracle/build_ref.sh <reference_dir>   (or P3M_REFERENCE_DIR set)
 set -e
-REF=${1:-/root/reference}
+REF=${1:-$P3M_REFERENCE_DIR}
+[ -n "$REF" ] || { echo "usage: sh oracle/build_ref.sh <reference_dir>" >&2; exit 2; }
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"

@@ -91,6 +91,9 @@ def ref():
                                                                          ctypes.c_double, _dp]
         R.ref_find_error.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         R.ref_find_error.restype = ctypes.c_double
+        R.ref_step_seconds.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double, ctypes.c_double, ctypes.c_int] + [
+            _dp] * 4 + [ctypes.c_double, ctypes.c_int]
+        R.ref_step_seconds.restype = ctypes.c_double
         R.ref_realteil.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double] * 3 + [_dp, _dp]
         R.ref_inhomo_error.argtypes = [ctypes.c_int] + [_dp] * 4 + [ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                                                     ctypes.c_double] + [ctypes.c_int] * 4 + [
@@ -265,6 +268,17 @@ def ref_forces(method, mesh, cao, mc, alpha, rcut, x, y, z, q, L, tuning=False, 
     if want_G:
         out["G"] = G.reshape(mesh, mesh, mesh)
     return out
+
+
+def ref_step_seconds(method, mesh, cao, mc, alpha, rcut, x, y, z, q, L, reps=1):
+    """Seconds per Calculate_forces of the reference (its timed region,
+    main.c:382-386), the mean of `reps` steps."""
+    x, y, z, q = map(_arr, (x, y, z, q))
+    t = ref().ref_step_seconds(method, mesh, cao, mc, alpha, rcut, len(x), _ptr(x), _ptr(y), _ptr(z), _ptr(q), L,
+                               int(reps))
+    if t < 0:
+        raise ValueError("ref_step_seconds failed")
+    return float(t)
 
 
 def ref_self_force_coeffs(method, mesh, cao, mc, alpha, x, y, z, q, L):

@@ -7,8 +7,10 @@
  *   method.Init (alpha = 0 as at main.c:191) -> Influence_function(alpha)
  *   -> Calculate_forces (common.c:268-327).
  */
+#define _POSIX_C_SOURCE 199309L
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #include "types.h"
 #include "common.h"
@@ -208,6 +210,42 @@ int ref_error_estimates(int method_id, int mesh, int cao, int mc, double alpha, 
  * interpolated he_q for a tabulated (mesh, cao) or -1 on a miss. */
 double ref_find_error(double alphaL, int mesh, int cao, int method_id) {
   return p3m_find_error(alphaL, mesh, cao, method_id);
+}
+
+/* Wall-clock seconds of the reference's timed region, one full
+ * Calculate_forces (common.c:268-327: zeroing, Realteil when rcut != 0,
+ * Kspace_force, f = f_k + f_r), as main.c:382-386 brackets it: Init and
+ * Influence_function run once before the clock starts.  Returns the mean of
+ * `reps` steps (<0 on an unknown method). */
+double ref_step_seconds(int method_id, int mesh, int cao, int mc, double alpha, double rcut, int n, const double *x,
+                        const double *y, const double *z, const double *q, double L, int reps) {
+  const method_t *m = method_by_id(method_id);
+  if (!m || method_id == 4 || reps < 1) return -1.0;
+  P3M_BRILLOUIN = mc;
+  system_t *s = make_system(n, x, y, z, q, L);
+  forces_t *fo = Init_forces(n);
+  parameters_t p;
+  memset(&p, 0, sizeof(p));
+  p.rcut = rcut;
+  p.mesh = mesh;
+  p.cao = cao;
+  p.cao3 = cao * cao * cao;
+  p.ip = cao - 1;
+  p.alpha = 0.0;
+  data_t *d = m->Init(s, &p);
+  p.alpha = alpha;
+  m->Influence_function(s, &p, d);
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
+  for (int r = 0; r < reps; r++) {
+    s->energy = 0.0;
+    Calculate_forces(m, s, &p, d, fo);
+  }
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  Free_data(d);
+  Free_forces(fo);
+  Free_system(s);
+  return ((double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec)) / reps;
 }
 
 /* The reference's real-space N^2 loop alone (realpart.c:124-167). */

@@ -43,6 +43,8 @@
 // lanes.  With fewer than 3 cells per side the all-pairs kernel runs.
 #include <math.h>
 
+#include <atomic>
+
 #include "p3mg_internal.cuh"
 
 namespace p3mg {
@@ -383,8 +385,10 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               if (N3) {
                 // the partner's force -fak d in its units S_j = fxs / |q_j|:
                 // -q_i q_j kf d fxs / |q_j| = -(q_i copysign(fxs, q_j)) kf d,
-                // no division (q_j = 0: units that the flush scales by |q_j| = 0)
-                const float sk = -(pif.w * copysignf(fxs, pj.w)) * kf;
+                // no division; a partner without charge takes no units (its
+                // accumulator would otherwise fill with terms the flush
+                // multiplies by |q_j| = 0)
+                const float sk = -(pif.w * (pj.w != 0.0f ? copysignf(fxs, pj.w) : 0.0f)) * kf;
                 const float sx = sk * ex, sy = sk * ey, sz = sk * ez;
                 if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < 16777216.0f) {
                   atomicAdd(&sfji[3 * sl], __float2int_rn(sx));
@@ -767,22 +771,26 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[P3MG_NOALLOC_SC
 namespace {
 
 constexpr int NA_MAX_DEVICES = 64;
-unsigned char *g_na_ptr[NA_MAX_DEVICES] = {nullptr};
+std::atomic<unsigned char *> g_na_ptr[NA_MAX_DEVICES];
 
 // Device address of the scratch array for the current device.  In host
 // code the symbol name only stands for the array, it is not an address the
 // GPU can use, so the address is looked up once per device (with that
-// device current) and cached.
+// device current) and cached.  Host threads that make their first call on
+// a device at the same time each look it up and store the same value; the
+// cache slots are atomic so that this is well defined.
 int noalloc_scratch(unsigned char **out) {
   int dev = 0;
   P3MG_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= NA_MAX_DEVICES) return P3MG_ERR_ARG;
-  if (!g_na_ptr[dev]) {
-    void *p = nullptr;
-    P3MG_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_na_ptr[dev] = (unsigned char *)p;
+  unsigned char *p = g_na_ptr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    void *a = nullptr;
+    P3MG_CUDA_TRY(cudaGetSymbolAddress(&a, g_noalloc_scratch));
+    p = (unsigned char *)a;
+    g_na_ptr[dev].store(p, std::memory_order_release);
   }
-  *out = g_na_ptr[dev];
+  *out = p;
   return P3MG_OK;
 }
 

@@ -1,9 +1,10 @@
 """Generate the committed golden fixtures from the REFERENCE itself.
 
-Run in a container that holds the reference sources (default
-/root/reference) after ``sh oracle/build_ref.sh``:
+Run in a container that holds the reference sources, after
+``sh oracle/build_ref.sh <reference_dir>``:
 
-    python tests/golden/make_golden.py [reference_dir]
+    python tests/golden/make_golden.py <reference_dir>
+    (or set P3M_REFERENCE_DIR and omit the argument)
 
 Outputs (numpy .npz, float64):
   wall.npz   -- the reference's own fixture tests-wall.pos (300 charges,
@@ -215,12 +216,19 @@ def main(ref_dir):
     print("wrote", os.path.join(HERE, "wall.npz"), os.path.join(HERE, "sweep.npz"), os.path.join(HERE, "cli"))
 
 
+def _reference_dir():
+    d = os.environ.get("P3M_REFERENCE_DIR")
+    if not d:
+        sys.exit("give the reference source directory as an argument or in P3M_REFERENCE_DIR")
+    return d
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 2 and sys.argv[1] == "--cli":
         make_cli_goldens(sys.argv[2:])  # only these command-line cases
     elif len(sys.argv) > 1 and sys.argv[1] == "--inhomo":
         make_inhomo_golden()
     elif len(sys.argv) > 1 and sys.argv[1] == "--vincent":
-        make_vincent_golden(sys.argv[2] if len(sys.argv) > 2 else "/root/reference")
+        make_vincent_golden(sys.argv[2] if len(sys.argv) > 2 else _reference_dir())
     else:
-        main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+        main(sys.argv[1] if len(sys.argv) > 1 else _reference_dir())

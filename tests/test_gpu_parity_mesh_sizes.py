@@ -1,0 +1,123 @@
+"""GPU parity at the benchmarked configuration and at every mesh size of the
+batched workloads, against the CPU oracle (not against this library's own
+FP64 path).
+
+The benchmarked step is method 1 (P3M_ik_i, p3m-ik-i.c:169-246, with the
+influence function of p3m-ik-i.c:78-166) at mesh 128, cao 7, mc 1,
+alpha 0.9, rcut 3.5 at density 1.  At a particle count the oracle finishes
+in seconds (30,000) the same parameters run every kernel the 1M-particle
+step runs: FP64 through the Stockham FFT, FP32-mixed through the
+register-tiled pencil FFT with the ik convolution folded into its first
+backward pass and the field packing into its last.  Meshes 32 and 64 (the
+other pencil sizes) run for methods 0/1/3, 48 and 96 (the tuning grid's
+other sizes, Stockham FFT) for methods 1 and 7, and 160 (the largest mesh of
+the multi-system batch) for methods 1 and 3.
+
+Bars: FP64 relative RMS <= 1e-10 on f, f_k and f_r (rel_rms =
+sqrt(sum |F_gpu - F_ref|^2) / sqrt(sum |F_ref|^2)); FP32-mixed <= 5e-6 on the
+total force f and <= 2e-5 on the k-space force f_k alone (FP32 rounding of
+the mesh, the FFTs and the interpolation; f_k is a few percent of f here).
+"""
+import functools
+
+import numpy as np
+import pytest
+
+import oracle as O
+import p3mg
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-10
+TOL_FP32_F = 5e-6
+TOL_FP32_FK = 2e-5
+
+ALPHA, RCUT, CAO, MC = 0.9, 3.5, 7, 1
+
+# method, mesh, n (density 1: L = n^(1/3))
+CASES = [
+    (1, 128, 30000),  # the benchmarked configuration's parameters
+    (0, 32, 20000),
+    (1, 32, 20000),
+    (3, 32, 20000),
+    (0, 64, 20000),
+    (1, 64, 20000),
+    (3, 64, 20000),
+    (1, 48, 20000),
+    (7, 48, 20000),
+    (1, 96, 20000),
+    (7, 96, 20000),
+    (1, 160, 20000),
+    (3, 160, 20000),
+]
+
+
+def _ids(c):
+    return "m%d_mesh%d_n%d" % c
+
+
+@functools.lru_cache(maxsize=None)
+def _system(n, seed):
+    L = float(n) ** (1.0 / 3.0)
+    return p3mg.generate_system(0, n, L, seed=seed) + (L,)
+
+
+@functools.lru_cache(maxsize=None)
+def _oracle(method, mesh, n):
+    x, y, z, q, L = _system(n, 1000 + mesh)
+    return O.forces(method, mesh, CAO, MC, ALPHA, RCUT, x, y, z, q, L, cells=True)
+
+
+def _gpu(method, mesh, n, precision, tiles=None):
+    x, y, z, q, L = _system(n, 1000 + mesh)
+    with p3mg.Context(method, mesh, CAO, MC, precision) as ctx:
+        if tiles is not None:
+            ctx.set_tiles(*tiles)
+        ctx.set_system(x, y, z, q, L)
+        ctx.influence(ALPHA)
+        return ctx.calculate_forces(RCUT)
+
+
+@pytest.mark.parametrize("case", CASES, ids=_ids)
+def test_fp64_matches_oracle(gpu, case):
+    ref = _oracle(*case)
+    out = _gpu(*case, p3mg.FP64)
+    assert O.rel_rms(out["f_k"], ref["f_k"]) <= TOL_FP64
+    assert O.rel_rms(out["f_r"], ref["f_r"]) <= TOL_FP64
+    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP64
+    assert abs(out["energy"] - ref["energy"]) <= TOL_FP64 * abs(ref["energy"])
+
+
+@pytest.mark.parametrize("case", CASES, ids=_ids)
+def test_fp32_mixed_matches_oracle(gpu, case):
+    ref = _oracle(*case)
+    out = _gpu(*case, p3mg.FP32_MIXED)
+    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
+    assert O.rel_rms(out["f_k"], ref["f_k"]) <= TOL_FP32_FK
+    assert abs(out["energy"] - ref["energy"]) <= TOL_FP32_F * abs(ref["energy"])
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c[1] in (32, 64, 128)], ids=_ids)
+def test_fp32_stockham_fft_matches_oracle(gpu, case):
+    # the same FP32 step with the Stockham FFT instead of the pencil FFT
+    # (a tile width chosen): both FFTs are held to the oracle
+    ref = _oracle(*case)
+    out = _gpu(*case, p3mg.FP32_MIXED, tiles=(8 if case[1] >= 64 else 4, 16))
+    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
+    assert O.rel_rms(out["f_k"], ref["f_k"]) <= TOL_FP32_FK
+
+
+def test_fp32_zero_charges_match_oracle(gpu):
+    # particles without charge next to charged ones: the FP32 pair kernel's
+    # Newton-3 partner accumulators take no units for them, and their forces
+    # are exactly zero
+    x, y, z, q, L = _system(20000, 77)
+    q = q.copy()
+    q[::7] = 0.0
+    ref = O.forces(1, 32, CAO, MC, ALPHA, RCUT, x, y, z, q, L, cells=True)
+    with p3mg.Context(1, 32, CAO, MC, p3mg.FP32_MIXED) as ctx:
+        ctx.set_system(x, y, z, q, L)
+        ctx.influence(ALPHA)
+        out = ctx.calculate_forces(RCUT)
+    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
+    assert not np.any(out["f_r"][:, ::7])

@@ -15,6 +15,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import oracle as O
 import p3mg
 
 pytestmark = pytest.mark.gpu
@@ -94,3 +95,64 @@ def test_noalloc_rejects_sizes_beyond_its_array(gpu):
     max_particles = 131072  # P3MG_NOALLOC_MAX_PARTICLES in include/p3mg.h
     assert f(max_particles + 1, None, None, None, None, 10.0, 3.0, 1.0, p3mg.FP64, None, None, None) == -10
     assert f(-1, None, None, None, None, 10.0, 3.0, 1.0, p3mg.FP64, None, None, None) == -1
+
+
+def _call(torch, f, s, prec, stream=None):
+    x, y, z, q, L, rcut, alpha = s
+    n = len(x)
+    dx, dy, dz, dq = _device(torch, (x, y, z, q))
+    fr = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    e = torch.zeros(1, dtype=torch.float64, device="cuda")
+    if stream is not None:
+        stream.wait_stream(torch.cuda.current_stream())
+    st = f(n, dx.data_ptr(), dy.data_ptr(), dz.data_ptr(), dq.data_ptr(), L, rcut, alpha, prec, fr.data_ptr(),
+           e.data_ptr(), None if stream is None else stream.cuda_stream)
+    assert st == 0, p3mg.load().p3mg_strerror(st)
+    torch.cuda.synchronize()
+    return fr.cpu().numpy().reshape(3, n), float(e.item())
+
+
+@pytest.mark.parametrize("system_type", [0, 4])
+def test_noalloc_capped_cell_grid(gpu, system_type):
+    """L / rcut = 50 would give 50 cells per side; the static array holds 16,
+    so the cells are about 3 rcut wide.  The Gaussian system (sigma L/6)
+    crowds the central cells past the staging capacity, so the chunked
+    candidate path runs too.  Compared with the oracle's real space and with
+    the context-based entry point, FP64 and FP32, two calls in a row."""
+    import torch
+    f = _entry(gpu)
+    n, L, rcut, alpha = 131072, 50.8, 1.0, 2.5
+    x, y, z, q = p3mg.generate_system(system_type, n, L, seed=31 + system_type)
+    s = (x, y, z, q, L, rcut, alpha)
+    fr_o, e_o = O.realspace(x, y, z, q, L, rcut, alpha, cells=True)
+    # FP32 positions are stored relative to their cell's origin; cells three
+    # times wider round them three times more coarsely (about 2e-7), and the
+    # closest pairs (about 0.01 apart among 131,072 particles) dominate the
+    # RMS force: rounding alone moves it by 6e-6 (uniform) / 1.1e-5 (Gaussian)
+    tol32 = 5e-5
+    for prec, tol in ((p3mg.FP64, TOL_FP64), (p3mg.FP32_MIXED, tol32)):
+        ref = _reference(x, y, z, q, L, rcut, alpha, prec)
+        for _ in range(2):
+            fr, e = _call(torch, f, s, prec)
+            assert _rel(fr, ref[0]) <= tol
+            assert _rel(fr, fr_o) <= tol
+            assert abs(e - e_o) <= tol * abs(e_o)
+
+
+def test_noalloc_all_pairs_branch_and_side_stream(gpu):
+    """Fewer than 3 cells per side (L < 3 rcut) takes the all-pairs kernel;
+    the second system runs the cell path on a non-default stream."""
+    import torch
+    f = _entry(gpu)
+    small = p3mg.generate_system(0, 500, 10.0, seed=41) + (10.0, 4.9, 0.7)
+    cells = p3mg.generate_system(0, 9000, 21.0, seed=42) + (21.0, 3.2, 1.0)
+    side = torch.cuda.Stream()
+    for s in (small, cells):
+        fr_o, e_o = O.realspace(*s[:4], s[4], s[5], s[6], cells=False)
+        for prec, tol in ((p3mg.FP64, TOL_FP64), (p3mg.FP32_MIXED, TOL_FP32)):
+            ref = _reference(*s[:4], s[4], s[5], s[6], prec)
+            for stream in (None, side):
+                fr, e = _call(torch, f, s, prec, stream)
+                assert _rel(fr, ref[0]) <= tol
+                assert _rel(fr, fr_o) <= tol
+                assert abs(e - e_o) <= tol * abs(e_o)
