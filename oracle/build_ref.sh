@@ -40,3 +40,15 @@ for s in $SRCS visit_writer fftw_shim gsl_shim dft; do LIBOBJS="$LIBOBJS $OBJ/$s
 $CC $CFLAGS $INC -o "$OUT/p3m" "$REF/main.c" $LIBOBJS -lm
 $CC -shared -o "$OUT/libp3mref.so" $LIBOBJS "$OBJ/ref_harness.o" -lm
 echo "built $OUT/p3m and $OUT/libp3mref.so"
+# The reference with the p3mg-backed method tables (p3m-standalone_b200/binding),
+# compiled against the reference's own headers and linked with libp3mg.so
+# (built first by p3m-standalone_b200/build.py): oracle/_ref/libp3mref_gpu.so
+PKG="$HERE/../p3m-standalone_b200"
+if [ -f "$PKG/libp3mg.so" ]; then
+  BINC="-I$PKG/binding -I$HERE/../include"
+  $CC $CFLAGS $INC $BINC -c "$PKG/binding/p3m-gpu.c" -o "$OBJ/p3m-gpu.o"
+  $CC $CFLAGS $INC $BINC -c "$HERE/ref_binding_harness.c" -o "$OBJ/ref_binding_harness.o"
+  $CC -shared -o "$OUT/libp3mref_gpu.so" $LIBOBJS "$OBJ/p3m-gpu.o" "$OBJ/ref_binding_harness.o" \
+    -L"$PKG" -lp3mg -Wl,-rpath,'$ORIGIN/../../p3m-standalone_b200' -lm
+  echo "built $OUT/libp3mref_gpu.so"
+fi

@@ -105,6 +105,34 @@ def ref():
     return _ref
 
 
+_refgpu = None
+
+
+def ref_binding_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libp3mref_gpu.so"))
+
+
+def ref_binding_forces(gpu, method, mesh, cao, mc, alpha, rcut, x, y, z, q, L, precision=0):
+    """The reference's own Init / Influence_function / Calculate_forces
+    (common.c:268-327) through its CPU method table (gpu=False) or through
+    the p3mg-backed table of p3m-standalone_b200/binding/p3m-gpu.c (gpu=True;
+    precision 0 = FP64, 1 = FP32-mixed): dict f, f_k, f_r, energy."""
+    global _refgpu
+    if _refgpu is None:
+        R = ctypes.CDLL(os.path.join(HERE, "_ref", "libp3mref_gpu.so"))
+        R.ref_binding_forces.argtypes = [ctypes.c_int] * 6 + [ctypes.c_double, ctypes.c_double, ctypes.c_int] + [
+            _dp] * 4 + [ctypes.c_double] + [_dp] * 4
+        _refgpu = R
+    x, y, z, q = map(_arr, (x, y, z, q))
+    n = len(x)
+    f, fk, fr, e = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n), np.zeros(1)
+    rc = _refgpu.ref_binding_forces(int(bool(gpu)), int(precision), method, mesh, cao, mc, alpha, rcut, n, _ptr(x),
+                                    _ptr(y), _ptr(z), _ptr(q), L, _ptr(f), _ptr(fk), _ptr(fr), _ptr(e))
+    if rc:
+        raise ValueError("ref_binding_forces failed (%d)" % rc)
+    return dict(f=f.reshape(3, n), f_k=fk.reshape(3, n), f_r=fr.reshape(3, n), energy=float(e[0]))
+
+
 def bspline(cao, x):
     w = np.zeros(8)
     dw = np.zeros(8)

@@ -115,6 +115,7 @@ int free_all(Ctx *c) {
   dfree(c->cell_key);
   dfree(c->cell_idx);
   dfree(c->cell_pos);
+  dfree(c->cell_done);
   dfree(c->Q);
   dfree(c->F);
   dfree(c->P);

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
                                                                   const int *__restrict__ start, int m, int B, int nb,
                                                                   double Hi, double shift, int SR, int SP,
                                                                   const int4 *__restrict__ lanetab,
-                                                                  typename cplx<real>::type *__restrict__ Q) {
+                                                                  real *__restrict__ Qr, int RP, int ES) {
   constexpr int NPASS = (CAO * CAO + 31) / 32;  // passes of 32 (b, c) columns
   constexpr bool FIXED = std::is_same<real, float>::value;
   typedef typename std::conditional<FIXED, int, real>::type acc_t;
@@ -165,14 +165,16 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
     if (gi >= m) gi %= m;
     if (gj >= m) gj %= m;
     if (gk >= m) gk %= m;
-    const size_t g = ((size_t)gi * m + gj) * m + gk;
+    // complex mesh (RP = m, ES = 2: real part, imaginary part) or the
+    // padded real layout of the r2c methods (RP = m + 2, ES = 1)
+    const size_t g = (((size_t)gi * m + gj) * RP + gk) * ES;
     const real v0 = FIXED ? (real)tile0[e] * inv_scale : (real)tile0[e];
     if (NMESH == 2) {
       const real v1 = FIXED ? (real)tile1[e] * inv_scale : (real)tile1[e];
-      if (v0 != (real)0) atomicAdd(&Q[g].x, v0);
-      if (v1 != (real)0) atomicAdd(&Q[g].y, v1);
+      if (v0 != (real)0) atomicAdd(&Qr[g], v0);
+      if (v1 != (real)0) atomicAdd(&Qr[g + 1], v1);
     } else {
-      if (v0 != (real)0) atomicAdd(&Q[g].x, v0);
+      if (v0 != (real)0) atomicAdd(&Qr[g], v0);
     }
   }
 }
@@ -227,6 +229,54 @@ __global__ void conv_ad_kernel(const typename cplx<real>::type *Qin, const Gt *_
   Qout[t] = v;
 }
 
+// The same convolutions on the half spectrum of the real-input methods
+// (m x m x (m/2 + 1), row pitch m/2 + 1): the loops of P3M_ik_r / P3M_ad_r
+// run k < m/2 + 1 and index G with the full-mesh r_ind = (i m + j) m + k
+// (p3m-ik-real.c:113-136, p3m-ad-real.c:92-101).
+template <typename real, typename Gt>
+__global__ void conv_ik_half_kernel(const typename cplx<real>::type *__restrict__ Q, const Gt *__restrict__ G, int m,
+                                    double twopi_over_L, size_t M, typename cplx<real>::type *__restrict__ F) {
+  typedef typename cplx<real>::type C;
+  const int H = m / 2 + 1;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)m * m * H) return;
+  G += (size_t)blockIdx.y * M;
+  F += (size_t)blockIdx.y * 3 * M;
+  const int k = (int)(t % H);
+  const size_t ij = t / H;
+  const int j = (int)(ij % m), i = (int)(ij / m);
+  const C qv = Q[t];
+  const real g = (real)G[ij * m + k];
+  const real s = (real)twopi_over_L;
+  const real qr = qv.x * g * s, qi = qv.y * g * s;
+  const real d0 = (real)dn_op(i, m), d1 = (real)dn_op(j, m), d2 = (real)dn_op(k, m);
+  C f;
+  f.x = -d0 * qi;
+  f.y = d0 * qr;
+  F[t] = f;
+  f.x = -d1 * qi;
+  f.y = d1 * qr;
+  F[M + t] = f;
+  f.x = -d2 * qi;
+  f.y = d2 * qr;
+  F[2 * M + t] = f;
+}
+
+template <typename real, typename Gt>
+__global__ void conv_ad_half_kernel(const typename cplx<real>::type *Qin, const Gt *__restrict__ G, int m, size_t M,
+                                    typename cplx<real>::type *Qout) {
+  const int H = m / 2 + 1;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)m * m * H) return;
+  G += (size_t)blockIdx.y * M;
+  Qout += (size_t)blockIdx.y * M;
+  const real g = (real)G[(t / H) * m + t % H];
+  typename cplx<real>::type v = Qin[t];
+  v.x *= g;
+  v.y *= g;
+  Qout[t] = v;
+}
+
 // ---------------------------------------------------------------- gather
 
 // Pack the three ik field meshes for the back-interpolation: per mesh point
@@ -256,6 +306,25 @@ __global__ void pack_ik_kernel(const typename cplx<real>::type *__restrict__ F, 
   }
 }
 
+// Pack the three real field meshes of method 6 (padded layout, row pitch
+// m + 2, one per slot of M complex) into (F_x, F_y, F_z, 0) per mesh point.
+template <typename real>
+__global__ void pack_ik_real_kernel(const real *__restrict__ F, int m, size_t M,
+                                    typename cplx<real>::vec4 *__restrict__ P) {
+  typedef typename cplx<real>::vec4 V;
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= M) return;
+  F += (size_t)blockIdx.y * 6 * M;  // alpha batch (grid.y): 3 slots of 2M reals
+  P += (size_t)blockIdx.y * M;
+  const size_t r = (t / m) * (m + 2) + t % m;
+  V v;
+  v.x = F[r];
+  v.y = F[2 * M + r];
+  v.z = F[4 * M + r];
+  v.w = (real)0;
+  P[t] = v;
+}
+
 // ik: f_d -= scale * q W F_d ; ad: f -= scale * phi * q/L * grad W.
 // scale = pref (one mesh) or pref/2 (interlaced, charge-assign.c:646-806).
 // One thread per brick-sorted particle; ik reads the packed fields (Fv =
@@ -265,12 +334,14 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_kernel(const double4 *_
                                                                  const int *__restrict__ sidx, int np, int m,
                                                                  double Hi, double shift, double pref, double Leni,
                                                                  const void *__restrict__ Fv, size_t M,
-                                                                 double *__restrict__ fk, int n) {
+                                                                 double *__restrict__ fk, int n, int RP, int ES) {
   typedef typename cplx<real>::type C;
   typedef typename cplx<real>::vec4 V;
   // alpha batch (grid.y): the potential (ad) or packed fields (ik) and the
   // forces of entry y
-  const C *__restrict__ F = reinterpret_cast<const C *>(Fv) + (size_t)blockIdx.y * M;
+  // ad: the potential as reals -- complex mesh (RP = m, ES = 2) or the
+  // padded real layout of the r2c methods (RP = m + 2, ES = 1)
+  const real *__restrict__ Fr = reinterpret_cast<const real *>(Fv) + (size_t)blockIdx.y * 2 * M;
   const V *__restrict__ P = reinterpret_cast<const V *>(Fv) + (size_t)blockIdx.y * NMESH * M;
   fk += (size_t)blockIdx.y * 3 * (size_t)n;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -313,12 +384,12 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_kernel(const double4 *_
             acc2 -= f.z * Bw;
           }
         } else {
+          const size_t rowr = ((size_t)gi * m + gj) * RP;
 #pragma unroll
           for (int c = 0; c < CAO; c++) {
             int gk = base[2] + c;
             gk -= (gk >= m) ? m : 0;
-            const C v = F[rowb + gk];
-            const real Bp = scale * (ii ? v.y : v.x);
+            const real Bp = scale * Fr[(rowr + gk) * ES + ii];
             acc0 -= Bp * (dx[a] * wy[b] * wz[c] * qL);
             acc1 -= Bp * (wx[a] * dy[b] * wz[c] * qL);
             acc2 -= Bp * (wx[a] * wy[b] * dz[c] * qL);
@@ -409,7 +480,6 @@ inline int scatter_row_pitch(int cao, int T, int word_bytes) {
 
 template <typename real, int CAO, int NMESH>
 int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
-  typedef typename cplx<real>::type C;
   auto kern = scatter_kernel<real, CAO, NMESH>;
   // raise the dynamic shared-memory limit once per instantiation (outside
   // any graph capture: the first step of a shape always runs eagerly)
@@ -430,9 +500,11 @@ int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
     P3MG_CUDA_TRY(cudaMalloc(&c->scatter_tab, sizeof(int4) * 32 * NPASS));
     P3MG_CUDA_TRY(cudaMemcpy(c->scatter_tab, host, sizeof(int4) * 32 * NPASS, cudaMemcpyHostToDevice));
   }
+  const bool rl = kspace_real(c);
   kern<<<nbr, ASSIGN_THREADS, smem, c->stream>>>(c->sorted_xyzq, c->brick_start, c->mesh, c->brick, c->nbrick1, Hi,
                                                 shift, SR, SP, reinterpret_cast<const int4 *>(c->scatter_tab),
-                                                reinterpret_cast<C *>(c->Q));
+                                                reinterpret_cast<real *>(c->Q), rl ? c->mesh + 2 : c->mesh,
+                                                rl ? 1 : 2);
   c->launches++;
   mark(c, EV_K3);
   P3MG_CUDA_TRY(cudaGetLastError());
@@ -459,25 +531,26 @@ int dispatch_gather(Ctx *c, const void *Fv, double *fk, int na) {
   const double Leni = 1.0 / c->L;
   const dim3 grid((c->n + ASSIGN_THREADS - 1) / ASSIGN_THREADS, na);
   const bool il = method_interlaced(c->method);
+  const int RP = kspace_real(c) ? c->mesh + 2 : c->mesh, ES = kspace_real(c) ? 1 : 2;
   mark(c, EV_K4);
   if (method_ad(c->method)) {
     // prefactor Mesh * Leni^3 (p3m-ad.c:202, p3m-ad-i.c:199, p3m-ad-real.c:110)
     const double pref = (double)c->mesh * Leni * Leni * Leni;
     if (il)
       gather_kernel<real, CAO, 2, true><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n, RP, ES);
     else
       gather_kernel<real, CAO, 1, true><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n, RP, ES);
   } else {
     // prefactor 1 / (2 L^3) (p3m-ik.c:242, p3m-ik-i.c:241, p3m-ik-real.c:144)
     const double pref = 1.0 / (2.0 * L3);
     if (il)
       gather_kernel<real, CAO, 2, false><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n, RP, ES);
     else
       gather_kernel<real, CAO, 1, false><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n);
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n, RP, ES);
   }
   c->launches++;
   mark(c, EV_K5);
@@ -523,6 +596,43 @@ int run_kspace(Ctx *c) {
   P3MG_CUDA_TRY(cudaMemsetAsync(c->Q, 0, M * sizeof(C), c->stream));
   P3MG_TRY(scatter_any<real>(c));
   mark(c, EV_S2);
+  if (kspace_real(c)) {
+    // methods 6 / 7: r2c, convolution over the half spectrum, c2r
+    typedef typename std::conditional<sizeof(real) == 8, double, float>::type Gt;
+    const Gt *G = reinterpret_cast<const Gt *>(c->precision == P3MG_FP64 ? (const void *)c->G : (const void *)c->G32);
+    const size_t Mh = (size_t)c->mesh * c->mesh * (c->mesh / 2 + 1);
+    const unsigned hblocks = (unsigned)((Mh + threads - 1) / threads);
+    P3MG_TRY(fft3d_real(c, c->Q, 1, -1));
+    if (method_ad(c->method)) {
+      conv_ad_half_kernel<real, Gt><<<hblocks, threads, 0, c->stream>>>(reinterpret_cast<C *>(c->Q), G, c->mesh, M,
+                                                                        reinterpret_cast<C *>(c->Q));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+      P3MG_TRY(fft3d_real(c, c->Q, 1, +1));
+    } else {
+      conv_ik_half_kernel<real, Gt><<<hblocks, threads, 0, c->stream>>>(
+          reinterpret_cast<const C *>(c->Q), G, c->mesh, 2.0 * P3MG_PI / c->L, M, reinterpret_cast<C *>(c->F));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+      P3MG_TRY(fft3d_real(c, c->F, 3, +1));
+      typedef typename cplx<real>::vec4 V;
+      pack_ik_real_kernel<real><<<mblocks, threads, 0, c->stream>>>(reinterpret_cast<const real *>(c->F), c->mesh, M,
+                                                                    reinterpret_cast<V *>(c->P));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+    }
+    mark(c, EV_S3);
+    P3MG_TRY(gather_any<real>(c, method_ad(c->method) ? c->Q : c->P, c->fk, 1));
+    if (method_self_force(c->method)) {
+      const int blocks = (c->n + threads - 1) / threads;
+      self_force_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, c->L / c->mesh, c->self_b,
+                                                            c->f);
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+    }
+    mark(c, EV_S4);
+    return P3MG_OK;
+  }
   // forward FFT, convolution, backward FFT(s)
   P3MG_TRY(fft3d(c, c->Q, 1, -1));
   if (method_ad(c->method)) {
@@ -591,13 +701,40 @@ int run_kspace_batch(Ctx *c, const KspaceBatch &b) {
   const int threads = 256;
   const int na = b.na;
   const dim3 mgrid((unsigned)((M + threads - 1) / threads), na);
+  const bool rl = kspace_real(c);
   if (b.forward) {
     P3MG_CUDA_TRY(cudaMemsetAsync(c->Q, 0, M * sizeof(C), c->stream));
     P3MG_TRY(scatter_any<real>(c));
-    P3MG_TRY(fft3d(c, c->Q, 1, -1));
+    if (rl)
+      P3MG_TRY(fft3d_real(c, c->Q, 1, -1));
+    else
+      P3MG_TRY(fft3d(c, c->Q, 1, -1));
   }
   const Gt *G = reinterpret_cast<const Gt *>(b.G);
-  if (method_ad(c->method)) {
+  if (rl) {
+    // methods 6 / 7: the half spectrum (r2c / c2r)
+    const size_t Mh = (size_t)c->mesh * c->mesh * (c->mesh / 2 + 1);
+    const dim3 hgrid((unsigned)((Mh + threads - 1) / threads), na);
+    if (method_ad(c->method)) {
+      conv_ad_half_kernel<real, Gt><<<hgrid, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), G, c->mesh,
+                                                                      M, reinterpret_cast<C *>(b.F));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+      P3MG_TRY(fft3d_real(c, b.F, na, +1));
+      P3MG_TRY(gather_any<real>(c, b.F, b.fk, na));
+    } else {
+      conv_ik_half_kernel<real, Gt><<<hgrid, threads, 0, c->stream>>>(
+          reinterpret_cast<const C *>(c->Q), G, c->mesh, 2.0 * P3MG_PI / c->L, M, reinterpret_cast<C *>(b.F));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+      P3MG_TRY(fft3d_real(c, b.F, 3 * na, +1));
+      pack_ik_real_kernel<real><<<mgrid, threads, 0, c->stream>>>(reinterpret_cast<const real *>(b.F), c->mesh, M,
+                                                                   reinterpret_cast<V *>(b.P));
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+      P3MG_TRY(gather_any<real>(c, b.P, b.fk, na));
+    }
+  } else if (method_ad(c->method)) {
     conv_ad_kernel<real, Gt><<<mgrid, threads, 0, c->stream>>>(reinterpret_cast<const C *>(c->Q), G, M,
                                                                reinterpret_cast<C *>(b.F));
     c->launches++;

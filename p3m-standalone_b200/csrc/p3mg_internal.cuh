@@ -102,6 +102,7 @@ struct Ctx {
   int *cell_key = nullptr;
   int *cell_idx = nullptr;
   void *cell_pos = nullptr;  // double4 (FP64) or float4 (FP32: position relative to the cell origin, q)
+  int *cell_done = nullptr;  // FP32: per cell, 1 when the half-cell group kernel finished it
 
   // mesh data (real type = double for FP64, float for FP32_MIXED)
   size_t M = 0;               // mesh^3
@@ -182,6 +183,13 @@ int free_all(Ctx *c);
 int fft_plan_init(Ctx *c);
 void fft_plan_free(Ctx *c);
 int fft3d(Ctx *c, void *data, int nbatch, int sign);
+// real-input transforms (methods 6, 7; even meshes whose half is 2/3/5/7-smooth):
+// padded real layout (row pitch m + 2 reals) <-> half spectrum
+// m x m x (m/2 + 1), in place, nbatch meshes at a slot stride of M complex
+bool fft_real_ok(const Ctx *c);
+int fft3d_real(Ctx *c, void *data, int nbatch, int sign);
+// methods 6 and 7 run the real-input transforms (r2c / c2r) where the mesh allows
+inline bool kspace_real(const Ctx *c) { return (c->method == 6 || c->method == 7) && fft_real_ok(c); }
 // register-tiled pencil passes (p3mg_fft_pencil.cu): FP32, m = 32, 64, 128
 bool fft_pencil_ok(const Ctx *c);
 int fft_pencil(Ctx *c, void *data, int nbatch, int sign);

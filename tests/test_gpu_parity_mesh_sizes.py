@@ -11,12 +11,18 @@ register-tiled pencil FFT with the ik convolution folded into its first
 backward pass and the field packing into its last.  Meshes 32 and 64 (the
 other pencil sizes) run for methods 0/1/3, 48 and 96 (the tuning grid's
 other sizes, Stockham FFT) for methods 1 and 7, and 160 (the largest mesh of
-the multi-system batch) for methods 1 and 3.
+the multi-system batch) for methods 1 and 3; the real-input methods 6 and
+7 run from mesh 16 to 128.
 
 Bars: FP64 relative RMS <= 1e-10 on f, f_k and f_r (rel_rms =
-sqrt(sum |F_gpu - F_ref|^2) / sqrt(sum |F_ref|^2)); FP32-mixed <= 5e-6 on the
-total force f and <= 2e-5 on the k-space force f_k alone (FP32 rounding of
-the mesh, the FFTs and the interpolation; f_k is a few percent of f here).
+sqrt(sum |F_gpu - F_ref|^2) / sqrt(sum |F_ref|^2)) and 1e-10 relative on the
+pair energy.  FP32-mixed: <= 5e-6 on the k-space force f_k (the mesh, the
+FFTs, the convolution and the interpolation in FP32; measured 3e-7 .. 1.2e-6
+on a B200) and <= 1.5e-5 on the real-space and total forces: the closest
+pairs dominate the RMS force (1/r^2), and FP32 coordinates relative to a
+cell origin carry about 1e-7 absolute rounding (measured 2e-6 .. 9e-6).  The
+FP32 pair energy is a sum of terms of both signs that cancel to a few
+percent of the largest ones, so its bar is 5e-4 relative.
 """
 import functools
 
@@ -29,8 +35,9 @@ import p3mg
 pytestmark = pytest.mark.gpu
 
 TOL_FP64 = 1e-10
-TOL_FP32_F = 5e-6
-TOL_FP32_FK = 2e-5
+TOL_FP32_FK = 5e-6
+TOL_FP32_F = 1.5e-5
+TOL_FP32_E = 5e-4
 
 ALPHA, RCUT, CAO, MC = 0.9, 3.5, 7, 1
 
@@ -49,6 +56,19 @@ CASES = [
     (7, 96, 20000),
     (1, 160, 20000),
     (3, 160, 20000),
+    # the real-input methods (r2c forward, convolution over the half
+    # spectrum, c2r backward: p3m-ik-real.c:72-76,108-138,
+    # p3m-ad-real.c:62-64,90-104) from mesh 16 to 128
+    (6, 16, 6000),
+    (7, 16, 6000),
+    (6, 24, 6000),
+    (7, 40, 12000),
+    (6, 32, 20000),
+    (7, 32, 20000),
+    (6, 64, 20000),
+    (7, 64, 20000),
+    (6, 128, 30000),
+    (7, 128, 30000),
 ]
 
 
@@ -92,9 +112,10 @@ def test_fp64_matches_oracle(gpu, case):
 def test_fp32_mixed_matches_oracle(gpu, case):
     ref = _oracle(*case)
     out = _gpu(*case, p3mg.FP32_MIXED)
-    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
     assert O.rel_rms(out["f_k"], ref["f_k"]) <= TOL_FP32_FK
-    assert abs(out["energy"] - ref["energy"]) <= TOL_FP32_F * abs(ref["energy"])
+    assert O.rel_rms(out["f_r"], ref["f_r"]) <= TOL_FP32_F
+    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
+    assert abs(out["energy"] - ref["energy"]) <= TOL_FP32_E * abs(ref["energy"])
 
 
 @pytest.mark.parametrize("case", [c for c in CASES if c[1] in (32, 64, 128)], ids=_ids)
@@ -103,8 +124,8 @@ def test_fp32_stockham_fft_matches_oracle(gpu, case):
     # (a tile width chosen): both FFTs are held to the oracle
     ref = _oracle(*case)
     out = _gpu(*case, p3mg.FP32_MIXED, tiles=(8 if case[1] >= 64 else 4, 16))
-    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
     assert O.rel_rms(out["f_k"], ref["f_k"]) <= TOL_FP32_FK
+    assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
 
 
 def test_fp32_zero_charges_match_oracle(gpu):
