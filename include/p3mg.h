@@ -221,10 +221,17 @@ int p3mg_backward(p3mg_ctx *ctx, double rcut, double grad_E, double *grad_x, dou
  * Results differ only by the rounding of the floating-point operations. */
 int p3mg_set_tiles(p3mg_ctx *ctx, int brick, int fft_w);
 
+/* Back-interpolation kernel of the ik methods (0, 1, 6; no counterpart in
+ * the reference): 0 (the default) puts one lane on each z offset of a
+ * particle's stencil (8 or 16 lanes per particle, each lane reading a
+ * column of consecutive mesh points), 1 runs one thread per particle.
+ * Results differ only by the rounding of the floating-point sums. */
+int p3mg_set_gather(p3mg_ctx *ctx, int mode);
+
 /* Tile autotuner (no counterpart in the reference): times the context's
- * force evaluation with rcut for every brick edge and FFT kernel, keeps
- * the fastest and returns it with its mean time in ms (outputs may be
- * NULL).  Needs p3mg_influence first. */
+ * force evaluation with rcut for every brick edge, FFT kernel and gather
+ * kernel, keeps the fastest and returns its brick edge, FFT kernel and
+ * mean time in ms (outputs may be NULL).  Needs p3mg_influence first. */
 int p3mg_autotune(p3mg_ctx *ctx, double rcut, int *brick, int *fft_w, double *ms);
 
 /* The reference's parameter tuner (Tune, tuning.c:250-370) on the GPU: for

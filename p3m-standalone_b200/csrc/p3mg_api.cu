@@ -115,7 +115,6 @@ int free_all(Ctx *c) {
   dfree(c->cell_key);
   dfree(c->cell_idx);
   dfree(c->cell_pos);
-  dfree(c->cell_done);
   dfree(c->Q);
   dfree(c->F);
   dfree(c->P);
@@ -758,6 +757,14 @@ extern "C" int p3mg_set_tiles(p3mg_ctx *h, int brick, int fft_w) {
   return set_tiles(&h->c, brick, fft_w);
 }
 
+extern "C" int p3mg_set_gather(p3mg_ctx *h, int mode) {
+  if (!h) return P3MG_ERR_ARG;
+  if (mode != 0 && mode != 1) return P3MG_ERR_ARG;
+  drop_graph(&h->c);
+  h->c.gather_mode = mode;
+  return P3MG_OK;
+}
+
 // Mean device time of `reps` steps after `warm` untimed ones (events on the
 // context stream; no graph).
 static int time_steps(Ctx *c, double rcut, int warm, int reps, double *ms) {
@@ -796,21 +803,26 @@ extern "C" int p3mg_autotune(p3mg_ctx *h, double rcut, int *brick_out, int *fft_
   // FFT: 0 = automatic (the pencil kernels where they apply), then the
   // Stockham tile widths
   const int bricks[2] = {4, 8}, ws[4] = {0, 4, 8, 16};
-  int bb = c->brick, bw = c->fft_w;
+  int bb = c->brick, bw = c->fft_w, bg = c->gather_mode;
   double best = 1e300;
   int st = P3MG_OK;
-  for (int ib = 0; ib < 2 && st == P3MG_OK; ib++)
-    for (int iw = 0; iw < 4 && st == P3MG_OK; iw++) {
-      if (bricks[ib] > c->mesh) continue;
-      st = set_tiles(c, bricks[ib], ws[iw]);
-      double ms = 0.0;
-      if (st == P3MG_OK) st = time_steps(c, rcut, 2, 5, &ms);
-      if (st == P3MG_OK && ms < best) {
-        best = ms;
-        bb = bricks[ib];
-        bw = ws[iw];
+  const int ngm = method_ad(c->method) ? 1 : 2;  // the gather variants apply to ik methods
+  for (int ig = 0; ig < ngm && st == P3MG_OK; ig++)
+    for (int ib = 0; ib < 2 && st == P3MG_OK; ib++)
+      for (int iw = 0; iw < 4 && st == P3MG_OK; iw++) {
+        if (bricks[ib] > c->mesh) continue;
+        c->gather_mode = ig;
+        st = set_tiles(c, bricks[ib], ws[iw]);
+        double ms = 0.0;
+        if (st == P3MG_OK) st = time_steps(c, rcut, 2, 5, &ms);
+        if (st == P3MG_OK && ms < best) {
+          best = ms;
+          bb = bricks[ib];
+          bw = ws[iw];
+          bg = ig;
+        }
       }
-    }
+  c->gather_mode = bg;
   if (st == P3MG_OK) st = set_tiles(c, bb, bw);
   c->timing = timing;
   if (st != P3MG_OK) return st;

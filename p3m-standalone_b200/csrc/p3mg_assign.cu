@@ -16,10 +16,12 @@
 // ((i m + j) m + k), x slowest) holds the charge density; interlaced
 // methods put the unshifted mesh in the real part and the half-cell
 // shifted mesh in the imaginary part (p3m-ik-i.c:189-190).  The r2c
-// methods (6, 7) use the same complex transform with a zero imaginary
-// part: on the k_z <= m/2 half it equals the r2c spectrum and the inverse
-// of the Hermitian products equals the c2r result, so their forces are the
-// same numbers up to rounding.
+// methods (6, 7) keep the charge in the padded real layout of an in-place
+// r2c transform (row pitch m + 2 reals, charge-assign.c:252,257), transform
+// it to the half spectrum m x m x (m/2 + 1), convolve there with G indexed
+// by the full-mesh r_ind, and transform back with c2r (p3m-ik-real.c:72-76,
+// 108-138, p3m-ad-real.c:62-64, 90-104): half the FFT bytes and flops of
+// the complex transforms.
 //
 // Scatter: particles are counting-sorted by the mesh brick (B^3 points)
 // that holds the base of their stencil; one CTA per brick accumulates the

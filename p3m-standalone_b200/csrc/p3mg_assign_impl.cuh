@@ -404,6 +404,81 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_kernel(const double4 *_
   fk[2 * (size_t)n + o] += (double)acc2;
 }
 
+// ik back-interpolation with the lanes on the z offsets of the stencil:
+// LPP lanes per particle (8 or 16), lane l < NMESH * CAO owns mesh
+// ii = l / CAO and z offset c = l % CAO and sums its CAO x CAO (a, b)
+// column.  For every (a, b) the CAO lanes of one (particle, mesh) read CAO
+// consecutive field vectors, so a load instruction touches a few whole
+// cache lines where one lane per particle (gather_kernel) touches one
+// scattered line per lane; the lane sums are then reduced over the
+// particle's lanes.  Same weights, geometry and prefactors as gather_kernel.
+template <typename real, int CAO, int NMESH>
+__global__ void __launch_bounds__(ASSIGN_THREADS) gather_lanes_kernel(const double4 *__restrict__ sxyzq,
+                                                                       const int *__restrict__ sidx, int np, int m,
+                                                                       double Hi, double shift, double pref,
+                                                                       const void *__restrict__ Fv, size_t M,
+                                                                       double *__restrict__ fk, int n) {
+  typedef typename cplx<real>::vec4 V;
+  constexpr int LPP = (NMESH * CAO <= 8) ? 8 : 16;
+  static_assert(NMESH * CAO <= 16, "lanes per particle");
+  constexpr int PPW = 32 / LPP;
+  const V *__restrict__ P = reinterpret_cast<const V *>(Fv) + (size_t)blockIdx.y * NMESH * M;
+  fk += (size_t)blockIdx.y * 3 * (size_t)n;
+  const int lane = threadIdx.x & 31;
+  const int p = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * PPW + lane / LPP;
+  const int l = lane % LPP;
+  real acc0 = 0, acc1 = 0, acc2 = 0;
+  if (p < np && l < NMESH * CAO) {
+    const double4 r = sxyzq[p];
+    const int ii = (NMESH == 2 && l >= CAO) ? 1 : 0;
+    const int c = l - ii * CAO;
+    int base[3], arg[3];
+    mesh_geometry(r.x, Hi, shift, ii, m, &base[0], &arg[0]);
+    mesh_geometry(r.y, Hi, shift, ii, m, &base[1], &arg[1]);
+    mesh_geometry(r.z, Hi, shift, ii, m, &base[2], &arg[2]);
+    real wx[CAO], wy[CAO], wz[CAO];
+    bspline_weights<real, CAO, false>(arg[0], wx, nullptr);
+    bspline_weights<real, CAO, false>(arg[1], wy, nullptr);
+    bspline_weights<real, CAO, false>(arg[2], wz, nullptr);
+    real wzc = wz[0];
+#pragma unroll
+    for (int k = 1; k < CAO; k++)
+      if (c == k) wzc = wz[k];
+    const real sw = (real)((NMESH == 2) ? 0.5 * pref : pref) * ((real)r.w * wzc);
+    int gk = base[2] + c;
+    gk -= (gk >= m) ? m : 0;
+    const V *__restrict__ Pm = P + (ii ? M : 0) + gk;
+#pragma unroll
+    for (int a = 0; a < CAO; a++) {
+      int gi = base[0] + a;
+      gi -= (gi >= m) ? m : 0;
+      const real swa = sw * wx[a];
+#pragma unroll
+      for (int b = 0; b < CAO; b++) {
+        int gj = base[1] + b;
+        gj -= (gj >= m) ? m : 0;
+        const V f = Pm[((size_t)gi * m + gj) * m];
+        const real w = swa * wy[b];
+        acc0 -= f.x * w;
+        acc1 -= f.y * w;
+        acc2 -= f.z * w;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = LPP / 2; o > 0; o >>= 1) {
+    acc0 += __shfl_xor_sync(0xffffffffu, acc0, o);
+    acc1 += __shfl_xor_sync(0xffffffffu, acc1, o);
+    acc2 += __shfl_xor_sync(0xffffffffu, acc2, o);
+  }
+  if (p < np && l == 0) {
+    const int o = sidx[p];
+    fk[o] += (double)acc0;
+    fk[(size_t)n + o] += (double)acc1;
+    fk[2 * (size_t)n + o] += (double)acc2;
+  }
+}
+
 // ---------------------------------------------------------- self forces
 
 // f_tot,d -= b_d(m') q^2 sin(2 pi (m'.x)/h) for the 27 m' (p3m-ad-self-forces.c:114-139)
@@ -542,6 +617,19 @@ int dispatch_gather(Ctx *c, const void *Fv, double *fk, int na) {
     else
       gather_kernel<real, CAO, 1, true><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
           c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n, RP, ES);
+  } else if (c->gather_mode == 0 && (il ? 2 : 1) * CAO <= 16) {
+    // prefactor 1 / (2 L^3) (p3m-ik.c:242, p3m-ik-i.c:241, p3m-ik-real.c:144);
+    // lanes on the stencil's z offsets
+    const double pref = 1.0 / (2.0 * L3);
+    constexpr int LPP2 = (2 * CAO <= 8) ? 8 : 16, LPP1 = (CAO <= 8) ? 8 : 16;
+    const size_t lanes = (size_t)c->n * (il ? LPP2 : LPP1);
+    const dim3 lgrid((unsigned)((lanes + ASSIGN_THREADS - 1) / ASSIGN_THREADS), na);
+    if (il)
+      gather_lanes_kernel<real, CAO, (2 * CAO <= 16) ? 2 : 1><<<lgrid, ASSIGN_THREADS, 0, c->stream>>>(
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Fv, c->M, fk, c->n);
+    else
+      gather_lanes_kernel<real, CAO, 1><<<lgrid, ASSIGN_THREADS, 0, c->stream>>>(
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Fv, c->M, fk, c->n);
   } else {
     // prefactor 1 / (2 L^3) (p3m-ik.c:242, p3m-ik-i.c:241, p3m-ik-real.c:144)
     const double pref = 1.0 / (2.0 * L3);

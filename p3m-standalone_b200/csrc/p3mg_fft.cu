@@ -9,6 +9,11 @@
 // shared memory (ping-pong buffers, no bit reversal), and writes the tile
 // back.  Tile layout is [element][pencil] so that the butterflies of
 // neighbouring threads touch neighbouring pencils (bank-conflict free).
+// The real-input transforms of methods 6 and 7 (fftw_plan_dft_r2c_3d /
+// c2r_3d, p3m-ik-real.c:72-76, p3m-ad-real.c:62-64) run their z axis as an
+// m/2-point complex transform of the packed real rows plus a split step
+// (fft_real_z_kernel) and their x and y axes on the m/2 + 1 columns of the
+// half spectrum.
 #include <math.h>
 #include <stdio.h>
 

@@ -86,6 +86,7 @@ struct Ctx {
   // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
   int brick = 8;
   int fft_w = 0;    // FFT: 0 automatic (pencil kernels where they apply), 4/8/16 Stockham tile width
+  int gather_mode = 0;  // ik gather: 0 lanes on the stencil's z offsets, 1 one thread per particle
   int nbrick1 = 0;  // bricks per dimension
   // particle counts / starts per sort key: brick, then mesh point in the
   // brick (B^3 keys per brick); the range of brick b is
@@ -102,7 +103,6 @@ struct Ctx {
   int *cell_key = nullptr;
   int *cell_idx = nullptr;
   void *cell_pos = nullptr;  // double4 (FP64) or float4 (FP32: position relative to the cell origin, q)
-  int *cell_done = nullptr;  // FP32: per cell, 1 when the half-cell group kernel finished it
 
   // mesh data (real type = double for FP64, float for FP32_MIXED)
   size_t M = 0;               // mesh^3

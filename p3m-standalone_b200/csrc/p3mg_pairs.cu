@@ -153,6 +153,227 @@ struct PairAcc<true> {
   typedef double type;
 };
 
+// FP32 Newton-3 pairs of a DENSE cell: one whose forward half-cells exceed
+// the staging arrays (the centre of a clustered system, a cell grid capped
+// to fewer, wider cells).  Instead of testing every staged candidate per
+// particle, the CTA takes its own half-cells A one at a time and shares one
+// candidate list among A's particles: the forward columns that can reach A
+// (clipped like a particle's columns, from A's own half-cell on) are listed
+// as (column, z) segments, A's particles are staged in blocks of DENSE_ABLK
+// and the candidates are streamed through the rest of the staging arrays in
+// chunks; a warp tests up to 32 of A's particles against 32 / P candidates
+// per instruction (P the power of two >= the block's particle count, lane =
+// candidate * P + particle) and queues the hits as (i, j) slot pairs that
+// are evaluated 32 at a time.  Both forces of a pair go to 32-bit
+// fixed-point accumulators of the two staged slots (slot s counts in units
+// fxs / |q_s|, the scale of pairs_cell_kernel with the maximum |q| of the
+// staged particles), flushed to the global forces after every chunk; a
+// contribution of thr = min(2^24, 2^30 / max(chunk, block)) units or more
+// goes straight to the global FP64 force (a slot takes at most that many
+// contributions between flushes, so no accumulator passes 2^30).  Pair
+// order: a pair belongs to the particle first in (J0, J1, J2, sorted slot)
+// order, as in pairs_cell_kernel.  Returns this thread's share of the pair
+// energy.
+constexpr int DENSE_ABLK = 128;  // particles of a half-cell staged per block
+constexpr int DENSE_NSEG = 65;   // (column, z) segments of one half-cell's candidates (13 x 5)
+
+__device__ __noinline__ double dense_cell_pairs(const float4 *__restrict__ pos32, const int *__restrict__ sidx,
+                                                const int *seg_src, const int *seg_pre, const double (*cell_off)[3],
+                                                const int *own_start, float4 *cf, int *csrc, int *acc,
+                                                unsigned *queues, double alpha, double rcut, double cs,
+                                                double *__restrict__ fr, int n) {
+  __shared__ int sa_sg[DENSE_NSEG], sa_cum[DENSE_NSEG + 1], sa_nseg;
+  __shared__ unsigned qmax_bits;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int CH = PAIR_JCH32 - DENSE_ABLK;
+  const float alphaf = (float)alpha;
+  const float rcf = (float)rcut;
+  const float fmul = fmaxf(alphaf * alphaf, 1.0f / (rcf * rcf));
+  const float rc2f = rcf * rcf;
+  const float prune_r2 = (float)(rcut * rcut * (1.0 + 1e-4));
+  const float preff = (float)(2.0 * alpha / 1.77245385090551602729816748334);
+  const float hf = (float)(0.5 * cs);
+  unsigned *q = queues + warp * PAIR_QCAP;
+  float e_sum = 0.0f, e_comp = 0.0f;
+  unsigned head = 0, tail = 0;
+  float fxs = 0.0f, fxs_inv = 0.0f, thr = 0.0f;
+  if (tid == 0) qmax_bits = 0u;
+
+  auto deposit = [&](int k, float sc, float ex, float ey, float ez, float fx, float fy, float fz) {
+    const float sx = sc * ex, sy = sc * ey, sz = sc * ez;
+    if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < thr) {
+      atomicAdd(&acc[3 * k], __float2int_rn(sx));
+      atomicAdd(&acc[3 * k + 1], __float2int_rn(sy));
+      atomicAdd(&acc[3 * k + 2], __float2int_rn(sz));
+    } else {
+      const int o = sidx[csrc[k]];
+      atomicAdd(&fr[o], (double)fx);
+      atomicAdd(&fr[(size_t)n + o], (double)fy);
+      atomicAdd(&fr[2 * (size_t)n + o], (double)fz);
+    }
+  };
+  auto process = [&](int take) {
+    __syncwarp();
+    if (lane < take) {
+      const unsigned e = q[(head + lane) & (PAIR_QCAP - 1)];
+      const int ki = (int)(e & 0xffffu), kj = (int)(e >> 16);
+      const float4 pi = cf[ki], pj = cf[kj];
+      const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
+      const float rr2 = ex * ex + ey * ey + ez * ez;
+      const float rinv = rsqrtf(rr2);
+      const float qq = pi.w * pj.w;
+      const float ar = alphaf * (rr2 * rinv);
+      const float gs = __expf(-ar * ar);
+      const float ec = erfc_fit(ar, gs);
+      const float kf = (ec * rinv + preff * gs) * (rinv * rinv);  // force / (q_i q_j r)
+      const float fak = qq * kf;
+      // i: +q_i q_j kf d in units fxs / |q_i| = q_j copysign(fxs, q_i) kf d;
+      // j: the opposite force in units fxs / |q_j|; no units without charge
+      deposit(ki, (pi.w != 0.0f ? pj.w * copysignf(fxs, pi.w) : 0.0f) * kf, ex, ey, ez, fak * ex, fak * ey,
+              fak * ez);
+      deposit(kj, -(pj.w != 0.0f ? pi.w * copysignf(fxs, pj.w) : 0.0f) * kf, ex, ey, ez, -fak * ex, -fak * ey,
+              -fak * ez);
+      const float term = qq * ec * rinv - e_comp;
+      const float tsum = e_sum + term;
+      e_comp = (tsum - e_sum) - term;
+      e_sum = tsum;
+    }
+    head += take;
+    __syncwarp();
+  };
+  auto warp_incl = [&](int v) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    return v;
+  };
+
+  for (int u = 0; u < 8; u++) {
+    const int srcA = own_start[u], nA = own_start[u + 1] - srcA;
+    if (nA == 0) continue;
+    const int U0 = (u >> 2) & 1, U1 = (u >> 1) & 1, U2 = u & 1;
+    __syncthreads();
+    if (warp == 0) {
+      // A's candidate segments in column order (lane r < 25 owns column
+      // (J0, J1) = (U0 - 2 + r / 5, U1 - 2 + r % 5); only the forward ones
+      // r >= 12; z cut to the half-cells within rcut of A)
+      int sgl = 0, nz = 0;
+      if (lane >= 12 && lane < 25) {
+        const int dj0 = lane / 5 - 2, dj1 = lane % 5 - 2;
+        const float dx = (float)max(abs(dj0) - 1, 0) * hf, dy = (float)max(abs(dj1) - 1, 0) * hf;
+        const float d2 = dx * dx + dy * dy;
+        if (d2 <= prune_r2) {
+          const int kz = min(2, 1 + (int)floorf(sqrtf(prune_r2 - d2) / hf));
+          const int lo = (lane == 12) ? U2 : U2 - kz, hi = U2 + kz;
+          sgl = (U0 + dj0 + 2) * 36 + (U1 + dj1 + 2) * 6 + 2 + lo;
+          nz = hi - lo + 1;
+        }
+      }
+      const int len = nz ? seg_pre[sgl + nz] - seg_pre[sgl] : 0;
+      const int in_s = warp_incl(nz), in_l = warp_incl(len);
+      const int s0 = in_s - nz;
+      int cum = in_l - len;
+      for (int zz = 0; zz < nz; zz++) {
+        const int sg = sgl + zz;
+        sa_sg[s0 + zz] = sg;
+        sa_cum[s0 + zz] = cum;
+        cum += seg_pre[sg + 1] - seg_pre[sg];
+      }
+      if (lane == 31) {
+        sa_nseg = in_s;
+        sa_cum[in_s] = in_l;
+      }
+    }
+    __syncthreads();
+    const int nseg = sa_nseg, C = sa_cum[nseg];
+    for (int ab0 = 0; ab0 < nA; ab0 += DENSE_ABLK) {
+      const int nab = min(DENSE_ABLK, nA - ab0);
+      for (int cc0 = 0; cc0 < C; cc0 += CH) {
+        const int ncand = min(CH, C - cc0);
+        __syncthreads();
+        // stage the A block (own cell: no offset) and the candidate chunk
+        float qm = 0.0f;
+        for (int t = tid; t < nab; t += PAIR_CTA) {
+          const int src = srcA + ab0 + t;
+          const float4 p = pos32[src];
+          cf[t] = p;
+          csrc[t] = src;
+          acc[3 * t] = acc[3 * t + 1] = acc[3 * t + 2] = 0;
+          qm = fmaxf(qm, fabsf(p.w));
+        }
+        for (int t = tid; t < ncand; t += PAIR_CTA) {
+          const int c = cc0 + t;
+          int sidx_s = 0;
+#pragma unroll
+          for (int step = 64; step > 0; step >>= 1)
+            if (sidx_s + step < nseg && sa_cum[sidx_s + step] <= c) sidx_s += step;
+          const int sg = sa_sg[sidx_s];
+          const int src = seg_src[sg] + (c - sa_cum[sidx_s]);
+          const int J0 = sg / 36, J1 = (sg / 6) % 6, J2 = sg % 6;
+          const int cidx = ((J0 / 2) * 3 + J1 / 2) * 3 + J2 / 2;
+          const float4 p = pos32[src];
+          const int k = DENSE_ABLK + t;
+          csrc[k] = src;
+          acc[3 * k] = acc[3 * k + 1] = acc[3 * k + 2] = 0;
+          cf[k] = make_float4(p.x + (float)cell_off[cidx][0], p.y + (float)cell_off[cidx][1],
+                              p.z + (float)cell_off[cidx][2], p.w);
+          qm = fmaxf(qm, fabsf(p.w));
+        }
+        qm = __int_as_float(__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(qm)));
+        if (lane == 0) atomicMax(&qmax_bits, (unsigned)__float_as_int(qm));
+        __syncthreads();
+        const float fscale = __int_as_float((int)qmax_bits) * fmul;
+        fxs = fscale > 0.0f ? 1048576.0f / fscale : 0.0f;
+        fxs_inv = fscale * (1.0f / 1048576.0f);
+        thr = fminf(16777216.0f, 1073741824.0f / (float)max(ncand, nab));
+        for (int a0 = 0; a0 < nab; a0 += 32) {
+          const int ng = min(32, nab - a0);
+          const int lp = 32 - __clz(ng - 1);  // P = 2^lp >= ng
+          const int ia = lane & ((1 << lp) - 1);
+          const bool aval = ia < ng;
+          const int ki = a0 + (aval ? ia : 0);
+          const float4 pa = cf[ki];
+          const int srci = csrc[ki];
+          const int cpr = 32 >> lp;
+          for (int cb = warp * cpr; cb < ncand; cb += PAIR_WARPS * cpr) {
+            const int t = cb + (lane >> lp);
+            const bool valid = aval && t < ncand;
+            const int kk = DENSE_ABLK + (valid ? t : 0);
+            const int srcc = csrc[kk];
+            const float4 pc = cf[kk];
+            const float dx = pa.x - pc.x, dy = pa.y - pc.y, dz = pa.z - pc.z;
+            // forward: every candidate outside A; inside A the later slots
+            const bool ok = valid & (srcc < srcA || srcc >= srcA + nA || srcc > srci) &
+                            (dx * dx + dy * dy + dz * dz <= rc2f);
+            const unsigned mask = __ballot_sync(0xffffffffu, ok);
+            if (ok)
+              q[(tail + __popc(mask & ((1u << lane) - 1u))) & (PAIR_QCAP - 1)] = (unsigned)ki | ((unsigned)kk << 16);
+            tail += __popc(mask);
+            if (tail - head >= 32) process(32);
+          }
+        }
+        if (tail != head) process((int)(tail - head));
+        __syncthreads();
+        if (tid == 0) qmax_bits = 0u;  // every thread read it before the barrier above
+        for (int k = tid; k < DENSE_ABLK + ncand; k += PAIR_CTA) {
+          if (k >= nab && k < DENSE_ABLK) continue;
+          const int ix = acc[3 * k], iy = acc[3 * k + 1], iz = acc[3 * k + 2];
+          if (ix != 0 || iy != 0 || iz != 0) {
+            const float inv = fxs_inv * fabsf(cf[k].w);
+            const int o = sidx[csrc[k]];
+            atomicAdd(&fr[o], (double)((float)ix * inv));
+            atomicAdd(&fr[(size_t)n + o], (double)((float)iy * inv));
+            atomicAdd(&fr[2 * (size_t)n + o], (double)((float)iz * inv));
+          }
+        }
+      }
+    }
+  }
+  return (double)e_sum - (double)e_comp;
+}
+
 template <bool DBL, int NA>
 __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__restrict__ posv,
                                                                const int *__restrict__ sidx,
@@ -160,11 +381,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
                                                                double rcut, double alpha_v,
                                                                const double *__restrict__ alphas, int nalpha,
                                                                double *__restrict__ fr, int n,
-                                                               double *__restrict__ energy,
-                                                               const int *__restrict__ done) {
+                                                               double *__restrict__ energy) {
   typedef typename PairAcc<DBL>::type acc_t;
-  // cells the half-cell group kernel has finished (FP32, one alpha)
-  if (done && done[blockIdx.x]) return;
   // alpha batch: grid.y = group of NA alphas (alphas on the device), outputs
   // per alpha k at fr + 3 n k and energy + k; without alphas the scalar alpha_v
   const int a0 = blockIdx.y * NA;
@@ -268,7 +486,14 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
     e_sum[a] = e_comp[a] = 0.0f;
   }
 
-  for (int ib = i0; ib < i1; ib += MAXI) {
+  double e_dense = 0.0;
+  if (N3 && !fits) {
+    // FP32 Newton-3 and the forward neighbourhood does not fit: half-cell
+    // groups with streamed candidates (dense_cell_pairs)
+    e_dense = dense_cell_pairs(pos32, sidx, seg_src, seg_pre, cell_off, own_start, cf, csrc, sfji,
+                               reinterpret_cast<unsigned *>(spi), alpha, rcut, cs, fr, n);
+  }
+  for (int ib = i0; ib < ((N3 && !fits) ? i0 : i1); ib += MAXI) {
     const int ni = min(MAXI, i1 - ib);
     __syncthreads();
     float qmi = 0.0f;
@@ -536,7 +761,7 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   }
 #pragma unroll
   for (int a = 0; a < NA; a++) {
-    double e_loc = DBL ? e_d[a] : ((double)e_sum[a] - (double)e_comp[a]);
+    double e_loc = DBL ? e_d[a] : ((double)e_sum[a] - (double)e_comp[a]) + (a == 0 ? e_dense : 0.0);
     for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
     if (lane == 0) ered[warp][a] = e_loc;
   }
@@ -548,260 +773,12 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   }
 }
 
-// FP32 pair forces with Newton's third law, one half-cell of the CTA's cell
-// at a time.  The staging and the pair order are those of
-// pairs_cell_kernel (the forward half of the 6^3 half-cells in (J0, J1, J2,
-// slot) order), but the candidate search is shared by every particle of a
-// half-cell A instead of being repeated per particle: a warp concatenates
-// the forward columns that can reach A once into a table of staged slots,
-// then tests |A| particles x (32 / P) candidates per instruction, P the
-// power of two >= |A| (lane = candidate * P + particle), and queues the
-// hits as (i, j) slot pairs that are evaluated 32 at a time.  Both forces
-// of a pair go to 32-bit fixed-point accumulators of the two staged slots
-// (slot s counts in units fxs / |q_s|), added to the global forces at the
-// end.  A contribution of t units or more goes straight to the global FP64
-// force instead, t = min(2^24, 2^30 / (staged + own particles)) -- a slot
-// receives at most that many contributions, so no accumulator passes 2^30.
-// A CTA whose forward half-cells exceed the staging capacity leaves its
-// cell to pairs_cell_kernel (done[cell] = 0).
-constexpr int GRP_TAB = 384;  // candidate-table entries per warp
-
-__host__ __device__ constexpr size_t group_smem_bytes() {
-  return (size_t)PAIR_JCH32 * (sizeof(float4) + sizeof(int) + 3 * sizeof(int)) +
-         (size_t)PAIR_WARPS * (GRP_TAB * sizeof(unsigned short) + PAIR_QCAP * sizeof(unsigned));
-}
-
-__global__ void __launch_bounds__(PAIR_CTA) pairs_group_kernel(const float4 *__restrict__ pos32,
-                                                                const int *__restrict__ sidx,
-                                                                const int *__restrict__ start, int nc, double L,
-                                                                double rcut, const double *__restrict__ alphas,
-                                                                double alpha_v, double *__restrict__ fr, int n,
-                                                                double *__restrict__ energy, int *__restrict__ done) {
-  extern __shared__ __align__(16) unsigned char grp_smem[];
-  float4 *cf = reinterpret_cast<float4 *>(grp_smem);
-  int *csrc = reinterpret_cast<int *>(cf + PAIR_JCH32);
-  int *acc = csrc + PAIR_JCH32;  // 3 fixed-point force components per staged slot
-  unsigned short *tabs = reinterpret_cast<unsigned short *>(acc + 3 * PAIR_JCH32);
-  unsigned *queues = reinterpret_cast<unsigned *>(tabs + PAIR_WARPS * GRP_TAB);
-  __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
-  __shared__ float cell_offf[27][3];
-  __shared__ double ered[PAIR_WARPS];
-  __shared__ unsigned qmax_bits;
-  __shared__ int own_seg[8], own_cnt[8];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int cell = blockIdx.x;
-  const int c2 = cell % nc, c1 = (cell / nc) % nc, c0 = cell / (nc * nc);
-  const double cs = L / nc;
-  const double alpha = alphas ? alphas[0] : alpha_v;
-  if (tid < 27) {
-    cell_offf[tid][0] = (float)((tid / 9 - 1) * cs);
-    cell_offf[tid][1] = (float)(((tid / 3) % 3 - 1) * cs);
-    cell_offf[tid][2] = (float)((tid % 3 - 1) * cs);
-  }
-  if (tid == 0) qmax_bits = 0u;
-  for (int sg = tid; sg < PAIR_NSEG; sg += PAIR_CTA) {
-    const int J0 = sg / 36 - 2, J1 = (sg / 6) % 6 - 2, J2 = sg % 6 - 2;
-    const int d0 = (J0 + 2) / 2 - 1, d1 = (J1 + 2) / 2 - 1, d2 = (J2 + 2) / 2 - 1;
-    const int v0 = (J0 + 2) & 1, v1 = (J1 + 2) & 1, v2 = (J2 + 2) & 1;
-    const int w0 = wrap_full(c0 + d0, nc), w1 = wrap_full(c1 + d1, nc), w2 = wrap_full(c2 + d2, nc);
-    const int key = ((w0 * nc + w1) * nc + w2) * 8 + (v0 << 2) + (v1 << 1) + v2;
-    const bool forward = J0 >= 1 || (J0 == 0 && (J1 >= 1 || (J1 == 0 && J2 >= 0)));
-    seg_src[sg] = start[key];
-    seg_pre[sg + 1] = forward ? start[key + 1] - start[key] : 0;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    seg_pre[0] = 0;
-    for (int sg = 0; sg < PAIR_NSEG; sg++) seg_pre[sg + 1] += seg_pre[sg];
-  }
-  __syncthreads();
-  const int total = seg_pre[PAIR_NSEG];
-  if (total > PAIR_JCH32) {
-    if (tid == 0) done[cell] = 0;
-    return;
-  }
-  if (tid < 8) {
-    const int sg = (2 + ((tid >> 2) & 1)) * 36 + (2 + ((tid >> 1) & 1)) * 6 + 2 + (tid & 1);
-    own_seg[tid] = seg_pre[sg];
-    own_cnt[tid] = seg_pre[sg + 1] - seg_pre[sg];
-  }
-  // stage the forward half-cells: positions relative to this cell's origin
-  float qm = 0.0f;
-  for (int kk = tid; kk < total; kk += PAIR_CTA) {
-    int sg = 0;
-#pragma unroll
-    for (int step = 128; step > 0; step >>= 1)
-      if (sg + step < PAIR_NSEG && seg_pre[sg + step] <= kk) sg += step;
-    const int src = seg_src[sg] + (kk - seg_pre[sg]);
-    const int J0 = sg / 36, J1 = (sg / 6) % 6, J2 = sg % 6;
-    const int cidx = ((J0 / 2) * 3 + J1 / 2) * 3 + J2 / 2;
-    const float4 p = pos32[src];
-    csrc[kk] = src;
-    acc[3 * kk] = acc[3 * kk + 1] = acc[3 * kk + 2] = 0;
-    cf[kk] = make_float4(p.x + cell_offf[cidx][0], p.y + cell_offf[cidx][1], p.z + cell_offf[cidx][2], p.w);
-    qm = fmaxf(qm, fabsf(p.w));
-  }
-  qm = __int_as_float(__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(qm)));
-  if (lane == 0) atomicMax(&qmax_bits, (unsigned)__float_as_int(qm));
-  __syncthreads();
-  // fixed-point scale (slot s counts in units fxs / |q_s|) and the largest
-  // contribution kept in shared memory
-  const float alphaf = (float)alpha;
-  const float rcf = (float)rcut;
-  const float fscale = __int_as_float((int)qmax_bits) * fmaxf(alphaf * alphaf, 1.0f / (rcf * rcf));
-  const float fxs = fscale > 0.0f ? 1048576.0f / fscale : 0.0f;
-  const float fxs_inv = fscale * (1.0f / 1048576.0f);
-  const int n_own = own_seg[7] + own_cnt[7] - own_seg[0];
-  const float thr = fminf(16777216.0f, 1073741824.0f / (float)(total + n_own));
-  const float rc2f = rcf * rcf;
-  const float prune_r2 = (float)(rcut * rcut * (1.0 + 1e-4));
-  const float preff = (float)(2.0 * alpha / 1.77245385090551602729816748334);
-  const float hf = (float)(0.5 * cs);
-  unsigned short *tab = tabs + warp * GRP_TAB;
-  unsigned *q = queues + warp * PAIR_QCAP;
-  float e_sum = 0.0f, e_comp = 0.0f;
-  unsigned head = 0, tail = 0;
-
-  // add one fixed-point contribution (s units along d) to slot k, or the
-  // force itself to the global FP64 force when it is too large
-  auto deposit = [&](int k, float s, float ex, float ey, float ez, float fx, float fy, float fz) {
-    const float sx = s * ex, sy = s * ey, sz = s * ez;
-    if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < thr) {
-      atomicAdd(&acc[3 * k], __float2int_rn(sx));
-      atomicAdd(&acc[3 * k + 1], __float2int_rn(sy));
-      atomicAdd(&acc[3 * k + 2], __float2int_rn(sz));
-    } else {
-      const int o = sidx[csrc[k]];
-      atomicAdd(&fr[o], (double)fx);
-      atomicAdd(&fr[(size_t)n + o], (double)fy);
-      atomicAdd(&fr[2 * (size_t)n + o], (double)fz);
-    }
-  };
-  // evaluate `take` queued pairs (one per lane) and pop them
-  auto process = [&](int take) {
-    __syncwarp();
-    if (lane < take) {
-      const unsigned e = q[(head + lane) & (PAIR_QCAP - 1)];
-      const int ki = (int)(e & 0xffffu), kj = (int)(e >> 16);
-      const float4 pi = cf[ki], pj = cf[kj];
-      const float ex = pi.x - pj.x, ey = pi.y - pj.y, ez = pi.z - pj.z;
-      const float rr2 = ex * ex + ey * ey + ez * ez;
-      const float rinv = rsqrtf(rr2);
-      const float qq = pi.w * pj.w;
-      const float ar = alphaf * (rr2 * rinv);
-      const float gs = __expf(-ar * ar);
-      const float ec = erfc_fit(ar, gs);
-      const float kf = (ec * rinv + preff * gs) * (rinv * rinv);  // force / (q_i q_j r)
-      const float fak = qq * kf;
-      // i: +q_i q_j kf d in units fxs / |q_i| = q_j copysign(fxs, q_i) kf d;
-      // j: the opposite force in units fxs / |q_j|; a slot without charge
-      // takes no units
-      deposit(ki, (pi.w != 0.0f ? pj.w * copysignf(fxs, pi.w) : 0.0f) * kf, ex, ey, ez, fak * ex, fak * ey,
-              fak * ez);
-      deposit(kj, -(pj.w != 0.0f ? pi.w * copysignf(fxs, pj.w) : 0.0f) * kf, ex, ey, ez, -fak * ex, -fak * ey,
-              -fak * ez);
-      const float term = qq * ec * rinv - e_comp;
-      const float tsum = e_sum + term;
-      e_comp = (tsum - e_sum) - term;
-      e_sum = tsum;
-    }
-    head += take;
-    __syncwarp();
-  };
-
-  for (int u = warp; u < 8; u += PAIR_WARPS) {
-    const int nA = own_cnt[u];
-    if (nA == 0) continue;
-    const int sA = own_seg[u];
-    const int U0 = (u >> 2) & 1, U1 = (u >> 1) & 1, U2 = u & 1;
-    // the forward columns that can reach half-cell A: lane r < 25 owns
-    // column (J0, J1) = (U0 - 2 + r / 5, U1 - 2 + r % 5); columns before
-    // A's own in (J0, J1) order hold no forward partner, A's own column
-    // starts at A; the z range is cut to the half-cells within rcut of A
-    int ca = 0, clen = 0;
-    if (lane >= 12 && lane < 25) {
-      const int dj0 = lane / 5 - 2, dj1 = lane % 5 - 2;
-      const float dx = (float)max(abs(dj0) - 1, 0) * hf, dy = (float)max(abs(dj1) - 1, 0) * hf;
-      const float d2 = dx * dx + dy * dy;
-      if (d2 <= prune_r2) {
-        const int kz = min(2, 1 + (int)floorf(sqrtf(prune_r2 - d2) / hf));
-        const int lo = (lane == 12) ? U2 : U2 - kz, hi = U2 + kz;
-        const int base = (U0 + dj0 + 2) * 36 + (U1 + dj1 + 2) * 6 + 2;
-        ca = seg_pre[base + lo];
-        clen = seg_pre[base + hi + 1] - ca;
-      }
-    }
-    int incl = clen;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    const int C = __shfl_sync(0xffffffffu, incl, 31);
-    const int excl = incl - clen;
-    for (int cc0 = 0; cc0 < C; cc0 += GRP_TAB) {
-      const int cend = min(C, cc0 + GRP_TAB);
-      __syncwarp();
-      // this lane's column entries inside the table chunk
-      const int t0 = max(excl, cc0), t1 = min(excl + clen, cend);
-      for (int t = t0; t < t1; t++) tab[t - cc0] = (unsigned short)(ca + (t - excl));
-      __syncwarp();
-      for (int a0 = 0; a0 < nA; a0 += 32) {
-        const int ng = min(32, nA - a0);
-        const int lp = 32 - __clz(ng - 1);  // P = 2^lp >= ng
-        const int P = 1 << lp;
-        const int ia = lane & (P - 1);
-        const bool aval = ia < ng;
-        const int ki = sA + a0 + (aval ? ia : 0);
-        const float4 pa = cf[ki];
-        const int cpr = 32 >> lp;
-        for (int cb = cc0; cb < cend; cb += cpr) {
-          const int c = cb + (lane >> lp);
-          const bool valid = aval && c < cend;
-          const int kk = tab[valid ? c - cc0 : 0];
-          const float4 pc = cf[kk];
-          const float dx = pa.x - pc.x, dy = pa.y - pc.y, dz = pa.z - pc.z;
-          const bool ok = valid & (kk > ki) & (dx * dx + dy * dy + dz * dz <= rc2f);
-          const unsigned mask = __ballot_sync(0xffffffffu, ok);
-          if (ok) q[(tail + __popc(mask & ((1u << lane) - 1u))) & (PAIR_QCAP - 1)] = (unsigned)ki | ((unsigned)kk << 16);
-          tail += __popc(mask);
-          if (tail - head >= 32) process(32);
-        }
-      }
-    }
-  }
-  if (tail != head) process((int)(tail - head));
-  __syncthreads();
-  // the staged slots' forces, added to the global forces
-  for (int kk = tid; kk < total; kk += PAIR_CTA) {
-    const int ix = acc[3 * kk], iy = acc[3 * kk + 1], iz = acc[3 * kk + 2];
-    if (ix != 0 || iy != 0 || iz != 0) {
-      const float inv = fxs_inv * fabsf(cf[kk].w);
-      const int o = sidx[csrc[kk]];
-      atomicAdd(&fr[o], (double)((float)ix * inv));
-      atomicAdd(&fr[(size_t)n + o], (double)((float)iy * inv));
-      atomicAdd(&fr[2 * (size_t)n + o], (double)((float)iz * inv));
-    }
-  }
-  double e_loc = (double)e_sum - (double)e_comp;
-  for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
-  if (lane == 0) ered[warp] = e_loc;
-  __syncthreads();
-  if (tid == 0) {
-    double s = 0.0;
-    for (int w = 0; w < PAIR_WARPS; w++) s += ered[w];
-    if (s != 0.0) atomicAdd(energy, s);
-    done[cell] = 1;
-  }
-}
-
 // Launch the cell kernel (FP64 or FP32 positions, already half-cell sorted).
 // An alpha batch (alphas with nalpha > 1) runs in groups of PAIR_NA32 /
 // PAIR_NA64 alphas per CTA.
 template <bool DBL, int NA>
 int launch_cells_na(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
-                    const double *alphas, int nalpha, double *fr, int n, double *energy, cudaStream_t s,
-                    const int *done = nullptr) {
+                    const double *alphas, int nalpha, double *fr, int n, double *energy, cudaStream_t s) {
   static bool attr_set = false;
   const size_t smem = pair_smem_bytes(DBL, NA);
   if (!attr_set) {
@@ -812,33 +789,15 @@ int launch_cells_na(const void *pos, const int *sidx, const int *start, int nc, 
   const int groups = alphas ? (nalpha + NA - 1) / NA : 1;
   const dim3 grid(nc * nc * nc, groups);
   pairs_cell_kernel<DBL, NA><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr,
-                                                         n, energy, done);
+                                                         n, energy);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
 
-// FP32, one alpha, with a per-cell flag array: the half-cell group kernel,
-// then the cell kernel for the cells it left (their neighbourhood exceeded
-// the staging capacity).  Two launches.
-int launch_group(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
-                 const double *alphas, double *fr, int n, double *energy, int *done, cudaStream_t s) {
-  static bool attr_set = false;
-  const size_t smem = group_smem_bytes();
-  if (!attr_set) {
-    P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
-  pairs_group_kernel<<<nc * nc * nc, PAIR_CTA, smem, s>>>(reinterpret_cast<const float4 *>(pos), sidx, start, nc, L,
-                                                          rcut, alphas, alpha, fr, n, energy, done);
-  P3MG_CUDA_TRY(cudaGetLastError());
-  return launch_cells_na<false, 1>(pos, sidx, start, nc, L, rcut, alpha, alphas, 1, fr, n, energy, s, done);
-}
-
 int launch_pairs_cells(bool dbl, const void *pos, const int *sidx, const int *start, int nc, double L, double rcut,
                        double alpha, const double *alphas, int nalpha, double *fr, int n, double *energy,
-                       cudaStream_t s, int *done = nullptr) {
+                       cudaStream_t s) {
   const bool group = alphas != nullptr && nalpha > 1;
-  if (!dbl && !group && done) return launch_group(pos, sidx, start, nc, L, rcut, alpha, alphas, fr, n, energy, done, s);
   if (dbl)
     return group ? launch_cells_na<true, PAIR_NA64>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr, n,
                                                      energy, s)
@@ -935,9 +894,6 @@ int pairs_reserve(Ctx *c, double rcut) {
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_count, sizeof(int) * nkey));
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_start, sizeof(int) * (nkey + 1)));
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_fill, sizeof(int) * nkey));
-    if (c->cell_done) cudaFree(c->cell_done);
-    c->cell_done = nullptr;
-    P3MG_CUDA_TRY(cudaMalloc(&c->cell_done, sizeof(int) * (nkey / 8)));
     c->ncell_cap = nkey;
     P3MG_TRY(scan_tmp_reserve(c, nkey));
   }
@@ -996,10 +952,9 @@ int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr,
   }
   P3MG_TRY(pairs_bin(c, rcut, &nc));
   mark(c, EV_K0);
-  const bool grp = c->precision != P3MG_FP64 && !(alphas != nullptr && nalpha > 1);
   P3MG_TRY(launch_pairs_cells(c->precision == P3MG_FP64, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut,
-                              0.0, alphas, nalpha, fr, n, energy, c->stream, c->cell_done));
-  c->launches += grp ? 2 : 1;
+                              0.0, alphas, nalpha, fr, n, energy, c->stream));
+  c->launches++;
   mark(c, EV_K1);
   return P3MG_OK;
 }

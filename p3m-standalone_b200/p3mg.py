@@ -103,6 +103,7 @@ def load():
     L.p3mg_energy.argtypes = [vp, ctypes.c_double, _dp]
     L.p3mg_backward.argtypes = [vp, ctypes.c_double, ctypes.c_double] + [_dp] * 7
     L.p3mg_set_tiles.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    L.p3mg_set_gather.argtypes = [vp, ctypes.c_int]
     _ip = ctypes.POINTER(ctypes.c_int)
     L.p3mg_autotune.argtypes = [vp, ctypes.c_double, _ip, _ip, _dp]
     L.p3mg_tune.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_dp] * 4 + [ctypes.c_double] * 3 + [
@@ -321,6 +322,10 @@ class Context:
 
     def set_tiles(self, brick, fft_w=0):
         _check(self._lib.p3mg_set_tiles(self._h, int(brick), int(fft_w)), "p3mg_set_tiles")
+
+    def set_gather(self, mode):
+        """ik back-interpolation kernel: 0 lanes on the stencil's z offsets, 1 one thread per particle."""
+        _check(self._lib.p3mg_set_gather(self._h, int(mode)), "p3mg_set_gather")
 
     def autotune(self, rcut):
         """Tile autotuner (p3mg_autotune): dict brick, fft_w, ms."""

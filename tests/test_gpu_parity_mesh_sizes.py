@@ -142,3 +142,38 @@ def test_fp32_zero_charges_match_oracle(gpu):
         out = ctx.calculate_forces(RCUT)
     assert O.rel_rms(out["f"], ref["f"]) <= TOL_FP32_F
     assert not np.any(out["f_r"][:, ::7])
+
+
+@pytest.mark.parametrize("case", [(1, 128, 30000), (0, 32, 20000), (6, 64, 20000)], ids=_ids)
+@pytest.mark.parametrize("precision", [p3mg.FP64, p3mg.FP32_MIXED])
+def test_gather_variants_match_oracle(gpu, case, precision):
+    # both ik back-interpolation kernels (lanes on the stencil's z offsets,
+    # one thread per particle) against the oracle
+    ref = _oracle(*case)
+    method, mesh, n = case
+    x, y, z, q, L = _system(n, 1000 + mesh)
+    tol = TOL_FP64 if precision == p3mg.FP64 else TOL_FP32_FK
+    with p3mg.Context(method, mesh, CAO, MC, precision) as ctx:
+        ctx.set_system(x, y, z, q, L)
+        ctx.influence(ALPHA)
+        for mode in (1, 0):
+            ctx.set_gather(mode)
+            fk = ctx.calculate_forces(0.0)["f_k"]
+            assert O.rel_rms(fk, ref["f_k"]) <= tol
+
+
+@pytest.mark.parametrize("system_type,n,L", [(4, 30000, 31.0), (0, 60000, 20.0)], ids=["gaussian", "density7"])
+def test_fp32_dense_cells_match_oracle(gpu, system_type, n, L):
+    # cells whose forward neighbourhood exceeds the pair kernel's staging
+    # arrays (the centre of a Gaussian system with sigma L/6, 13.7 times the
+    # mean density; a uniform system at density 7.5): the half-cell groups
+    # stream their candidates through shared memory in chunks.  Closer pairs
+    # than at density 1 raise the FP32 rounding of the closest ones.
+    x, y, z, q = p3mg.generate_system(system_type, n, L, seed=91)
+    fr_ref, e_ref = O.realspace(x, y, z, q, L, RCUT, ALPHA, cells=True)
+    for prec, tol in ((p3mg.FP64, TOL_FP64), (p3mg.FP32_MIXED, 5e-5)):
+        with p3mg.Context(1, 32, CAO, MC, prec) as ctx:
+            ctx.set_system(x, y, z, q, L)
+            fr, e = ctx.real_forces(RCUT, ALPHA)
+        assert O.rel_rms(fr, fr_ref) <= tol
+        assert abs(e - e_ref) <= (TOL_FP64 if prec == p3mg.FP64 else TOL_FP32_E) * abs(e_ref)
