@@ -41,47 +41,6 @@ namespace {
 
 constexpr int ADJ_THREADS = 256;
 
-template <typename real>
-__device__ __forceinline__ void add_real(typename cplx<real>::type *p, int ii, real v) {
-  atomicAdd(ii ? &p->y : &p->x, v);
-}
-
-// Charge assignment with exact weights: one thread per particle, global atomics.
-template <typename real, int CAO, int NMESH>
-__global__ void __launch_bounds__(ADJ_THREADS) adj_scatter_kernel(const double *__restrict__ x,
-                                                                   const double *__restrict__ y,
-                                                                   const double *__restrict__ z,
-                                                                   const double *__restrict__ q, int n, double Hi,
-                                                                   double shift, int m,
-                                                                   typename cplx<real>::type *__restrict__ Q) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double xs[3] = {x[i], y[i], z[i]};
-  const real qi = (real)q[i];
-#pragma unroll
-  for (int ii = 0; ii < NMESH; ii++) {
-    int base[3];
-    real w[3][CAO];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      double u;
-      mesh_geometry_exact(xs[d], Hi, shift, ii, m, &base[d], &u);
-      bspline_weights_u<real, CAO, false>((real)u, w[d], nullptr);
-    }
-    for (int a = 0; a < CAO; a++) {
-      const int gi = wrap_full(base[0] + a, m);
-      const real wa = qi * w[0][a];
-      for (int b = 0; b < CAO; b++) {
-        const int gj = wrap_full(base[1] + b, m);
-        const real wab = wa * w[1][b];
-        const size_t row = ((size_t)gi * m + gj) * m;
-#pragma unroll
-        for (int cc = 0; cc < CAO; cc++) add_real<real>(&Q[row + wrap_full(base[2] + cc, m)], ii, wab * w[2][cc]);
-      }
-    }
-  }
-}
-
 // sum_k G |P^|^2 and sum_k dG |P^|^2 (P^ the packed transform) into acc[0..1]
 template <typename real>
 __global__ void adj_energy_sums_kernel(const typename cplx<real>::type *__restrict__ P, const double *__restrict__ G,
@@ -125,63 +84,10 @@ __global__ void adj_conv_kernel(const typename cplx<real>::type *__restrict__ P,
   Phi[t] = v;
 }
 
-// dE_k/dx_i and dE_k/dq_i from the potential meshes (exact weights), times ge:
-// gx += ge s q_i (m/L) sum phi dW/du ..., gq += ge s sum phi W, s = 1/(L^3 nmesh).
-template <typename real, int CAO, int NMESH>
-__global__ void __launch_bounds__(ADJ_THREADS) adj_gather_kernel(const double *__restrict__ x,
-                                                                  const double *__restrict__ y,
-                                                                  const double *__restrict__ z,
-                                                                  const double *__restrict__ q, int n, double Hi,
-                                                                  double shift, int m,
-                                                                  const typename cplx<real>::type *__restrict__ Phi,
-                                                                  double s, double ge, double *__restrict__ gx,
-                                                                  double *__restrict__ gq) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double xs[3] = {x[i], y[i], z[i]};
-  real sp = 0, s0 = 0, s1 = 0, s2 = 0;
-#pragma unroll
-  for (int ii = 0; ii < NMESH; ii++) {
-    int base[3];
-    real w[3][CAO], dw[3][CAO];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      double u;
-      mesh_geometry_exact(xs[d], Hi, shift, ii, m, &base[d], &u);
-      bspline_weights_u<real, CAO, true>((real)u, w[d], dw[d]);
-    }
-    for (int a = 0; a < CAO; a++) {
-      const int gi = wrap_full(base[0] + a, m);
-      for (int b = 0; b < CAO; b++) {
-        const int gj = wrap_full(base[1] + b, m);
-        const size_t row = ((size_t)gi * m + gj) * m;
-        real t0 = 0, t1 = 0;  // sum_c phi W_c, sum_c phi dW_c
-#pragma unroll
-        for (int cc = 0; cc < CAO; cc++) {
-          const typename cplx<real>::type v = Phi[row + wrap_full(base[2] + cc, m)];
-          const real ph = ii ? v.y : v.x;
-          t0 += ph * w[2][cc];
-          t1 += ph * dw[2][cc];
-        }
-        sp += w[0][a] * w[1][b] * t0;
-        s0 += dw[0][a] * w[1][b] * t0;
-        s1 += w[0][a] * dw[1][b] * t0;
-        s2 += w[0][a] * w[1][b] * t1;
-      }
-    }
-  }
-  const double gs = ge * s;
-  const double gd = gs * q[i] * Hi;  // d/dx = (m/L) d/du
-  gx[i] += gd * (double)s0;
-  gx[(size_t)n + i] += gd * (double)s1;
-  gx[2 * (size_t)n + i] += gd * (double)s2;
-  gq[i] += gs * (double)sp;
-}
-
 __device__ __forceinline__ double adj_min_image(double d, double L) { return d - L * round(d / L); }
 
-// Real space: one thread per particle over the 27 neighbour cells of the
-// half-cell list (or all particles when nc == 0).  Accumulates
+// Real space with fewer than 3 cells per side: one thread per particle over
+// all particles (the cell-list case runs pairs_cell_kernel's adjoint form).  Accumulates
 // gx += -ge f_i, gq += ge phi_i, and acc[0] += E_r, acc[1] += dE_r/dalpha.
 template <typename real>
 __global__ void __launch_bounds__(ADJ_THREADS) adj_pairs_kernel(const double *__restrict__ x,
@@ -289,41 +195,6 @@ __global__ void adj_self_kernel(const double *__restrict__ q, int n, double c_se
   if (i < n) gq[i] += c_self * q[i] + c_neut;
 }
 
-template <typename real, int CAO, int NMESH>
-void launch_adj_scatter(Ctx *c, typename cplx<real>::type *Q) {
-  const int blocks = (c->n + ADJ_THREADS - 1) / ADJ_THREADS;
-  adj_scatter_kernel<real, CAO, NMESH><<<blocks, ADJ_THREADS, 0, c->stream>>>(
-      c->x, c->y, c->z, c->q, c->n, (double)c->mesh / c->L, (double)((c->cao - 1) / 2), c->mesh, Q);
-}
-
-template <typename real, int CAO, int NMESH>
-void launch_adj_gather(Ctx *c, const typename cplx<real>::type *Phi, double s, double ge, double *gx, double *gq) {
-  const int blocks = (c->n + ADJ_THREADS - 1) / ADJ_THREADS;
-  adj_gather_kernel<real, CAO, NMESH><<<blocks, ADJ_THREADS, 0, c->stream>>>(
-      c->x, c->y, c->z, c->q, c->n, (double)c->mesh / c->L, (double)((c->cao - 1) / 2), c->mesh, Phi, s, ge, gx, gq);
-}
-
-template <typename real, int NMESH>
-void dispatch_adj(Ctx *c, bool gather, typename cplx<real>::type *mesh, double s, double ge, double *gx, double *gq) {
-#define ADJ_CASE(K)                                                          \
-  case K:                                                                    \
-    if (gather)                                                              \
-      launch_adj_gather<real, K, NMESH>(c, mesh, s, ge, gx, gq);             \
-    else                                                                     \
-      launch_adj_scatter<real, K, NMESH>(c, mesh);                           \
-    break;
-  switch (c->cao) {
-    ADJ_CASE(1)
-    ADJ_CASE(2)
-    ADJ_CASE(3)
-    ADJ_CASE(4)
-    ADJ_CASE(5)
-    ADJ_CASE(6)
-    ADJ_CASE(7)
-  }
-#undef ADJ_CASE
-}
-
 // c of the k-space energy: 1 for ad, 1/2 for ik influence functions
 double kspace_factor(const Ctx *c) { return method_ad(c->method) ? 1.0 : 0.5; }
 
@@ -337,17 +208,22 @@ int adjoint_run(Ctx *c, double rcut, double ge, double *gx, double *gq, double *
   C *P = reinterpret_cast<C *>(c->Q);
   C *Phi = reinterpret_cast<C *>(c->adj_phi);
   // mesh part: Q (exact weights) -> P^ -> sums of G |P^|^2 and dG |P^|^2
+  // charge assignment with exact weights through the brick-tiled scatter
+  // of the forces (particles brick-sorted first)
   P3MG_CUDA_TRY(cudaMemsetAsync(P, 0, M * sizeof(C), c->stream));
   if (c->n > 0) {
-    if (nmesh == 2)
-      dispatch_adj<real, 2>(c, false, P, 0, 0, nullptr, nullptr);
-    else
-      dispatch_adj<real, 1>(c, false, P, 0, 0, nullptr, nullptr);
-    c->launches++;
-    P3MG_CUDA_TRY(cudaGetLastError());
+    P3MG_TRY(kspace_prepare(c));
+    P3MG_TRY(adjoint_scatter(c));
   }
   P3MG_TRY(fft3d(c, P, 1, -1));
-  P3MG_TRY(influence_with_derivative(c, c->adj_G, c->adj_dG));
+  // G and dG/dalpha depend only on alpha and L for a context (the mesh,
+  // cao and aliasing range are fixed): computed once per (alpha, L), like
+  // G_opt for the forces
+  if (!(c->adj_key_alpha == c->alpha && c->adj_key_L == c->L)) {
+    P3MG_TRY(influence_with_derivative(c, c->adj_G, c->adj_dG));
+    c->adj_key_alpha = c->alpha;
+    c->adj_key_L = c->L;
+  }
   adj_energy_sums_kernel<real><<<mblocks, ADJ_THREADS, 0, c->stream>>>(P, c->adj_G, c->adj_dG, M, sums);
   adj_conv_kernel<real><<<mblocks, ADJ_THREADS, 0, c->stream>>>(P, c->adj_G, M, Phi);
   c->launches += 2;
@@ -355,22 +231,24 @@ int adjoint_run(Ctx *c, double rcut, double ge, double *gx, double *gq, double *
   P3MG_TRY(fft3d(c, Phi, 1, +1));
   if (c->n > 0) {
     const double s = kspace_factor(c) / (L3 * nmesh);
-    if (nmesh == 2)
-      dispatch_adj<real, 2>(c, true, Phi, s, ge, gx, gq);
-    else
-      dispatch_adj<real, 1>(c, true, Phi, s, ge, gx, gq);
-    c->launches++;
-    P3MG_CUDA_TRY(cudaGetLastError());
+    P3MG_TRY(adjoint_gather(c, Phi, s, ge, gx, gq));
   }
   // real space
   if (rcut > 0.0 && c->n > 0) {
     int nc = 0;
     P3MG_TRY(pairs_bin(c, rcut, &nc));
-    const int blocks = (c->n + ADJ_THREADS - 1) / ADJ_THREADS;
-    adj_pairs_kernel<real><<<blocks, ADJ_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, L, rcut, c->alpha, nc,
-                                                                  c->cell_start, c->cell_idx, ge, gx, gq, sums + 2);
-    c->launches++;
-    P3MG_CUDA_TRY(cudaGetLastError());
+    if (nc >= 3) {
+      // the warp-cooperative cell kernel of the forces, with the potential
+      // and dE_r/dalpha summed beside the force (pairs_cell_kernel, ADJ)
+      P3MG_TRY(pairs_adjoint(c, rcut, nc, ge, gx, gq, sums + 2));
+    } else {
+      const int blocks = (c->n + ADJ_THREADS - 1) / ADJ_THREADS;
+      adj_pairs_kernel<real><<<blocks, ADJ_THREADS, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, L, rcut, c->alpha,
+                                                                    0, c->cell_start, c->cell_idx, ge, gx, gq,
+                                                                    sums + 2);
+      c->launches++;
+      P3MG_CUDA_TRY(cudaGetLastError());
+    }
   }
   // charge sums for the self and neutralising terms
   if (c->n > 0) {

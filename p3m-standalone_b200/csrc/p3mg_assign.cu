@@ -258,4 +258,16 @@ int kspace_batch(Ctx *c, const KspaceBatch &b) {
   return kspace_batch_f32(c, b);
 }
 
+int adjoint_scatter_f32(Ctx *c);
+int adjoint_scatter_f64(Ctx *c);
+int adjoint_gather_f32(Ctx *c, const void *Phi, double s, double ge, double *gx, double *gq);
+int adjoint_gather_f64(Ctx *c, const void *Phi, double s, double ge, double *gx, double *gq);
+
+int adjoint_scatter(Ctx *c) { return c->precision == P3MG_FP64 ? adjoint_scatter_f64(c) : adjoint_scatter_f32(c); }
+
+int adjoint_gather(Ctx *c, const void *Phi, double s, double ge, double *gx, double *gq) {
+  return c->precision == P3MG_FP64 ? adjoint_gather_f64(c, Phi, s, ge, gx, gq)
+                                   : adjoint_gather_f32(c, Phi, s, ge, gx, gq);
+}
+
 }  // namespace p3mg

@@ -46,7 +46,10 @@ __host__ __device__ constexpr size_t scatter_stage_bytes() {
 // resolution is below the FP32 rounding of the contributions for the few
 // hundred particles of a brick at density 1; integer sums also make the
 // tile independent of the order of the atomics.  FP64 accumulates doubles.
-template <typename real, int CAO, int NMESH>
+// EXACT: B-spline weights at the exact in-cell offset instead of the
+// reference's 2^-17 table bins (the energy and its adjoint, which must be
+// smooth in the positions); the stencil base is the same.
+template <typename real, int CAO, int NMESH, bool EXACT = false>
 __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *__restrict__ sxyzq,
                                                                   const int *__restrict__ start, int m, int B, int nb,
                                                                   double Hi, double shift, int SR, int SP,
@@ -108,17 +111,22 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
 #pragma unroll
       for (int ii = 0; ii < NMESH; ii++) {
         int base[3], arg[3];
-        mesh_geometry(r.x, Hi, shift, ii, m, &base[0], &arg[0]);
-        mesh_geometry(r.y, Hi, shift, ii, m, &base[1], &arg[1]);
-        mesh_geometry(r.z, Hi, shift, ii, m, &base[2], &arg[2]);
+        double uu[3];
+        mesh_geometry_u(r.x, Hi, shift, ii, m, &base[0], &arg[0], &uu[0]);
+        mesh_geometry_u(r.y, Hi, shift, ii, m, &base[1], &arg[1], &uu[1]);
+        mesh_geometry_u(r.z, Hi, shift, ii, m, &base[2], &arg[2], &uu[2]);
         int rel0 = base[0] - o0, rel1 = base[1] - o1, rel2 = base[2] - o2;
         rel0 += (rel0 < 0) ? m : 0;
         rel1 += (rel1 < 0) ? m : 0;
         rel2 += (rel2 < 0) ? m : 0;
         real w[3][CAO];
-        bspline_weights<real, CAO, false>(arg[0], w[0], nullptr);
-        bspline_weights<real, CAO, false>(arg[1], w[1], nullptr);
-        bspline_weights<real, CAO, false>(arg[2], w[2], nullptr);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          if (EXACT)
+            bspline_weights_u<real, CAO, false>((real)uu[d], w[d], nullptr);
+          else
+            bspline_weights<real, CAO, false>(arg[d], w[d], nullptr);
+        }
         const int v = t * NMESH + ii;
         real *dst = sw + (size_t)v * 3 * CAO;
 #pragma unroll
@@ -479,6 +487,101 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_lanes_kernel(const doub
   }
 }
 
+// The k-space part of the energy's adjoint from the potential meshes Phi
+// (complex layout, unshifted mesh in the real part, shifted in the
+// imaginary part): per brick-sorted particle, with the weights W and their
+// derivatives dW at the exact in-cell offset,
+//   gx += ge s q_i (m/L) sum Phi dW/du ...,  gq += ge s sum Phi W,
+// s = c / (L^3 nmesh) (c = 1 for the ad, 1/2 for the ik influence
+// functions).  Same loop structure as gather_kernel's ad branch.
+template <typename real, int CAO, int NMESH>
+__global__ void __launch_bounds__(ASSIGN_THREADS) adj_gather_sorted_kernel(const double4 *__restrict__ sxyzq,
+                                                                            const int *__restrict__ sidx, int np,
+                                                                            int m, double Hi, double shift,
+                                                                            const typename cplx<real>::type *__restrict__ Phi,
+                                                                            double s, double ge,
+                                                                            double *__restrict__ gx,
+                                                                            double *__restrict__ gq, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  const double4 r = sxyzq[p];
+  const real *__restrict__ Pr = reinterpret_cast<const real *>(Phi);
+  real sp = 0, s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+  for (int ii = 0; ii < NMESH; ii++) {
+    int base[3], arg[3];
+    double uu[3];
+    mesh_geometry_u(r.x, Hi, shift, ii, m, &base[0], &arg[0], &uu[0]);
+    mesh_geometry_u(r.y, Hi, shift, ii, m, &base[1], &arg[1], &uu[1]);
+    mesh_geometry_u(r.z, Hi, shift, ii, m, &base[2], &arg[2], &uu[2]);
+    real w[3][CAO], dw[3][CAO];
+#pragma unroll
+    for (int d = 0; d < 3; d++) bspline_weights_u<real, CAO, true>((real)uu[d], w[d], dw[d]);
+#pragma unroll
+    for (int a = 0; a < CAO; a++) {
+      int gi = base[0] + a;
+      gi -= (gi >= m) ? m : 0;
+#pragma unroll
+      for (int b = 0; b < CAO; b++) {
+        int gj = base[1] + b;
+        gj -= (gj >= m) ? m : 0;
+        const size_t row = ((size_t)gi * m + gj) * m;
+        real t0 = 0, t1 = 0;  // sum_c phi W_c, sum_c phi dW_c
+#pragma unroll
+        for (int c = 0; c < CAO; c++) {
+          int gk = base[2] + c;
+          gk -= (gk >= m) ? m : 0;
+          const real ph = Pr[2 * (row + gk) + ii];
+          t0 += ph * w[2][c];
+          t1 += ph * dw[2][c];
+        }
+        sp += w[0][a] * w[1][b] * t0;
+        s0 += dw[0][a] * w[1][b] * t0;
+        s1 += w[0][a] * dw[1][b] * t0;
+        s2 += w[0][a] * w[1][b] * t1;
+      }
+    }
+  }
+  const int o = sidx[p];
+  const double gs = ge * s;
+  const double gd = gs * r.w * Hi;  // d/dx = (m/L) d/du
+  gx[o] += gd * (double)s0;
+  gx[(size_t)n + o] += gd * (double)s1;
+  gx[2 * (size_t)n + o] += gd * (double)s2;
+  gq[o] += gs * (double)sp;
+}
+
+template <typename real, int CAO>
+int dispatch_adj_gather(Ctx *c, const void *Phi, double s, double ge, double *gx, double *gq) {
+  typedef typename cplx<real>::type C;
+  const double Hi = (double)c->mesh / c->L;
+  const double shift = (double)((c->cao - 1) / 2);
+  const unsigned blocks = (unsigned)((c->n + ASSIGN_THREADS - 1) / ASSIGN_THREADS);
+  if (method_interlaced(c->method))
+    adj_gather_sorted_kernel<real, CAO, 2><<<blocks, ASSIGN_THREADS, 0, c->stream>>>(
+        c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, reinterpret_cast<const C *>(Phi), s, ge, gx, gq, c->n);
+  else
+    adj_gather_sorted_kernel<real, CAO, 1><<<blocks, ASSIGN_THREADS, 0, c->stream>>>(
+        c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, reinterpret_cast<const C *>(Phi), s, ge, gx, gq, c->n);
+  c->launches++;
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
+template <typename real>
+int adj_gather_any(Ctx *c, const void *Phi, double s, double ge, double *gx, double *gq) {
+  switch (c->cao) {
+    case 1: return dispatch_adj_gather<real, 1>(c, Phi, s, ge, gx, gq);
+    case 2: return dispatch_adj_gather<real, 2>(c, Phi, s, ge, gx, gq);
+    case 3: return dispatch_adj_gather<real, 3>(c, Phi, s, ge, gx, gq);
+    case 4: return dispatch_adj_gather<real, 4>(c, Phi, s, ge, gx, gq);
+    case 5: return dispatch_adj_gather<real, 5>(c, Phi, s, ge, gx, gq);
+    case 6: return dispatch_adj_gather<real, 6>(c, Phi, s, ge, gx, gq);
+    case 7: return dispatch_adj_gather<real, 7>(c, Phi, s, ge, gx, gq);
+  }
+  return P3MG_ERR_CAO;
+}
+
 // ---------------------------------------------------------- self forces
 
 // f_tot,d -= b_d(m') q^2 sin(2 pi (m'.x)/h) for the 27 m' (p3m-ad-self-forces.c:114-139)
@@ -553,9 +656,9 @@ inline int scatter_row_pitch(int cao, int T, int word_bytes) {
   return sr;
 }
 
-template <typename real, int CAO, int NMESH>
+template <typename real, int CAO, int NMESH, bool EXACT = false>
 int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
-  auto kern = scatter_kernel<real, CAO, NMESH>;
+  auto kern = scatter_kernel<real, CAO, NMESH, EXACT>;
   // raise the dynamic shared-memory limit once per instantiation (outside
   // any graph capture: the first step of a shape always runs eagerly)
   static size_t smem_set = 0;
@@ -575,7 +678,7 @@ int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
     P3MG_CUDA_TRY(cudaMalloc(&c->scatter_tab, sizeof(int4) * 32 * NPASS));
     P3MG_CUDA_TRY(cudaMemcpy(c->scatter_tab, host, sizeof(int4) * 32 * NPASS, cudaMemcpyHostToDevice));
   }
-  const bool rl = kspace_real(c);
+  const bool rl = !EXACT && kspace_real(c);  // the adjoint keeps the complex mesh
   kern<<<nbr, ASSIGN_THREADS, smem, c->stream>>>(c->sorted_xyzq, c->brick_start, c->mesh, c->brick, c->nbrick1, Hi,
                                                 shift, SR, SP, reinterpret_cast<const int4 *>(c->scatter_tab),
                                                 reinterpret_cast<real *>(c->Q), rl ? c->mesh + 2 : c->mesh,
@@ -586,14 +689,14 @@ int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
   return P3MG_OK;
 }
 
-template <typename real, int CAO>
+template <typename real, int CAO, bool EXACT = false>
 int dispatch_scatter(Ctx *c) {
   const int nmesh = method_interlaced(c->method) ? 2 : 1;
   const int T = brick_tile(c->brick, CAO, nmesh);
   const int SR = scatter_row_pitch(CAO, T, (int)sizeof(real)), SP = T * SR;
   const size_t tile = (size_t)nmesh * T * SP * sizeof(real);
-  if (nmesh == 2) return launch_scatter<real, CAO, 2>(c, tile + scatter_stage_bytes<real, CAO, 2>(), SR, SP);
-  return launch_scatter<real, CAO, 1>(c, tile + scatter_stage_bytes<real, CAO, 1>(), SR, SP);
+  if (nmesh == 2) return launch_scatter<real, CAO, 2, EXACT>(c, tile + scatter_stage_bytes<real, CAO, 2>(), SR, SP);
+  return launch_scatter<real, CAO, 1, EXACT>(c, tile + scatter_stage_bytes<real, CAO, 1>(), SR, SP);
 }
 
 // Gather launch for na batch entries (grid.y): fields / potential Fv of
@@ -660,16 +763,16 @@ int gather_any(Ctx *c, const void *Fv, double *fk, int na) {
   return P3MG_ERR_CAO;
 }
 
-template <typename real>
+template <typename real, bool EXACT = false>
 int scatter_any(Ctx *c) {
   switch (c->cao) {
-    case 1: return dispatch_scatter<real, 1>(c);
-    case 2: return dispatch_scatter<real, 2>(c);
-    case 3: return dispatch_scatter<real, 3>(c);
-    case 4: return dispatch_scatter<real, 4>(c);
-    case 5: return dispatch_scatter<real, 5>(c);
-    case 6: return dispatch_scatter<real, 6>(c);
-    case 7: return dispatch_scatter<real, 7>(c);
+    case 1: return dispatch_scatter<real, 1, EXACT>(c);
+    case 2: return dispatch_scatter<real, 2, EXACT>(c);
+    case 3: return dispatch_scatter<real, 3, EXACT>(c);
+    case 4: return dispatch_scatter<real, 4, EXACT>(c);
+    case 5: return dispatch_scatter<real, 5, EXACT>(c);
+    case 6: return dispatch_scatter<real, 6, EXACT>(c);
+    case 7: return dispatch_scatter<real, 7, EXACT>(c);
   }
   return P3MG_ERR_CAO;
 }

@@ -150,6 +150,8 @@ struct Ctx {
   // energy / adjoint buffers (allocated on first use): G and dG/dalpha at
   // alpha, the potential mesh, 8 reduction slots, the gradients (3 n + n)
   double *adj_G = nullptr, *adj_dG = nullptr, *adj_sums = nullptr, *adj_grad = nullptr;
+  // alpha and box length adj_G / adj_dG were computed for (-1: none yet)
+  double adj_key_alpha = -1.0, adj_key_L = -1.0;
   void *adj_phi = nullptr;
   int adj_cap = 0;
   size_t sweep_cap = 0;
@@ -227,6 +229,7 @@ double ewald_error(int n, double q2, double L, double rcut, int kmax, double alp
 int pairs_reserve(Ctx *c, double rcut);
 int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr, double *energy);
 int pairs_bin(Ctx *c, double rcut, int *nc_out);
+int pairs_adjoint(Ctx *c, double rcut, int nc, double ge, double *gx, double *gq, double *sums);
 int influence_with_derivative(Ctx *c, double *G_out, double *dG_out);
 int adjoint(Ctx *c, double rcut, double ge, double *gx, double *gq, double energy[5], double *dalpha, double *dL);
 
@@ -247,6 +250,11 @@ struct KspaceBatch {
   bool forward = true;  // run the scatter and forward FFT into Q first
 };
 int kspace_batch(Ctx *c, const KspaceBatch &b);
+// the energy's adjoint on the brick-sorted particles (kspace_prepare first):
+// exact-weight charge assignment into the complex mesh Q, and the gradient
+// gather from the potential meshes Phi (see adj_gather_sorted_kernel)
+int adjoint_scatter(Ctx *c);
+int adjoint_gather(Ctx *c, const void *Phi, double s, double ge, double *gx, double *gq);
 int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, double *S26, double *b81_all);
 int g_to_f32_n(Ctx *c, const double *G, float *G32, size_t count);
 size_t sweep_bytes_per_alpha(const Ctx *c);
@@ -288,6 +296,23 @@ __device__ inline void mesh_geometry(double xc, double Hi, double shift, int ii,
   a = a < 0 ? 0 : (a > P3MG_NINTERP - 1 ? P3MG_NINTERP - 1 : a);
   *base = wrap_full(nmp, m);
   *arg = a;
+}
+
+// mesh_geometry plus the exact in-cell offset u = frac in [0, 1) of the
+// same rounded position (so the stencil base always agrees with the
+// binning's).
+__device__ inline void mesh_geometry_u(double xc, double Hi, double shift, int ii, int m, int *base, int *arg,
+                                       double *u) {
+  double pos = __dadd_rn(__dmul_rn(xc, Hi), -shift);
+  if (ii) pos = __dadd_rn(pos, 0.5);
+  double nf = floor(__dadd_rn(pos, 0.5));
+  int nmp = (int)nf;
+  double frac = __dadd_rn(__dadd_rn(pos, -nf), 0.5);
+  int a = (int)floor(__dmul_rn(frac, (double)P3MG_NINTERP));
+  a = a < 0 ? 0 : (a > P3MG_NINTERP - 1 ? P3MG_NINTERP - 1 : a);
+  *base = wrap_full(nmp, m);
+  *arg = a;
+  *u = frac;
 }
 
 // Cardinal B-spline weights of order CAO at the tabulated offset of bin

@@ -127,15 +127,17 @@ constexpr int PAIR_NSEG = 216;   // 6x6x6 half-cells around the cell
 
 // Newton's third law: FP32 with one alpha per CTA (see pairs_cell_kernel)
 __host__ __device__ constexpr bool pair_n3(bool dbl, int na) { return !dbl && na == 1; }
-__host__ __device__ constexpr int pair_jch(bool dbl, int na) { return pair_n3(dbl, na) ? PAIR_JCH32 : PAIR_JCH; }
+__host__ __device__ constexpr int pair_jch(bool dbl, int na, bool adj = false) {
+  return pair_n3(dbl, na) && !adj ? PAIR_JCH32 : PAIR_JCH;
+}
 __host__ __device__ constexpr int pair_maxi(bool dbl) { return dbl ? PAIR_MAXI : PAIR_MAXI32; }
 
 // staged positions, sorted slots, (Newton-3) partner-force accumulators,
 // the i batch and its forces per alpha of the group, the warp queues
-__host__ __device__ constexpr size_t pair_smem_bytes(bool dbl, int na) {
-  return (size_t)pair_jch(dbl, na) * (sizeof(float4) + sizeof(int) + (pair_n3(dbl, na) ? 3 * sizeof(float) : 0)) +
+__host__ __device__ constexpr size_t pair_smem_bytes(bool dbl, int na, bool adj = false) {
+  return (size_t)pair_jch(dbl, na, adj) * (sizeof(float4) + sizeof(int) + (pair_n3(dbl, na) && !adj ? 3 * sizeof(float) : 0)) +
          (size_t)pair_maxi(dbl) * sizeof(float4) +
-         (size_t)pair_maxi(dbl) * 3 * na * (dbl ? sizeof(double) : sizeof(float)) +
+         (size_t)pair_maxi(dbl) * (adj ? 4 : 3) * na * (dbl ? sizeof(double) : sizeof(float)) +
          (size_t)PAIR_WARPS * PAIR_QCAP * sizeof(unsigned short);
 }
 
@@ -374,15 +376,22 @@ __device__ __noinline__ double dense_cell_pairs(const float4 *__restrict__ pos32
   return (double)e_sum - (double)e_comp;
 }
 
-template <bool DBL, int NA>
+// ADJ (one alpha, no Newton-3): the pair part of the energy's adjoint --
+// fr -= ge f_i (dE_r/dx), pot += ge phi_i (dE_r/dq, phi_i = sum_j q_j
+// erfc(alpha r)/r), energy[0] += E_r and energy[1] += dE_r/dalpha =
+// 1/2 sum q_i q_j (-2/sqrt(pi)) exp(-alpha^2 r^2).
+template <bool DBL, int NA, bool ADJ = false>
 __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__restrict__ posv,
                                                                const int *__restrict__ sidx,
                                                                const int *__restrict__ start, int nc, double L,
                                                                double rcut, double alpha_v,
                                                                const double *__restrict__ alphas, int nalpha,
                                                                double *__restrict__ fr, int n,
-                                                               double *__restrict__ energy) {
+                                                               double *__restrict__ energy,
+                                                               double *__restrict__ pot = nullptr, double ge = 0.0) {
   typedef typename PairAcc<DBL>::type acc_t;
+  static_assert(!ADJ || NA == 1, "the adjoint runs one alpha");
+  constexpr int NC = ADJ ? 4 : 3;  // per-i sums: force (and the potential)
   // alpha batch: grid.y = group of NA alphas (alphas on the device), outputs
   // per alpha k at fr + 3 n k and energy + k; without alphas the scalar alpha_v
   const int a0 = blockIdx.y * NA;
@@ -399,8 +408,8 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   // added atomically.  FP64 keeps every ordered pair (the reference's loop,
   // reproducible bit for bit from run to run), and so does an alpha group,
   // whose per-alpha partner accumulators would not fit.
-  constexpr bool N3 = pair_n3(DBL, NA);
-  constexpr int JCH = pair_jch(DBL, NA);
+  constexpr bool N3 = pair_n3(DBL, NA) && !ADJ;
+  constexpr int JCH = pair_jch(DBL, NA, ADJ);
   extern __shared__ __align__(16) unsigned char pair_smem[];
   float4 *cf = reinterpret_cast<float4 *>(pair_smem);
   int *csrc = reinterpret_cast<int *>(cf + JCH);  // sorted slot of each staged candidate
@@ -408,11 +417,11 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   float4 *spi = reinterpret_cast<float4 *>(N3 ? reinterpret_cast<unsigned char *>(sfj + 3 * JCH)
                                               : reinterpret_cast<unsigned char *>(csrc + JCH));
   constexpr int MAXI = pair_maxi(DBL);
-  acc_t *sfi = reinterpret_cast<acc_t *>(spi + MAXI);  // [MAXI][NA][3]
-  unsigned short *queue = reinterpret_cast<unsigned short *>(sfi + 3 * NA * MAXI);
+  acc_t *sfi = reinterpret_cast<acc_t *>(spi + MAXI);  // [MAXI][NA][NC]
+  unsigned short *queue = reinterpret_cast<unsigned short *>(sfi + NC * NA * MAXI);
   __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
   __shared__ double cell_off[27][3];
-  __shared__ double ered[PAIR_WARPS][NA];
+  __shared__ double ered[PAIR_WARPS][NA + (ADJ ? 1 : 0)];
   __shared__ float qmax_i_w[PAIR_WARPS];                         // FP32: |q| maxima of the i batch
   int *sfji = reinterpret_cast<int *>(sfj);                        // FP32: fixed-point partner forces
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -485,6 +494,9 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
     e_d[a] = 0.0;
     e_sum[a] = e_comp[a] = 0.0f;
   }
+  // ADJ: dE_r/dalpha, FP64 or compensated FP32
+  double de_d = 0.0;
+  float de_sum = 0.0f, de_comp = 0.0f;
 
   double e_dense = 0.0;
   if (N3 && !fits) {
@@ -506,7 +518,7 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         spi[t] = p;
         qmi = fmaxf(qmi, fabsf(p.w));
       }
-      for (int a = 0; a < 3 * NA; a++) sfi[3 * NA * t + a] = (acc_t)0;
+      for (int a = 0; a < NC * NA; a++) sfi[NC * NA * t + a] = (acc_t)0;
     }
     if (N3) {
       qmi = __int_as_float(__reduce_max_sync(0xffffffffu, (unsigned)__float_as_int(qmi)));
@@ -564,9 +576,9 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         for (int v = 1; v < 8; v++)
           if (isorted >= own_start[v]) u = v;
         const int kself = own_seg[u] + (isorted - own_start[u]) - k0;
-        acc_t fx[NA], fy[NA], fz[NA];
+        acc_t fx[NA], fy[NA], fz[NA], ph[NA];
 #pragma unroll
-        for (int a = 0; a < NA; a++) fx[a] = fy[a] = fz[a] = (acc_t)0;
+        for (int a = 0; a < NA; a++) fx[a] = fy[a] = fz[a] = ph[a] = (acc_t)0;
         unsigned head = 0, tail = 0;
         // evaluate `take` queued interactions (one per lane) and pop them
         auto process = [&](int take) {
@@ -585,11 +597,16 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
                   if (a < nag) {
                     const double ar = alpha_g[a] * rr;
                     const double ec = erfc(ar);
-                    const double fak = pid.w * pj.w * (ec / rr + prefd_g[a] * exp(-ar * ar)) / (rr * rr);
+                    const double gd = exp(-ar * ar);
+                    const double fak = pid.w * pj.w * (ec / rr + prefd_g[a] * gd) / (rr * rr);
                     fx[a] += fak * ddx;
                     fy[a] += fak * ddy;
                     fz[a] += fak * ddz;
                     e_d[a] += 0.5 * pid.w * pj.w * ec / rr;
+                    if (ADJ) {
+                      ph[a] += pj.w * ec / rr;
+                      de_d += 0.5 * pid.w * pj.w * (-2.0 / wupi) * gd;
+                    }
                   }
                 }
               }
@@ -633,6 +650,13 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               const float tsum = e_sum[a] + term;
               e_comp[a] = (tsum - e_sum[a]) - term;
               e_sum[a] = tsum;
+              if (ADJ) {
+                ph[a] += pj.w * ec * rinv;
+                const float dterm = -(float)(1.0 / wupi) * qq * gs - de_comp;
+                const float dsum = de_sum + dterm;
+                de_comp = (dsum - de_sum) - dterm;
+                de_sum = dsum;
+              }
               }
             }
           }
@@ -716,12 +740,14 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
             fx[a] += __shfl_xor_sync(0xffffffffu, fx[a], o);
             fy[a] += __shfl_xor_sync(0xffffffffu, fy[a], o);
             fz[a] += __shfl_xor_sync(0xffffffffu, fz[a], o);
+            if (ADJ) ph[a] += __shfl_xor_sync(0xffffffffu, ph[a], o);
           }
           if (lane == 0) {
-            acc_t *si = sfi + 3 * (NA * il + a);
+            acc_t *si = sfi + NC * (NA * il + a);
             si[0] += fx[a];
             si[1] += fy[a];
             si[2] += fz[a];
+            if (ADJ) si[3] += ph[a];
           }
         }
       }
@@ -748,10 +774,16 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         atomicAdd(&fr[o], (double)sfi[3 * t]);
         atomicAdd(&fr[(size_t)n + o], (double)sfi[3 * t + 1]);
         atomicAdd(&fr[2 * (size_t)n + o], (double)sfi[3 * t + 2]);
+      } else if (ADJ) {
+        const acc_t *si = sfi + NC * t;
+        fr[o] -= ge * (double)si[0];
+        fr[(size_t)n + o] -= ge * (double)si[1];
+        fr[2 * (size_t)n + o] -= ge * (double)si[2];
+        pot[o] += ge * (double)si[3];
       } else {
         for (int a = 0; a < nag; a++) {
           double *fa = fr + (size_t)a * 3 * (size_t)n;
-          const acc_t *si = sfi + 3 * (NA * t + a);
+          const acc_t *si = sfi + NC * (NA * t + a);
           fa[o] += (double)si[0];
           fa[(size_t)n + o] += (double)si[1];
           fa[2 * (size_t)n + o] += (double)si[2];
@@ -765,8 +797,13 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
     for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
     if (lane == 0) ered[warp][a] = e_loc;
   }
+  if (ADJ) {
+    double d_loc = DBL ? de_d : ((double)de_sum - (double)de_comp);
+    for (int o = 16; o > 0; o >>= 1) d_loc += __shfl_xor_sync(0xffffffffu, d_loc, o);
+    if (lane == 0) ered[warp][ADJ ? NA : 0] = d_loc;
+  }
   __syncthreads();
-  if (tid < nag) {
+  if (tid < nag + (ADJ ? 1 : 0)) {
     double s = 0.0;
     for (int w = 0; w < PAIR_WARPS; w++) s += ered[w][tid];
     if (s != 0.0) atomicAdd(energy + tid, s);
@@ -790,6 +827,24 @@ int launch_cells_na(const void *pos, const int *sidx, const int *start, int nc, 
   const dim3 grid(nc * nc * nc, groups);
   pairs_cell_kernel<DBL, NA><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr,
                                                          n, energy);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
+// The pair part of the energy's adjoint (pairs_cell_kernel with ADJ):
+// gx -= ge f, gq += ge phi, sums[0] += E_r, sums[1] += dE_r/dalpha.
+template <bool DBL>
+int launch_cells_adj(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
+                     double *gx, double *gq, double ge, int n, double *sums, cudaStream_t s) {
+  static bool attr_set = false;
+  const size_t smem = pair_smem_bytes(DBL, 1, true);
+  if (!attr_set) {
+    P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<DBL, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    attr_set = true;
+  }
+  pairs_cell_kernel<DBL, 1, true><<<nc * nc * nc, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, nullptr, 1,
+                                                                      gx, n, sums, gq, ge);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -930,6 +985,21 @@ int pairs_bin(Ctx *c, double rcut, int *nc_out) {
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   *nc_out = nc;
+  return P3MG_OK;
+}
+
+// The pair part of the energy's adjoint on the context's half-cell list
+// (binned by pairs_bin with cells_per_side >= 3): gx -= ge dE_r/dx... as
+// launch_cells_adj.  Returns P3MG_ERR_STATE when the list is not binned.
+int pairs_adjoint(Ctx *c, double rcut, int nc, double ge, double *gx, double *gq, double *sums) {
+  if (nc < 3) return P3MG_ERR_STATE;
+  if (c->precision == P3MG_FP64)
+    P3MG_TRY(launch_cells_adj<true>(c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut, c->alpha, gx, gq, ge, c->n,
+                                    sums, c->stream));
+  else
+    P3MG_TRY(launch_cells_adj<false>(c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut, c->alpha, gx, gq, ge,
+                                     c->n, sums, c->stream));
+  c->launches++;
   return P3MG_OK;
 }
 
