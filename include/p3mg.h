@@ -222,10 +222,11 @@ int p3mg_backward(p3mg_ctx *ctx, double rcut, double grad_E, double *grad_x, dou
 int p3mg_set_tiles(p3mg_ctx *ctx, int brick, int fft_w);
 
 /* Back-interpolation kernel of the ik methods (0, 1, 6; no counterpart in
- * the reference): 0 (the default) puts one lane on each z offset of a
- * particle's stencil (8 or 16 lanes per particle, each lane reading a
- * column of consecutive mesh points), 1 runs one thread per particle.
- * Results differ only by the rounding of the floating-point sums. */
+ * the reference): 0 puts one lane on each z offset of a particle's stencil
+ * (8 or 16 lanes per particle, each lane reading a column of consecutive
+ * mesh points), 1 runs one thread per particle.  The default is 0 for
+ * P3MG_FP64 and 1 for P3MG_FP32_MIXED (the faster of the two for each on a
+ * B200).  Results differ only by the rounding of the floating-point sums. */
 int p3mg_set_gather(p3mg_ctx *ctx, int mode);
 
 /* Tile autotuner (no counterpart in the reference): times the context's

@@ -315,6 +315,10 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
   c->cao = cao;
   c->mc = mc;
   c->precision = precision;
+  // ik gather: lanes on the stencil's z offsets for the 32-byte FP64 field
+  // vectors, one thread per particle for the 16-byte FP32 ones (each the
+  // faster at the 1M-particle headline on a B200)
+  c->gather_mode = (precision == P3MG_FP64) ? 0 : 1;
   c->M = (size_t)mesh * mesh * mesh;
   int st = P3MG_OK;
   do {

@@ -86,7 +86,7 @@ struct Ctx {
   // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
   int brick = 8;
   int fft_w = 0;    // FFT: 0 automatic (pencil kernels where they apply), 4/8/16 Stockham tile width
-  int gather_mode = 0;  // ik gather: 0 lanes on the stencil's z offsets, 1 one thread per particle
+  int gather_mode = 0;  // ik gather: 0 lanes on the stencil's z offsets, 1 one thread per particle (set by p3mg_create)
   int nbrick1 = 0;  // bricks per dimension
   // particle counts / starts per sort key: brick, then mesh point in the
   // brick (B^3 keys per brick); the range of brick b is
