@@ -211,6 +211,15 @@ int p3mg_energy(p3mg_ctx *ctx, double rcut, double parts[5]);
 int p3mg_backward(p3mg_ctx *ctx, double rcut, double grad_E, double *grad_x, double *grad_y, double *grad_z,
                   double *grad_q, double *grad_alpha, double *grad_L, double parts[5]);
 
+/* The same adjoint with the gradients left in device memory (no
+ * counterpart in the reference): *grad_xyz receives a device pointer to
+ * grad_E dE/dx (3n doubles: x block, y block, z block) and *grad_q one to
+ * grad_E dE/dq (n doubles), both valid until the next backward call, the
+ * next p3mg_set_system or p3mg_destroy (either may be NULL).  The scalars
+ * are returned as by p3mg_backward; the call returns once they are known. */
+int p3mg_backward_device(p3mg_ctx *ctx, double rcut, double grad_E, const double **grad_xyz, const double **grad_q,
+                         double *grad_alpha, double *grad_L, double parts[5]);
+
 /* Tile shapes (no counterpart in the reference): brick edge of the
  * charge-assignment tiles (4 or 8 mesh points; the default is 8 for meshes
  * of 64 and more, else 4) and the FFT kernel: 0 (the default) for the

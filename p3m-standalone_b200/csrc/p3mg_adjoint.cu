@@ -188,11 +188,12 @@ __global__ void charge_sums_kernel(const double *__restrict__ q, int n, double *
   }
 }
 
-// self and neutralising terms of dE/dq: ge (-2 alpha/sqrt(pi) q_i - pi Q/(alpha^2 L^3))
-__global__ void adj_self_kernel(const double *__restrict__ q, int n, double c_self, double c_neut,
-                                double *__restrict__ gq) {
+// self and neutralising terms of dE/dq: ge (-2 alpha/sqrt(pi) q_i - pi Q/(alpha^2 L^3)),
+// Q = sum q read from the device sums (sums[4]) so the host need not wait for it
+__global__ void adj_self_kernel(const double *__restrict__ q, int n, double c_self, double c_neut_per_Q,
+                                const double *__restrict__ sums, double *__restrict__ gq) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) gq[i] += c_self * q[i] + c_neut;
+  if (i < n) gq[i] += c_self * q[i] + c_neut_per_Q * sums[4];
 }
 
 // c of the k-space energy: 1 for ad, 1/2 for ik influence functions
@@ -277,12 +278,22 @@ int adjoint(Ctx *c, double rcut, double ge, double *gx, double *gq, double energ
     P3MG_TRY(adjoint_run<double>(c, rcut, ge, gx, gq, c->adj_sums));
   else
     P3MG_TRY(adjoint_run<float>(c, rcut, ge, gx, gq, c->adj_sums));
+  const double L = c->L, L3 = L * L * L, a = c->alpha;
+  const double sqrtpi = 1.77245385090551602729816748334;
+  if (gq && c->n > 0 && ge != 0.0) {
+    const double c_self = ge * (-2.0 * a / sqrtpi);
+    const double c_neut = (a > 0.0) ? ge * (-P3MG_PI / (a * a * L3)) : 0.0;
+    adj_self_kernel<<<(c->n + ADJ_THREADS - 1) / ADJ_THREADS, ADJ_THREADS, 0, c->stream>>>(c->q, c->n, c_self, c_neut,
+                                                                                           c->adj_sums, gq);
+    c->launches++;
+    P3MG_CUDA_TRY(cudaGetLastError());
+  }
+  // the energy parts and dE/dalpha, dE/dL need the device sums: one small
+  // copy at the end of the queued work
   double s[8];
   P3MG_CUDA_TRY(cudaMemcpyAsync(s, c->adj_sums, sizeof(s), cudaMemcpyDeviceToHost, c->stream));
   P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  const double L = c->L, L3 = L * L * L, a = c->alpha;
   const int nmesh = method_interlaced(c->method) ? 2 : 1;
-  const double sqrtpi = 1.77245385090551602729816748334;
   const double kf = kspace_factor(c);
   const double Ek = kf * s[0] / (2.0 * L3 * nmesh), dEk = kf * s[1] / (2.0 * L3 * nmesh);
   const double Er = s[2], dEr = s[3];
@@ -299,14 +310,6 @@ int adjoint(Ctx *c, double rcut, double ge, double *gx, double *gq, double energ
   const double dEa = dEk + dEr + dEs + dEn;
   if (dalpha) *dalpha = ge * dEa;
   if (dL) *dL = ge * (a * dEa - E) / L;
-  if (gq && c->n > 0 && ge != 0.0) {
-    const double c_self = ge * (-2.0 * a / sqrtpi);
-    const double c_neut = (a > 0.0) ? ge * (-P3MG_PI * Qn / (a * a * L3)) : 0.0;
-    adj_self_kernel<<<(c->n + ADJ_THREADS - 1) / ADJ_THREADS, ADJ_THREADS, 0, c->stream>>>(c->q, c->n, c_self, c_neut,
-                                                                                           gq);
-    c->launches++;
-    P3MG_CUDA_TRY(cudaGetLastError());
-  }
   return P3MG_OK;
 }
 

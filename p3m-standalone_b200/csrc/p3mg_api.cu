@@ -728,6 +728,35 @@ extern "C" int p3mg_backward(p3mg_ctx *h, double rcut, double grad_E, double *gr
   return P3MG_OK;
 }
 
+extern "C" int p3mg_backward_device(p3mg_ctx *h, double rcut, double grad_E, const double **grad_xyz,
+                                    const double **grad_q, double *grad_alpha, double *grad_L, double parts[5]) {
+  if (!h) return P3MG_ERR_ARG;
+  Ctx *c = &h->c;
+  if (!(c->L > 0.0)) return P3MG_ERR_NOSYS;
+  if (!c->have_G) return P3MG_ERR_STATE;
+  if (!(c->alpha > 0.0) || !(rcut >= 0.0) || !isfinite(grad_E)) return P3MG_ERR_ARG;
+  cudaSetDevice(c->device);
+  const size_t n = (size_t)c->n;
+  if (!c->adj_grad || c->adj_cap < c->n) {
+    if (c->adj_grad) cudaFree(c->adj_grad);
+    c->adj_grad = nullptr;
+    c->adj_cap = 0;
+    P3MG_CUDA_TRY(cudaMalloc(&c->adj_grad, 4 * (n > 0 ? n : 1) * sizeof(double)));
+    c->adj_cap = c->n;
+  }
+  double *gx = c->adj_grad, *gq = c->adj_grad + 3 * n;
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->adj_grad, 0, 4 * n * sizeof(double), c->stream));
+  double e5[5], da = 0.0, dl = 0.0;
+  P3MG_TRY(adjoint(c, rcut, grad_E, gx, gq, e5, &da, &dl));
+  if (parts)
+    for (int k = 0; k < 5; k++) parts[k] = e5[k];
+  if (grad_alpha) *grad_alpha = da;
+  if (grad_L) *grad_L = dl;
+  if (grad_xyz) *grad_xyz = gx;
+  if (grad_q) *grad_q = gq;
+  return P3MG_OK;
+}
+
 extern "C" int p3mg_energy(p3mg_ctx *h, double rcut, double parts[5]) {
   if (!parts) return P3MG_ERR_ARG;
   return p3mg_backward(h, rcut, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, parts);

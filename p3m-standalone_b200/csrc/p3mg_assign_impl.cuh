@@ -412,47 +412,107 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_kernel(const double4 *_
   fk[2 * (size_t)n + o] += (double)acc2;
 }
 
+// Piecewise polynomials of the order-CAO cardinal B-spline: c[k * CAO + i]
+// is the coefficient of u^i of M_CAO on [k, k + 1) in the local variable u
+// = x - k, so the charge-assignment weight of stencil point j at in-cell
+// offset u is w_j(u) = M_CAO(u + CAO - 1 - j) = sum_i c[(CAO-1-j) CAO + i] u^i
+// (the same weights as bspline_weights_u).  From the recursion on the
+// pieces, P_{n,k}(u) = [(k + u) P_{n-1,k}(u) + (n - k - u) P_{n-1,k-1}(u)] / (n - 1),
+// P_{1,0} = 1 (de Boor), evaluated on the host in double.
+template <typename real>
+struct PieceCoef {
+  real c[P3MG_MAX_CAO * P3MG_MAX_CAO];
+};
+
+template <typename real>
+inline PieceCoef<real> bspline_pieces(int cao) {
+  double P[P3MG_MAX_CAO][P3MG_MAX_CAO] = {{0.0}};  // [piece][power] of the current order
+  P[0][0] = 1.0;
+  for (int n = 2; n <= cao; n++) {
+    double Q[P3MG_MAX_CAO][P3MG_MAX_CAO] = {{0.0}};
+    for (int k = 0; k < n; k++) {
+      for (int i = 0; i < n - 1; i++) {
+        if (k <= n - 2) {  // (k + u) P_{n-1,k}
+          Q[k][i] += k * P[k][i];
+          Q[k][i + 1] += P[k][i];
+        }
+        if (k >= 1) {  // (n - k - u) P_{n-1,k-1}
+          Q[k][i] += (n - k) * P[k - 1][i];
+          Q[k][i + 1] -= P[k - 1][i];
+        }
+      }
+      for (int i = 0; i < n; i++) Q[k][i] /= (double)(n - 1);
+    }
+    for (int k = 0; k < P3MG_MAX_CAO; k++)
+      for (int i = 0; i < P3MG_MAX_CAO; i++) P[k][i] = Q[k][i];
+  }
+  PieceCoef<real> out;
+  for (int k = 0; k < P3MG_MAX_CAO * P3MG_MAX_CAO; k++) out.c[k] = (real)0;
+  for (int k = 0; k < cao; k++)
+    for (int i = 0; i < cao; i++) out.c[k * cao + i] = (real)P[k][i];
+  return out;
+}
+
 // ik back-interpolation with the lanes on the z offsets of the stencil:
 // LPP lanes per particle (8 or 16), lane l < NMESH * CAO owns mesh
 // ii = l / CAO and z offset c = l % CAO and sums its CAO x CAO (a, b)
 // column.  For every (a, b) the CAO lanes of one (particle, mesh) read CAO
 // consecutive field vectors, so a load instruction touches a few whole
-// cache lines where one lane per particle (gather_kernel) touches one
-// scattered line per lane; the lane sums are then reduced over the
-// particle's lanes.  Same weights, geometry and prefactors as gather_kernel.
+// cache lines where one thread per particle (gather_kernel) touches one
+// scattered line per lane.  Lane c evaluates only the weights of stencil
+// index c (one polynomial piece, Horner) on the three axes and takes the
+// others from its group's lanes by shuffles; the lane sums are reduced over
+// the particle's lanes at the end.  Same geometry, table bins and
+// prefactors as gather_kernel.
 template <typename real, int CAO, int NMESH>
 __global__ void __launch_bounds__(ASSIGN_THREADS) gather_lanes_kernel(const double4 *__restrict__ sxyzq,
                                                                        const int *__restrict__ sidx, int np, int m,
                                                                        double Hi, double shift, double pref,
                                                                        const void *__restrict__ Fv, size_t M,
-                                                                       double *__restrict__ fk, int n) {
+                                                                       double *__restrict__ fk, int n,
+                                                                       const PieceCoef<real> pcoef) {
   typedef typename cplx<real>::vec4 V;
   constexpr int LPP = (NMESH * CAO <= 8) ? 8 : 16;
   static_assert(NMESH * CAO <= 16, "lanes per particle");
   constexpr int PPW = 32 / LPP;
+  __shared__ real coef[CAO * CAO];
+  if (threadIdx.x < CAO * CAO) coef[threadIdx.x] = pcoef.c[threadIdx.x];
+  __syncthreads();
   const V *__restrict__ P = reinterpret_cast<const V *>(Fv) + (size_t)blockIdx.y * NMESH * M;
   fk += (size_t)blockIdx.y * 3 * (size_t)n;
   const int lane = threadIdx.x & 31;
   const int p = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * PPW + lane / LPP;
   const int l = lane % LPP;
-  real acc0 = 0, acc1 = 0, acc2 = 0;
-  if (p < np && l < NMESH * CAO) {
-    const double4 r = sxyzq[p];
-    const int ii = (NMESH == 2 && l >= CAO) ? 1 : 0;
-    const int c = l - ii * CAO;
-    int base[3], arg[3];
-    mesh_geometry(r.x, Hi, shift, ii, m, &base[0], &arg[0]);
-    mesh_geometry(r.y, Hi, shift, ii, m, &base[1], &arg[1]);
-    mesh_geometry(r.z, Hi, shift, ii, m, &base[2], &arg[2]);
-    real wx[CAO], wy[CAO], wz[CAO];
-    bspline_weights<real, CAO, false>(arg[0], wx, nullptr);
-    bspline_weights<real, CAO, false>(arg[1], wy, nullptr);
-    bspline_weights<real, CAO, false>(arg[2], wz, nullptr);
-    real wzc = wz[0];
+  const bool act = p < np && l < NMESH * CAO;
+  const int lc = act ? l : 0;  // idle lanes mirror lane 0 of their group (their shuffles stay in range)
+  const int ii = (NMESH == 2 && lc >= CAO) ? 1 : 0;
+  const int c = lc - ii * CAO;
+  const int src0 = (lane & ~(LPP - 1)) + ii * CAO;  // lane holding stencil index 0 of this (particle, mesh)
+  const double4 r = sxyzq[p < np ? p : (np > 0 ? np - 1 : 0)];
+  int base[3], arg[3];
+  mesh_geometry(r.x, Hi, shift, ii, m, &base[0], &arg[0]);
+  mesh_geometry(r.y, Hi, shift, ii, m, &base[1], &arg[1]);
+  mesh_geometry(r.z, Hi, shift, ii, m, &base[2], &arg[2]);
+  // this lane's weights: piece CAO-1-c at the three tabulated offsets
+  const real *cp = coef + (CAO - 1 - c) * CAO;
+  real wc[3];
 #pragma unroll
-    for (int k = 1; k < CAO; k++)
-      if (c == k) wzc = wz[k];
-    const real sw = (real)((NMESH == 2) ? 0.5 * pref : pref) * ((real)r.w * wzc);
+  for (int d = 0; d < 3; d++) {
+    const real u = (real)(arg[d] - P3MG_NINTERP / 2) * (real)(1.0 / P3MG_NINTERP) + (real)0.5;
+    real h = cp[CAO - 1];
+#pragma unroll
+    for (int i = CAO - 2; i >= 0; i--) h = h * u + cp[i];
+    wc[d] = h;
+  }
+  real wx[CAO], wy[CAO];
+#pragma unroll
+  for (int a = 0; a < CAO; a++) {
+    wx[a] = __shfl_sync(0xffffffffu, wc[0], src0 + a);
+    wy[a] = __shfl_sync(0xffffffffu, wc[1], src0 + a);
+  }
+  real acc0 = 0, acc1 = 0, acc2 = 0;
+  if (act) {
+    const real sw = (real)((NMESH == 2) ? 0.5 * pref : pref) * ((real)r.w * wc[2]);
     int gk = base[2] + c;
     gk -= (gk >= m) ? m : 0;
     const V *__restrict__ Pm = P + (ii ? M : 0) + gk;
@@ -461,11 +521,12 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) gather_lanes_kernel(const doub
       int gi = base[0] + a;
       gi -= (gi >= m) ? m : 0;
       const real swa = sw * wx[a];
+      const V *__restrict__ Pa = Pm + (size_t)gi * m * m;
 #pragma unroll
       for (int b = 0; b < CAO; b++) {
         int gj = base[1] + b;
         gj -= (gj >= m) ? m : 0;
-        const V f = Pm[((size_t)gi * m + gj) * m];
+        const V f = Pa[(size_t)gj * m];
         const real w = swa * wy[b];
         acc0 -= f.x * w;
         acc1 -= f.y * w;
@@ -727,12 +788,13 @@ int dispatch_gather(Ctx *c, const void *Fv, double *fk, int na) {
     constexpr int LPP2 = (2 * CAO <= 8) ? 8 : 16, LPP1 = (CAO <= 8) ? 8 : 16;
     const size_t lanes = (size_t)c->n * (il ? LPP2 : LPP1);
     const dim3 lgrid((unsigned)((lanes + ASSIGN_THREADS - 1) / ASSIGN_THREADS), na);
+    static const PieceCoef<real> pcoef = bspline_pieces<real>(CAO);
     if (il)
       gather_lanes_kernel<real, CAO, (2 * CAO <= 16) ? 2 : 1><<<lgrid, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Fv, c->M, fk, c->n);
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Fv, c->M, fk, c->n, pcoef);
     else
       gather_lanes_kernel<real, CAO, 1><<<lgrid, ASSIGN_THREADS, 0, c->stream>>>(
-          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Fv, c->M, fk, c->n);
+          c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Fv, c->M, fk, c->n, pcoef);
   } else {
     // prefactor 1 / (2 L^3) (p3m-ik.c:242, p3m-ik-i.c:241, p3m-ik-real.c:144)
     const double pref = 1.0 / (2.0 * L3);

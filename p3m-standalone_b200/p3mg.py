@@ -102,6 +102,8 @@ def load():
     L.p3mg_sweep_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_int), _dp]
     L.p3mg_energy.argtypes = [vp, ctypes.c_double, _dp]
     L.p3mg_backward.argtypes = [vp, ctypes.c_double, ctypes.c_double] + [_dp] * 7
+    L.p3mg_backward_device.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(vp),
+                                       ctypes.POINTER(vp), _dp, _dp, _dp]
     L.p3mg_set_tiles.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.p3mg_set_gather.argtypes = [vp, ctypes.c_int]
     _ip = ctypes.POINTER(ctypes.c_int)
@@ -319,6 +321,16 @@ class Context:
                                        _p(gq), _p(da), _p(dl), _p(e)), "p3mg_backward")
         return dict(energy=dict(zip(("total", "kspace", "realspace", "self", "neutral"), e)), dx=gx, dq=gq,
                     dalpha=float(da[0]), dL=float(dl[0]))
+
+    def backward_device(self, rcut, grad_E=1.0):
+        """p3mg_backward_device: dict energy parts, dalpha, dL and the device
+        pointers (ints) of the gradients dx (3n) and dq (n)."""
+        gx, gq = ctypes.c_void_p(), ctypes.c_void_p()
+        da, dl, e5 = ctypes.c_double(0.0), ctypes.c_double(0.0), np.zeros(5)
+        _check(self._lib.p3mg_backward_device(self._h, float(rcut), float(grad_E), ctypes.byref(gx), ctypes.byref(gq),
+                                              ctypes.byref(da), ctypes.byref(dl), _p(e5)), "p3mg_backward_device")
+        return dict(energy=dict(zip(("total", "kspace", "realspace", "self", "neutral"), e5)), dalpha=da.value,
+                    dL=dl.value, dx_ptr=gx.value, dq_ptr=gq.value)
 
     def set_tiles(self, brick, fft_w=0):
         _check(self._lib.p3mg_set_tiles(self._h, int(brick), int(fft_w)), "p3mg_set_tiles")

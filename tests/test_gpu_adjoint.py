@@ -174,3 +174,30 @@ def test_torch_autograd_wrapper(gpu):
     em = energy_at(2, 64, 5, 1, 1.0, 3.0, *p, q, 46.4)
     assert abs(pos.grad[i, d].item() - 3.0 * (ep - em) / (2 * H)) <= 1e-6 * abs(3.0 * (ep - em) / (2 * H))
     assert qt.grad is not None and Lt.grad is not None and at.grad is not None
+
+
+@pytest.mark.parametrize("precision", [p3mg.FP64, p3mg.FP32_MIXED])
+def test_backward_device_matches_host(gpu, precision):
+    # p3mg_backward_device leaves the gradients on the GPU: the same numbers
+    # as p3mg_backward's host arrays, two calls in a row
+    import ctypes
+    x, y, z, q = p3mg.generate_system(3, 4000, 21.5, seed=17)
+    with p3mg.Context(1, 32, 5, 1, precision) as ctx:
+        ctx.set_system(x, y, z, q, 21.5)
+        ctx.influence(1.0)
+        h = ctx.backward(3.0, grad_E=2.0)
+        for _ in range(2):
+            d = ctx.backward_device(3.0, grad_E=2.0)
+            n = len(x)
+            gx, gq = np.zeros(3 * n), np.zeros(n)
+            cudart = ctypes.CDLL("libcudart.so")
+            cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+            assert cudart.cudaMemcpy(gx.ctypes.data, d["dx_ptr"], gx.nbytes, 2) == 0
+            assert cudart.cudaMemcpy(gq.ctypes.data, d["dq_ptr"], gq.nbytes, 2) == 0
+            # the mesh sums take global atomics across bricks: equal up to
+            # the rounding of their order
+            tol = 1e-12 if precision == p3mg.FP64 else 1e-6
+            assert O.rel_rms(gx.reshape(3, n), h["dx"]) <= tol
+            assert O.rel_rms(gq, h["dq"]) <= tol
+            assert abs(d["dalpha"] - h["dalpha"]) <= tol * abs(h["energy"]["total"])
+            assert abs(d["energy"]["total"] - h["energy"]["total"]) <= tol * abs(h["energy"]["total"])
