@@ -179,6 +179,20 @@ int p3mg_alpha_range(double alphamin, double alphamax, double alphastep, int cap
 int p3mg_sweep(p3mg_ctx *ctx, double rcut, int nalpha, const double *alphas, const double *ref_x,
                const double *ref_y, const double *ref_z, double *rms_out, double *f_out, int max_batch);
 
+/* The tuning grid over (mesh, cao) of the reference's Tune (tuning.c:250-370)
+ * at every alpha: nctx contexts holding the SAME system (particle count,
+ * positions, charges, box, precision; each its own method, mesh and cao,
+ * distinct contexts) each evaluated at the nalpha alphas like p3mg_sweep
+ * with max_batch > 0 (every alpha exact).  The real-space forces depend
+ * on neither mesh nor cao: they are computed once per alpha (on ctxs[0]'s
+ * stream) and shared; the contexts' k-space passes then run concurrently
+ * on their own streams.  rms_out (host, nctx x nalpha, row = context)
+ * receives sqrt(sum |f - ref|^2) / sqrt(n) against the reference forces
+ * ref_x/y/z (host, n each).  No counterpart in the reference, which runs
+ * Calculate_forces point by point. */
+int p3mg_sweep_grid(p3mg_ctx *const *ctxs, int nctx, double rcut, int nalpha, const double *alphas,
+                    const double *ref_x, const double *ref_y, const double *ref_z, double *rms_out);
+
 /* Interpolation nodes the context's last p3mg_sweep used (0: every alpha
  * was evaluated) and, in check (may be NULL), the larger relative RMS
  * difference between interpolated and evaluated forces at its two check

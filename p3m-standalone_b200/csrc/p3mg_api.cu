@@ -687,6 +687,36 @@ extern "C" int p3mg_sweep(p3mg_ctx *h, double rcut, int nalpha, const double *al
   return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref : nullptr, rms_out, f_out, budget, max_batch > 0);
 }
 
+extern "C" int p3mg_sweep_grid(p3mg_ctx *const *hs, int nctx, double rcut, int nalpha, const double *alphas,
+                               const double *ref_x, const double *ref_y, const double *ref_z, double *rms_out) {
+  if (!hs || nctx < 1 || nalpha < 0 || (nalpha > 0 && !alphas) || !ref_x || !ref_y || !ref_z || !rms_out)
+    return P3MG_ERR_ARG;
+  if (!(rcut >= 0.0)) return P3MG_ERR_ARG;
+  for (int k = 0; k < nalpha; k++)
+    if (!isfinite(alphas[k]) || alphas[k] < 0.0) return P3MG_ERR_ARG;
+  std::vector<Ctx *> cs((size_t)nctx);
+  for (int i = 0; i < nctx; i++) {
+    if (!hs[i]) return P3MG_ERR_ARG;
+    cs[i] = &hs[i]->c;
+    if (!(cs[i]->L > 0.0)) return P3MG_ERR_NOSYS;
+    // one system: the shared real-space forces must fit every context
+    if (cs[i]->n != cs[0]->n || cs[i]->L != cs[0]->L || cs[i]->precision != cs[0]->precision ||
+        cs[i]->device != cs[0]->device)
+      return P3MG_ERR_ARG;
+    for (int j = 0; j < i; j++)
+      if (cs[j] == cs[i]) return P3MG_ERR_ARG;
+  }
+  if (nalpha == 0) return P3MG_OK;
+  cudaSetDevice(cs[0]->device);
+  const double *const ref[3] = {ref_x, ref_y, ref_z};
+  size_t free_b = 0, total_b = 0;
+  P3MG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  size_t budget = free_b / 2;
+  const size_t cap = (size_t)32 << 30;
+  if (budget > cap) budget = cap;
+  return sweep_grid_run(cs.data(), nctx, rcut, nalpha, alphas, ref, rms_out, budget);
+}
+
 extern "C" int p3mg_sweep_nodes(p3mg_ctx *h, int *nodes, double *check) {
   if (!h || !nodes) return P3MG_ERR_ARG;
   *nodes = h->c.sweep_nodes;

@@ -152,6 +152,7 @@ struct Ctx {
   double *adj_G = nullptr, *adj_dG = nullptr, *adj_sums = nullptr, *adj_grad = nullptr;
   // alpha and box length adj_G / adj_dG were computed for (-1: none yet)
   double adj_key_alpha = -1.0, adj_key_L = -1.0;
+  double *sweep_rms2 = nullptr;  // the last sweep's squared errors per alpha (device, in its workspace)
   void *adj_phi = nullptr;
   int adj_cap = 0;
   size_t sweep_cap = 0;
@@ -261,6 +262,8 @@ size_t sweep_bytes_per_alpha(const Ctx *c);
 // ref: host reference rows x, y, z (n doubles each), or NULL
 int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *const *ref, double *rms_out,
               double *f_out, size_t budget, bool exact);
+int sweep_grid_run(Ctx *const *cs, int nctx, double rcut, int na, const double *alphas, const double *const *ref,
+                   double *rms_out, size_t budget);
 
 // misc kernels (p3mg_api.cu)
 int zero_forces(Ctx *c);

@@ -272,9 +272,14 @@ namespace {
 // f_dev (device, na 3n doubles, may be NULL) receives the total forces as
 // well.  late_ref (host rows, may be NULL) is uploaded to late_dst once the
 // evaluation is queued, for the caller's use after it.
+// fr_pre (device, na 3n doubles, may be NULL): the real-space forces of
+// every alpha, computed elsewhere (the tuning grid shares them between
+// contexts that hold the same system); then no pairs run here.  async:
+// return once the work is queued, the squared errors left in
+// c->sweep_rms2 (device) for the caller to read after synchronising.
 int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double *const *ref, double *rms_out,
                 double *f_out, size_t budget, double *f_dev, const double *const *late_ref = nullptr,
-                double *late_dst = nullptr) {
+                double *late_dst = nullptr, const double *fr_pre = nullptr, bool async = false) {
   const size_t n3 = 3 * (size_t)c->n;
   const size_t per = sweep_bytes_per_alpha(c);
   int chunk = (int)(budget / per);
@@ -301,7 +306,7 @@ int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double 
     e = cudaMemcpyAsync(w.alphas, alphas, (size_t)na * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(w.rms2, 0, (size_t)na * sizeof(double), c->stream);
     if (e != cudaSuccess) break;
-    if (rcut != 0.0) {
+    if (rcut != 0.0 && !fr_pre) {
       st = pairs_reserve(c, rcut);
       if (st != P3MG_OK) break;
     }
@@ -321,10 +326,12 @@ int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double 
       const size_t fb = (size_t)nch * n3 * sizeof(double);
       e = cudaMemsetAsync(w.f, 0, fb, c->stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(w.fk, 0, fb, c->stream);
-      if (e == cudaSuccess) e = cudaMemsetAsync(w.fr, 0, fb, c->stream);
+      if (e == cudaSuccess && !fr_pre) e = cudaMemsetAsync(w.fr, 0, fb, c->stream);
       if (e == cudaSuccess) e = cudaMemsetAsync(w.energy, 0, (size_t)nch * sizeof(double), c->stream);
       if (e != cudaSuccess) break;
-      if (rcut != 0.0) {
+      if (fr_pre) {
+        w.fr = const_cast<double *>(fr_pre) + (size_t)a0 * n3;  // read only
+      } else if (rcut != 0.0) {
         st = pairs_run(c, rcut, dal, nch, w.fr, w.energy);
         if (st != P3MG_OK) break;
       }
@@ -366,6 +373,8 @@ int sweep_exact(Ctx *c, double rcut, int na, const double *alphas, const double 
       e = upload_ref(c, late_ref, late_dst);
       if (e != cudaSuccess) break;
     }
+    c->sweep_rms2 = w.rms2;
+    if (async) return P3MG_OK;
     if (rms_out && ref) {
       e = cudaMemcpyAsync(rms_out, w.rms2, (size_t)na * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
       if (e != cudaSuccess) break;
@@ -499,6 +508,69 @@ int sweep_run(Ctx *c, double rcut, int na, const double *alphas, const double *c
     }
   }
   return sweep_exact(c, rcut, na, alphas, ref, rms_out, f_out, budget, nullptr);
+}
+
+// The tuning grid: every alpha on every context (same system, different
+// mesh / cao / method).  The real-space forces of all alphas are computed
+// once on cs[0]'s stream; the other contexts wait for them (an event) and
+// run their k-space batches concurrently on their own streams, each with
+// its share of the memory budget; one synchronisation at the end.
+int sweep_grid_run(Ctx *const *cs, int nctx, double rcut, int na, const double *alphas, const double *const *ref,
+                   double *rms_out, size_t budget) {
+  Ctx *c0 = cs[0];
+  const size_t n3 = 3 * (size_t)c0->n;
+  double *shared = nullptr;  // alphas, then na 3n real-space forces and na energies
+  cudaEvent_t ready = nullptr;
+  int st = P3MG_OK;
+  cudaError_t e = cudaSuccess;
+  const size_t bytes = ((size_t)na + (size_t)na * n3 + (size_t)na) * sizeof(double);
+  e = cudaMalloc(&shared, bytes);
+  if (e != cudaSuccess) {
+    record_cuda_error(e);
+    return e == cudaErrorMemoryAllocation ? P3MG_ERR_ALLOC : P3MG_ERR_CUDA;
+  }
+  double *d_al = shared, *fr_all = shared + na, *e_all = fr_all + (size_t)na * n3;
+  do {
+    e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e != cudaSuccess) break;
+    e = cudaMemcpyAsync(d_al, alphas, (size_t)na * sizeof(double), cudaMemcpyHostToDevice, c0->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(fr_all, 0, ((size_t)na * n3 + na) * sizeof(double), c0->stream);
+    if (e != cudaSuccess) break;
+    if (rcut != 0.0 && c0->n > 0) {
+      st = pairs_reserve(c0, rcut);
+      if (st == P3MG_OK) st = pairs_run(c0, rcut, d_al, na, fr_all, e_all);
+      if (st != P3MG_OK) break;
+    }
+    e = cudaEventRecord(ready, c0->stream);
+    if (e != cudaSuccess) break;
+    const size_t share = budget / (size_t)nctx;
+    for (int i = 0; i < nctx && st == P3MG_OK; i++) {
+      e = cudaStreamWaitEvent(cs[i]->stream, ready, 0);
+      if (e != cudaSuccess) break;
+      cs[i]->sweep_nodes = 0;
+      cs[i]->sweep_check = -1.0;
+      st = sweep_exact(cs[i], rcut, na, alphas, ref, nullptr, nullptr, share, nullptr, nullptr, nullptr, fr_all, true);
+    }
+    if (st != P3MG_OK || e != cudaSuccess) break;
+    for (int i = 0; i < nctx; i++) {
+      double *row = rms_out + (size_t)i * na;
+      e = cudaMemcpyAsync(row, cs[i]->sweep_rms2, (size_t)na * sizeof(double), cudaMemcpyDeviceToHost,
+                          cs[i]->stream);
+      if (e != cudaSuccess) break;
+    }
+    if (e != cudaSuccess) break;
+    for (int i = 0; i < nctx && e == cudaSuccess; i++) e = cudaStreamSynchronize(cs[i]->stream);
+    if (e != cudaSuccess) break;
+    for (size_t k = 0; k < (size_t)nctx * na; k++) rms_out[k] = sqrt(rms_out[k]) / sqrt((double)c0->n);
+  } while (0);
+  if (e != cudaSuccess) {
+    record_cuda_error(e);
+    st = P3MG_ERR_CUDA;
+  }
+  for (int i = 0; i < nctx; i++) cudaStreamSynchronize(cs[i]->stream);
+  if (ready) cudaEventDestroy(ready);
+  cudaFree(shared);
+  return st;
 }
 
 }  // namespace p3mg

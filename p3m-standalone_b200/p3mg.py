@@ -100,6 +100,8 @@ def load():
     L.p3mg_alpha_range.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int, _dp]
     L.p3mg_sweep.argtypes = [vp, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
     L.p3mg_sweep_nodes.argtypes = [vp, ctypes.POINTER(ctypes.c_int), _dp]
+    L.p3mg_sweep_grid.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp,
+                                  _dp, _dp]
     L.p3mg_energy.argtypes = [vp, ctypes.c_double, _dp]
     L.p3mg_backward.argtypes = [vp, ctypes.c_double, ctypes.c_double] + [_dp] * 7
     L.p3mg_backward_device.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(vp),
@@ -441,6 +443,19 @@ class Method:
     @staticmethod
     def Kspace_force(ctx, forces):
         ctx.kspace_forces(forces["f_k"], forces["f"])
+
+
+def sweep_grid(contexts, rcut, alphas, ref):
+    """p3mg_sweep_grid: RMS error against ref (3, n) of every context (same
+    system, different mesh / cao / method) at every alpha, real space
+    shared; returns an array (len(contexts), len(alphas))."""
+    alphas = np.ascontiguousarray(alphas, dtype=np.float64)
+    ref = np.ascontiguousarray(ref, dtype=np.float64)
+    hs = (ctypes.c_void_p * len(contexts))(*[c.handle.value for c in contexts])
+    out = np.zeros((len(contexts), len(alphas)))
+    _check(load().p3mg_sweep_grid(hs, len(contexts), float(rcut), len(alphas), _p(alphas), _p(ref[0]), _p(ref[1]),
+                                  _p(ref[2]), _p(out)), "p3mg_sweep_grid")
+    return out
 
 
 def alpha_range(alphamin, alphamax, alphastep):

@@ -154,3 +154,28 @@ def test_wide_alpha_range_is_evaluated_alpha_by_alpha(gpu):
         ctx.set_system(x, y, z, q, 10.0)
         r = ctx.sweep(3.0, p3mg.alpha_range(0.1, 2.5, 0.05))
         assert r["nodes"] == 0
+
+
+@pytest.mark.parametrize("precision,tol", [(p3mg.FP64, 1e-10), (p3mg.FP32_MIXED, 1e-5)])
+def test_sweep_grid_matches_sweeps(gpu, precision, tol):
+    # p3mg_sweep_grid: several (mesh, cao) points of one system, real space
+    # computed once and shared, k-space passes concurrent -- the same RMS
+    # errors per alpha as each context's own exact sweep
+    L = 12.0
+    x, y, z, q = p3mg.generate_system(5, 1500, L, seed=29)
+    al = np.linspace(0.5, 2.0, 12)
+    with p3mg.Context(7, 16, 7, 1) as ec:
+        ec.set_system(x, y, z, q, L)
+        ref = ec.ewald_forces()["f"]
+    pts = [(7, 16, 5), (7, 24, 7), (7, 32, 3), (2, 20, 4)]
+    ctxs = [p3mg.Context(m, mesh, cao, 1, precision) for m, mesh, cao in pts]
+    try:
+        for c in ctxs:
+            c.set_system(x, y, z, q, L)
+        grid = p3mg.sweep_grid(ctxs, 3.0, al, ref)
+        for i, c in enumerate(ctxs):
+            own = c.sweep(3.0, al, ref=ref, max_batch=len(al))["rms"]
+            assert np.max(np.abs(grid[i] - own) / own) <= tol
+    finally:
+        for c in ctxs:
+            c.close()
