@@ -115,6 +115,8 @@ int free_all(Ctx *c) {
   dfree(c->cell_key);
   dfree(c->cell_idx);
   dfree(c->cell_pos);
+  dfree(c->pair_units);
+  c->pair_units_cap = 0;
   dfree(c->Q);
   dfree(c->F);
   dfree(c->P);

@@ -103,6 +103,8 @@ struct Ctx {
   int *cell_key = nullptr;
   int *cell_idx = nullptr;
   void *cell_pos = nullptr;  // double4 (FP64) or float4 (FP32: position relative to the cell origin, q)
+  void *pair_units = nullptr;  // FP32 dense-cell work units (int2) + 2 counters
+  size_t pair_units_cap = 0;
 
   // mesh data (real type = double for FP64, float for FP32_MIXED)
   size_t M = 0;               // mesh^3

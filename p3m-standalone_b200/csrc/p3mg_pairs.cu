@@ -174,16 +174,18 @@ struct PairAcc<true> {
 // goes straight to the global FP64 force (a slot takes at most that many
 // contributions between flushes, so no accumulator passes 2^30).  Pair
 // order: a pair belongs to the particle first in (J0, J1, J2, sorted slot)
-// order, as in pairs_cell_kernel.  Returns this thread's share of the pair
-// energy.
-constexpr int DENSE_ABLK = 128;  // particles of a half-cell staged per block
+// order, as in pairs_cell_kernel.  Half-cells u_first .. u_last - 1 and,
+// with ab_only >= 0, only their block ab_only (one work unit of
+// dense_units_kernel).  Returns this thread's share of the pair energy.
+constexpr int DENSE_ABLK = 64;   // particles of a half-cell staged per block (one work unit)
 constexpr int DENSE_NSEG = 65;   // (column, z) segments of one half-cell's candidates (13 x 5)
 
 __device__ __noinline__ double dense_cell_pairs(const float4 *__restrict__ pos32, const int *__restrict__ sidx,
                                                 const int *seg_src, const int *seg_pre, const double (*cell_off)[3],
                                                 const int *own_start, float4 *cf, int *csrc, int *acc,
                                                 unsigned *queues, double alpha, double rcut, double cs,
-                                                double *__restrict__ fr, int n) {
+                                                double *__restrict__ fr, int n, int u_first = 0, int u_last = 8,
+                                                int ab_only = -1) {
   __shared__ int sa_sg[DENSE_NSEG], sa_cum[DENSE_NSEG + 1], sa_nseg;
   __shared__ unsigned qmax_bits;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -252,7 +254,7 @@ __device__ __noinline__ double dense_cell_pairs(const float4 *__restrict__ pos32
     return v;
   };
 
-  for (int u = 0; u < 8; u++) {
+  for (int u = u_first; u < u_last; u++) {
     const int srcA = own_start[u], nA = own_start[u + 1] - srcA;
     if (nA == 0) continue;
     const int U0 = (u >> 2) & 1, U1 = (u >> 1) & 1, U2 = u & 1;
@@ -290,7 +292,8 @@ __device__ __noinline__ double dense_cell_pairs(const float4 *__restrict__ pos32
     }
     __syncthreads();
     const int nseg = sa_nseg, C = sa_cum[nseg];
-    for (int ab0 = 0; ab0 < nA; ab0 += DENSE_ABLK) {
+    for (int ab0 = ab_only >= 0 ? ab_only * DENSE_ABLK : 0; ab0 < (ab_only >= 0 ? min(nA, (ab_only + 1) * DENSE_ABLK) : nA);
+         ab0 += DENSE_ABLK) {
       const int nab = min(DENSE_ABLK, nA - ab0);
       for (int cc0 = 0; cc0 < C; cc0 += CH) {
         const int ncand = min(CH, C - cc0);
@@ -388,7 +391,9 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
                                                                const double *__restrict__ alphas, int nalpha,
                                                                double *__restrict__ fr, int n,
                                                                double *__restrict__ energy,
-                                                               double *__restrict__ pot = nullptr, double ge = 0.0) {
+                                                               double *__restrict__ pot = nullptr, double ge = 0.0,
+                                                               int2 *__restrict__ units = nullptr,
+                                                               int *__restrict__ unit_count = nullptr) {
   typedef typename PairAcc<DBL>::type acc_t;
   static_assert(!ADJ || NA == 1, "the adjoint runs one alpha");
   constexpr int NC = ADJ ? 4 : 3;  // per-i sums: force (and the potential)
@@ -501,9 +506,23 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   double e_dense = 0.0;
   if (N3 && !fits) {
     // FP32 Newton-3 and the forward neighbourhood does not fit: half-cell
-    // groups with streamed candidates (dense_cell_pairs)
-    e_dense = dense_cell_pairs(pos32, sidx, seg_src, seg_pre, cell_off, own_start, cf, csrc, sfji,
-                               reinterpret_cast<unsigned *>(spi), alpha, rcut, cs, fr, n);
+    // groups with streamed candidates (dense_cell_pairs), either queued as
+    // work units (one per block of DENSE_ABLK particles of an own
+    // half-cell) for dense_units_kernel, which spreads a dense cell over
+    // many CTAs, or, without a unit list, all here
+    if (units) {
+      if (tid < 8) {
+        const int nA = own_start[tid + 1] - own_start[tid];
+        const int nb = (nA + DENSE_ABLK - 1) / DENSE_ABLK;
+        if (nb > 0) {
+          const int base = atomicAdd(unit_count, nb);
+          for (int b = 0; b < nb; b++) units[base + b] = make_int2(cell, (tid << 24) | b);
+        }
+      }
+    } else {
+      e_dense = dense_cell_pairs(pos32, sidx, seg_src, seg_pre, cell_off, own_start, cf, csrc, sfji,
+                                 reinterpret_cast<unsigned *>(spi), alpha, rcut, cs, fr, n);
+    }
   }
   for (int ib = i0; ib < ((N3 && !fits) ? i0 : i1); ib += MAXI) {
     const int ni = min(MAXI, i1 - ib);
@@ -810,6 +829,81 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   }
 }
 
+// Work units of the dense cells (queued by pairs_cell_kernel<false, 1>):
+// a persistent grid takes (cell, own half-cell, block of DENSE_ABLK
+// particles) units from the list through an atomic counter, sets up the
+// cell's staged segments as pairs_cell_kernel does, and runs that unit of
+// dense_cell_pairs.  A cell 13 times denser than the mean (the centre of a
+// Gaussian system) thus spreads over tens of CTAs instead of one.
+__global__ void __launch_bounds__(PAIR_CTA) dense_units_kernel(const float4 *__restrict__ pos32,
+                                                                const int *__restrict__ sidx,
+                                                                const int *__restrict__ start, int nc, double L,
+                                                                double rcut, const double *__restrict__ alphas,
+                                                                double alpha_v, double *__restrict__ fr, int n,
+                                                                double *__restrict__ energy,
+                                                                const int2 *__restrict__ units,
+                                                                const int *__restrict__ unit_count,
+                                                                int *__restrict__ unit_next) {
+  constexpr int JCH = PAIR_JCH32;
+  extern __shared__ __align__(16) unsigned char unit_smem[];
+  float4 *cf = reinterpret_cast<float4 *>(unit_smem);
+  int *csrc = reinterpret_cast<int *>(cf + JCH);
+  int *acc = csrc + JCH;
+  unsigned *queues = reinterpret_cast<unsigned *>(acc + 3 * JCH);
+  __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
+  __shared__ double cell_off[27][3];
+  __shared__ int own_start[9];
+  __shared__ int item_s;
+  __shared__ double ered[PAIR_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double alpha = alphas ? alphas[0] : alpha_v;
+  const double cs = L / nc;
+  const int count = *unit_count;
+  double e_loc = 0.0;
+  for (;;) {
+    __syncthreads();
+    if (tid == 0) item_s = atomicAdd(unit_next, 1);
+    __syncthreads();
+    const int item = item_s;
+    if (item >= count) break;
+    const int2 un = units[item];
+    const int cell = un.x, u = un.y >> 24, ab = un.y & 0xffffff;
+    const int c2 = cell % nc, c1 = (cell / nc) % nc, c0 = cell / (nc * nc);
+    if (tid < 27) {
+      cell_off[tid][0] = (tid / 9 - 1) * cs;
+      cell_off[tid][1] = ((tid / 3) % 3 - 1) * cs;
+      cell_off[tid][2] = (tid % 3 - 1) * cs;
+    }
+    for (int sg = tid; sg < PAIR_NSEG; sg += PAIR_CTA) {
+      const int J0 = sg / 36 - 2, J1 = (sg / 6) % 6 - 2, J2 = sg % 6 - 2;
+      const int d0 = (J0 + 2) / 2 - 1, d1 = (J1 + 2) / 2 - 1, d2 = (J2 + 2) / 2 - 1;
+      const int v0 = (J0 + 2) & 1, v1 = (J1 + 2) & 1, v2 = (J2 + 2) & 1;
+      const int w0 = wrap_full(c0 + d0, nc), w1 = wrap_full(c1 + d1, nc), w2 = wrap_full(c2 + d2, nc);
+      const int key = ((w0 * nc + w1) * nc + w2) * 8 + (v0 << 2) + (v1 << 1) + v2;
+      const bool forward = J0 >= 1 || (J0 == 0 && (J1 >= 1 || (J1 == 0 && J2 >= 0)));
+      seg_src[sg] = start[key];
+      seg_pre[sg + 1] = forward ? start[key + 1] - start[key] : 0;
+    }
+    if (tid < 9) own_start[tid] = start[cell * 8 + tid];
+    __syncthreads();
+    if (tid == 0) {
+      seg_pre[0] = 0;
+      for (int sg = 0; sg < PAIR_NSEG; sg++) seg_pre[sg + 1] += seg_pre[sg];
+    }
+    __syncthreads();
+    e_loc += dense_cell_pairs(pos32, sidx, seg_src, seg_pre, cell_off, own_start, cf, csrc, acc, queues, alpha, rcut,
+                              cs, fr, n, u, u + 1, ab);
+  }
+  for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
+  if (lane == 0) ered[warp] = e_loc;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int w = 0; w < PAIR_WARPS; w++) s += ered[w];
+    if (s != 0.0) atomicAdd(energy, s);
+  }
+}
+
 // Launch the cell kernel (FP64 or FP32 positions, already half-cell sorted).
 // An alpha batch (alphas with nalpha > 1) runs in groups of PAIR_NA32 /
 // PAIR_NA64 alphas per CTA.
@@ -845,6 +939,31 @@ int launch_cells_adj(const void *pos, const int *sidx, const int *start, int nc,
   }
   pairs_cell_kernel<DBL, 1, true><<<nc * nc * nc, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, nullptr, 1,
                                                                       gx, n, sums, gq, ge);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
+// FP32, one alpha, with a work-unit list (units: capacity for every
+// block of DENSE_ABLK particles of every half-cell; counters: 2 ints the
+// caller zeroes before each call): the cell kernel, whose dense cells only
+// queue units, then the persistent unit kernel.
+int launch_cells_units(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
+                       const double *alphas, double *fr, int n, double *energy, int2 *units, int *counters,
+                       cudaStream_t s) {
+  static bool attr_set = false;
+  const size_t smem = pair_smem_bytes(false, 1);
+  if (!attr_set) {
+    P3MG_CUDA_TRY(
+        cudaFuncSetAttribute(pairs_cell_kernel<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    P3MG_CUDA_TRY(cudaFuncSetAttribute(dense_units_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  pairs_cell_kernel<false, 1><<<nc * nc * nc, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, 1, fr,
+                                                                  n, energy, nullptr, 0.0, units, counters);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  // one persistent CTA per SM-slot: 148 SMs x 6 resident CTAs of this size
+  dense_units_kernel<<<148 * 6, PAIR_CTA, smem, s>>>(reinterpret_cast<const float4 *>(pos), sidx, start, nc, L, rcut,
+                                                     alphas, alpha, fr, n, energy, units, counters, counters + 1);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
@@ -940,6 +1059,18 @@ int pairs_reserve(Ctx *c, double rcut) {
   const int nc = cells_per_side(c->L, rcut);
   if (nc < 3) return P3MG_OK;
   const int nkey = 8 * nc * nc * nc;
+  // FP32 dense-cell work units: at most one per started block of
+  // DENSE_ABLK particles of every half-cell, and the two counters
+  if (c->precision != P3MG_FP64) {
+    const size_t need = (size_t)c->cap / DENSE_ABLK + (size_t)nkey + 8;
+    if (need > c->pair_units_cap) {
+      if (c->pair_units) cudaFree(c->pair_units);
+      c->pair_units = nullptr;
+      c->pair_units_cap = 0;
+      P3MG_CUDA_TRY(cudaMalloc(&c->pair_units, sizeof(int2) * need + 2 * sizeof(int)));
+      c->pair_units_cap = need;
+    }
+  }
   if (nkey > c->ncell_cap) {
     if (c->cell_count) cudaFree(c->cell_count);
     if (c->cell_start) cudaFree(c->cell_start);
@@ -1022,9 +1153,18 @@ int pairs_run(Ctx *c, double rcut, const double *alphas, int nalpha, double *fr,
   }
   P3MG_TRY(pairs_bin(c, rcut, &nc));
   mark(c, EV_K0);
-  P3MG_TRY(launch_pairs_cells(c->precision == P3MG_FP64, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut,
-                              0.0, alphas, nalpha, fr, n, energy, c->stream));
-  c->launches++;
+  if (c->precision != P3MG_FP64 && !(alphas != nullptr && nalpha > 1) && c->pair_units) {
+    int2 *units = reinterpret_cast<int2 *>(c->pair_units);
+    int *counters = reinterpret_cast<int *>(units + c->pair_units_cap);
+    P3MG_CUDA_TRY(cudaMemsetAsync(counters, 0, 2 * sizeof(int), c->stream));
+    P3MG_TRY(launch_cells_units(c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut, 0.0, alphas, fr, n, energy,
+                                units, counters, c->stream));
+    c->launches += 2;
+  } else {
+    P3MG_TRY(launch_pairs_cells(c->precision == P3MG_FP64, c->cell_pos, c->cell_idx, c->cell_start, nc, c->L, rcut,
+                                0.0, alphas, nalpha, fr, n, energy, c->stream));
+    c->launches++;
+  }
   mark(c, EV_K1);
   return P3MG_OK;
 }

@@ -156,7 +156,7 @@ def test_wide_alpha_range_is_evaluated_alpha_by_alpha(gpu):
         assert r["nodes"] == 0
 
 
-@pytest.mark.parametrize("precision,tol", [(p3mg.FP64, 1e-10), (p3mg.FP32_MIXED, 1e-5)])
+@pytest.mark.parametrize("precision,tol", [(p3mg.FP64, 1e-12), (p3mg.FP32_MIXED, 1e-6)])
 def test_sweep_grid_matches_sweeps(gpu, precision, tol):
     # p3mg_sweep_grid: several (mesh, cao) points of one system, real space
     # computed once and shared, k-space passes concurrent -- the same RMS
@@ -167,6 +167,7 @@ def test_sweep_grid_matches_sweeps(gpu, precision, tol):
     with p3mg.Context(7, 16, 7, 1) as ec:
         ec.set_system(x, y, z, q, L)
         ref = ec.ewald_forces()["f"]
+    frms = float(np.sqrt(np.sum(ref ** 2) / len(x)))
     pts = [(7, 16, 5), (7, 24, 7), (7, 32, 3), (2, 20, 4)]
     ctxs = [p3mg.Context(m, mesh, cao, 1, precision) for m, mesh, cao in pts]
     try:
@@ -175,7 +176,9 @@ def test_sweep_grid_matches_sweeps(gpu, precision, tol):
         grid = p3mg.sweep_grid(ctxs, 3.0, al, ref)
         for i, c in enumerate(ctxs):
             own = c.sweep(3.0, al, ref=ref, max_batch=len(al))["rms"]
-            assert np.max(np.abs(grid[i] - own) / own) <= tol
+            # the mesh sums take floating-point atomics: runs agree to the
+            # rounding of the forces, tol of the RMS force
+            assert np.max(np.abs(grid[i] - own)) <= tol * frms
     finally:
         for c in ctxs:
             c.close()
