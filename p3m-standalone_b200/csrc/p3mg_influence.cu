@@ -356,9 +356,17 @@ __global__ void self_force_sum_kernel(const double *__restrict__ G, int m, int c
       double T[3][3];
 #pragma unroll
       for (int d = 0; d < 3; d++) {
+        // sinc(x + j) = (-1)^j sin(pi x) / (pi (x + j)), x = k_d / m: one
+        // sine per axis for the five alias offsets j = -2..2
+        const double x = mi * (double)tk[d];
+        const double s0 = sin(P3MG_PI * x);
         double u[5];
 #pragma unroll
-        for (int c = 0; c < 5; c++) u[c] = ipow_d(sinc_pi(mi * (double)(tk[d] + (c - 2) * m)), cao);
+        for (int c = 0; c < 5; c++) {
+          const double dj = x + (double)(c - 2);
+          const double sc = (dj == 0.0) ? 1.0 : ((c & 1) ? -s0 : s0) / (P3MG_PI * dj);
+          u[c] = ipow_d(sc, cao);
+        }
 #pragma unroll
         for (int p = -1; p <= 1; p++) T[d][p + 1] = u[1] * u[1 + p] + u[2] * u[2 + p] + u[3] * u[3 + p];
       }

@@ -859,6 +859,7 @@ __global__ void __launch_bounds__(PAIR_CTA) dense_units_kernel(const float4 *__r
   const double alpha = alphas ? alphas[0] : alpha_v;
   const double cs = L / nc;
   const int count = *unit_count;
+  if (count == 0) return;  // no dense cell: the usual case at uniform density
   double e_loc = 0.0;
   for (;;) {
     __syncthreads();
@@ -961,8 +962,9 @@ int launch_cells_units(const void *pos, const int *sidx, const int *start, int n
   pairs_cell_kernel<false, 1><<<nc * nc * nc, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, 1, fr,
                                                                   n, energy, nullptr, 0.0, units, counters);
   P3MG_CUDA_TRY(cudaGetLastError());
-  // one persistent CTA per SM-slot: 148 SMs x 6 resident CTAs of this size
-  dense_units_kernel<<<148 * 6, PAIR_CTA, smem, s>>>(reinterpret_cast<const float4 *>(pos), sidx, start, nc, L, rcut,
+  // persistent CTAs, four per SM (148 SMs): a dense cell's units spread
+  // over them; without dense cells each returns after one load
+  dense_units_kernel<<<148 * 4, PAIR_CTA, smem, s>>>(reinterpret_cast<const float4 *>(pos), sidx, start, nc, L, rcut,
                                                      alphas, alpha, fr, n, energy, units, counters, counters + 1);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
