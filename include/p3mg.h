@@ -247,9 +247,15 @@ int p3mg_set_tiles(p3mg_ctx *ctx, int brick, int fft_w);
 /* Back-interpolation kernel of the ik methods (0, 1, 6; no counterpart in
  * the reference): 0 puts one lane on each z offset of a particle's stencil
  * (8 or 16 lanes per particle, each lane reading a column of consecutive
- * mesh points), 1 runs one thread per particle.  The default is 0 for
- * P3MG_FP64 and 1 for P3MG_FP32_MIXED (the faster of the two for each on a
- * B200).  Results differ only by the rounding of the floating-point sums. */
+ * mesh points), 1 runs one thread per particle; P3MG_FP32_MIXED only: 2
+ * stages each mesh brick's field tile in shared memory with TMA tensor
+ * copies (plain loads where the tile wraps around the periodic mesh) and
+ * puts a warp's lanes on the (mesh, b, c) columns of one particle at a
+ * time, 3 the same with plain loads only.  The default is 0 for P3MG_FP64
+ * and 2 for P3MG_FP32_MIXED (the fastest for each on a B200; a tile that
+ * does not fit in shared memory runs mode 1).  Modes 2 and 3 return
+ * P3MG_ERR_ARG for P3MG_FP64 contexts.  Results differ only by the
+ * rounding of the floating-point sums. */
 int p3mg_set_gather(p3mg_ctx *ctx, int mode);
 
 /* Tile autotuner (no counterpart in the reference): times the context's

@@ -102,6 +102,7 @@ int free_all(Ctx *c) {
   dfree(c->fk);
   dfree(c->fr);
   dfree(c->energy);
+  dfree(c->dev_status);
   dfree(c->d_alpha);
   dfree(c->brick_count);
   dfree(c->brick_start);
@@ -318,9 +319,10 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
   c->mc = mc;
   c->precision = precision;
   // ik gather: lanes on the stencil's z offsets for the 32-byte FP64 field
-  // vectors, one thread per particle for the 16-byte FP32 ones (each the
-  // faster at the 1M-particle headline on a B200)
-  c->gather_mode = (precision == P3MG_FP64) ? 0 : 1;
+  // vectors, TMA-staged brick tiles in shared memory for the 16-byte FP32
+  // ones (each the fastest at the 1M-particle headline on a B200; a tile
+  // that does not fit falls back to one thread per particle)
+  c->gather_mode = (precision == P3MG_FP64) ? 0 : 2;
   c->M = (size_t)mesh * mesh * mesh;
   int st = P3MG_OK;
   do {
@@ -367,6 +369,7 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     }
     ALLOC(c->self_b, 81 * sizeof(double));
     ALLOC(c->energy, 2 * sizeof(double));
+    ALLOC(c->dev_status, sizeof(int));
     ALLOC(c->d_alpha, 2 * sizeof(double));
     ALLOC(c->brick_count, nbr * sizeof(int));
     ALLOC(c->brick_start, (nbr + 1) * sizeof(int));
@@ -375,6 +378,7 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     st = scan_tmp_reserve(c, nbr);
     if (st != P3MG_OK) break;
     cudaMemset(c->self_b, 0, 81 * sizeof(double));
+    cudaMemset(c->dev_status, 0, sizeof(int));
     memset(c->self_b_host, 0, sizeof(c->self_b_host));
     st = fft_plan_init(c);
     if (st != P3MG_OK) break;
@@ -439,6 +443,18 @@ int p3mg_influence(p3mg_ctx *h, double alpha) {
   if (!isfinite(alpha) || alpha < 0.0) return P3MG_ERR_ARG;
   cudaSetDevice(c->device);
   return influence_compute(c, alpha);
+}
+
+// Device status word of the context's kernels (set when a bounded wait
+// gave up); read after the stream has been synchronised, then cleared.
+static int check_device_status(Ctx *c) {
+  int st = 0;
+  P3MG_CUDA_TRY(cudaMemcpyAsync(&st, c->dev_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (st == 0) return P3MG_OK;
+  P3MG_CUDA_TRY(cudaMemsetAsync(c->dev_status, 0, sizeof(int), c->stream));
+  snprintf(g_last_cuda_error, sizeof(g_last_cuda_error), "a kernel's bounded wait gave up (device status %d)", st);
+  return P3MG_ERR_CUDA;
 }
 
 static int copy_out3(Ctx *c, const double *src, double *hx, double *hy, double *hz, bool accumulate) {
@@ -526,7 +542,7 @@ int p3mg_get_forces(p3mg_ctx *h, double *f_x, double *f_y, double *f_z, double *
   P3MG_TRY(copy_out3(c, c->fk, fk_x, fk_y, fk_z, false));
   P3MG_TRY(copy_out3(c, c->fr, fr_x, fr_y, fr_z, false));
   if (energy) P3MG_CUDA_TRY(cudaMemcpy(energy, c->energy, sizeof(double), cudaMemcpyDeviceToHost));
-  return P3MG_OK;
+  return check_device_status(c);
 }
 
 int p3mg_calculate_forces(p3mg_ctx *h, double rcut, double *f_x, double *f_y, double *f_z, double *fk_x, double *fk_y,
@@ -824,7 +840,8 @@ extern "C" int p3mg_set_tiles(p3mg_ctx *h, int brick, int fft_w) {
 
 extern "C" int p3mg_set_gather(p3mg_ctx *h, int mode) {
   if (!h) return P3MG_ERR_ARG;
-  if (mode != 0 && mode != 1) return P3MG_ERR_ARG;
+  if (mode < 0 || mode > 3) return P3MG_ERR_ARG;
+  if (mode >= 2 && (h->c.precision == P3MG_FP64 || !gather_tile_fits(&h->c))) return P3MG_ERR_ARG;
   drop_graph(&h->c);
   h->c.gather_mode = mode;
   return P3MG_OK;
@@ -871,7 +888,9 @@ extern "C" int p3mg_autotune(p3mg_ctx *h, double rcut, int *brick_out, int *fft_
   int bb = c->brick, bw = c->fft_w, bg = c->gather_mode;
   double best = 1e300;
   int st = P3MG_OK;
-  const int ngm = method_ad(c->method) ? 1 : 2;  // the gather variants apply to ik methods
+  // the gather variants apply to ik methods: lanes on z offsets, thread
+  // per particle and (FP32) the TMA-staged brick tiles
+  const int ngm = method_ad(c->method) ? 1 : (c->precision == P3MG_FP64 ? 2 : 3);
   for (int ig = 0; ig < ngm && st == P3MG_OK; ig++)
     for (int ib = 0; ib < 2 && st == P3MG_OK; ib++)
       for (int iw = 0; iw < 4 && st == P3MG_OK; iw++) {

@@ -781,6 +781,10 @@ int dispatch_gather(Ctx *c, const void *Fv, double *fk, int na) {
     else
       gather_kernel<real, CAO, 1, true><<<grid, ASSIGN_THREADS, 0, c->stream>>>(
           c->sorted_xyzq, c->sorted_idx, c->n, c->mesh, Hi, shift, pref, Leni, Fv, c->M, fk, c->n, RP, ES);
+  } else if (std::is_same<real, float>::value && c->gather_mode >= 2 && gather_tile_fits(c)) {
+    // prefactor 1 / (2 L^3) (p3m-ik.c:242, p3m-ik-i.c:241, p3m-ik-real.c:144);
+    // brick tiles in shared memory
+    P3MG_TRY(gather_tile_f32(c, Fv, fk, na, 1.0 / (2.0 * L3)));
   } else if (c->gather_mode == 0 && (il ? 2 : 1) * CAO <= 16) {
     // prefactor 1 / (2 L^3) (p3m-ik.c:242, p3m-ik-i.c:241, p3m-ik-real.c:144);
     // lanes on the stencil's z offsets

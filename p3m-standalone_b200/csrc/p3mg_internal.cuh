@@ -79,6 +79,9 @@ struct Ctx {
   double *x = nullptr, *y = nullptr, *z = nullptr, *q = nullptr;  // inputs (device)
   double *f = nullptr, *fk = nullptr, *fr = nullptr;              // outputs, 3n each (device)
   double *energy = nullptr;                                        // device: [0] pair energy, [1] compensation
+  // device status word: kernels with bounded waits set bit 0 when a wait
+  // gave up (read and cleared by the host-synchronising entry points)
+  int *dev_status = nullptr;
 
   // scatter lane table (int2 per lane and iteration, built on the first step)
   void *scatter_tab = nullptr;
@@ -86,7 +89,11 @@ struct Ctx {
   // k-space binning by mesh brick (particles sorted by the brick of their stencil base)
   int brick = 8;
   int fft_w = 0;    // FFT: 0 automatic (pencil kernels where they apply), 4/8/16 Stockham tile width
-  int gather_mode = 0;  // ik gather: 0 lanes on the stencil's z offsets, 1 one thread per particle (set by p3mg_create)
+  // ik gather: 0 lanes on the stencil's z offsets, 1 one thread per
+  // particle, 2 FP32 brick tiles in shared memory staged by TMA (plain loads
+  // where a tile wraps around the mesh), 3 the same tiles with plain loads
+  // only (set by p3mg_create)
+  int gather_mode = 0;
   int nbrick1 = 0;  // bricks per dimension
   // particle counts / starts per sort key: brick, then mesh point in the
   // brick (B^3 keys per brick); the range of brick b is
@@ -213,6 +220,11 @@ int error_map(Ctx *c, int mesh, int cao, const double *fk[3], const double *ref[
 
 // influence (p3mg_influence.cu)
 int influence_compute(Ctx *c, double alpha);
+
+// FP32 ik back-interpolation through shared-memory brick tiles
+// (p3mg_gather_tile.cu; gather_mode 2 and 3)
+bool gather_tile_fits(const Ctx *c);
+int gather_tile_f32(Ctx *c, const void *Fv, double *fk, int na, double pref);
 
 // charge assignment / back-interpolation (p3mg_assign.cu)
 int kspace_prepare(Ctx *c);

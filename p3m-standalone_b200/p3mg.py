@@ -338,7 +338,8 @@ class Context:
         _check(self._lib.p3mg_set_tiles(self._h, int(brick), int(fft_w)), "p3mg_set_tiles")
 
     def set_gather(self, mode):
-        """ik back-interpolation kernel: 0 lanes on the stencil's z offsets, 1 one thread per particle."""
+        """ik back-interpolation kernel: 0 lanes on the stencil's z offsets, 1 one thread per particle,
+        2 (FP32) TMA-staged brick tiles in shared memory, 3 (FP32) the same tiles with plain loads."""
         _check(self._lib.p3mg_set_gather(self._h, int(mode)), "p3mg_set_gather")
 
     def autotune(self, rcut):

@@ -147,19 +147,47 @@ def test_fp32_zero_charges_match_oracle(gpu):
 @pytest.mark.parametrize("case", [(1, 128, 30000), (0, 32, 20000), (6, 64, 20000)], ids=_ids)
 @pytest.mark.parametrize("precision", [p3mg.FP64, p3mg.FP32_MIXED])
 def test_gather_variants_match_oracle(gpu, case, precision):
-    # both ik back-interpolation kernels (lanes on the stencil's z offsets,
-    # one thread per particle) against the oracle
+    # every ik back-interpolation kernel (lanes on the stencil's z offsets,
+    # one thread per particle; FP32 also the shared-memory brick tiles,
+    # TMA-staged and plain-loaded) against the oracle
     ref = _oracle(*case)
     method, mesh, n = case
     x, y, z, q, L = _system(n, 1000 + mesh)
     tol = TOL_FP64 if precision == p3mg.FP64 else TOL_FP32_FK
+    modes = (1, 0) if precision == p3mg.FP64 else (1, 0, 2, 3)
     with p3mg.Context(method, mesh, CAO, MC, precision) as ctx:
         ctx.set_system(x, y, z, q, L)
         ctx.influence(ALPHA)
-        for mode in (1, 0):
+        if precision == p3mg.FP64:
+            # the brick-tile kernels are FP32 only
+            with pytest.raises(p3mg.P3MGError):
+                ctx.set_gather(2)
+        for mode in modes:
             ctx.set_gather(mode)
             fk = ctx.calculate_forces(0.0)["f_k"]
-            assert O.rel_rms(fk, ref["f_k"]) <= tol
+            assert O.rel_rms(fk, ref["f_k"]) <= tol, mode
+
+
+@pytest.mark.parametrize("method", [0, 1, 6])
+@pytest.mark.parametrize("cao,mesh,brick", [(3, 32, 4), (5, 32, 8), (7, 16, 4), (4, 20, 8), (7, 36, 8)])
+def test_fp32_tile_gather_shapes(gpu, method, cao, mesh, brick):
+    # the brick-tile gather at other orders, brick edges and meshes that
+    # are not multiples of the brick (tiles wrapping around the periodic
+    # mesh, TMA boxes reaching past its end) against the oracle
+    if method == 6 and mesh % 2:
+        pytest.skip("method 6 needs an even mesh")
+    n = 3000
+    L = float(n) ** (1.0 / 3.0)
+    x, y, z, q = p3mg.generate_system(0, n, L, seed=cao * 100 + mesh)
+    ref = O.forces(method, mesh, cao, MC, ALPHA, 0.0, x, y, z, q, L)
+    with p3mg.Context(method, mesh, cao, MC, p3mg.FP32_MIXED) as ctx:
+        ctx.set_tiles(brick, 0)
+        ctx.set_system(x, y, z, q, L)
+        ctx.influence(ALPHA)
+        for mode in (2, 3):
+            ctx.set_gather(mode)
+            fk = ctx.calculate_forces(0.0)["f_k"]
+            assert O.rel_rms(fk, ref["f_k"]) <= TOL_FP32_FK, mode
 
 
 @pytest.mark.parametrize("system_type,n,L", [(4, 30000, 31.0), (0, 60000, 20.0)], ids=["gaussian", "density7"])
