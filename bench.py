@@ -389,7 +389,8 @@ def run_ours(args, rank, world, local_rank):
             "roofline_hbm": {"kernel": "gather_tile_kernel", "achieved": round(g_achieved, 2), "peak": peak,
                              "unit": "GB/s", "frac": round(g_achieved / peak, 4), "peak_source": peak_kind,
                              "algorithmic_bytes": int(g_bytes), "traffic": profile_traffic("gather_tile_kernel"),
-                             "note": "the gather is bound by L1 throughput (78 % under ncu), not HBM"},
+                             "note": "the tile gather is bound by the shared-memory pipe (LSU wavefronts at 82 % "
+                                     "of peak under ncu), not HBM"},
             "step_roofline": {"algorithmic_bytes": int(algorithmic_bytes(W["method"], n, W["mesh"], 4)),
                               "achieved_gbs": round(algorithmic_bytes(W["method"], n, W["mesh"], 4)
                                                     / (r32["ms"] * 1e-3) / 1e9, 2)},
