@@ -492,16 +492,13 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   const float prune_r2 = (float)(rcut * rcut * (1.0 + 1e-4));
   const float4 *pos32 = reinterpret_cast<const float4 *>(posv);
   const double4 *pos64 = reinterpret_cast<const double4 *>(posv);
+  // pair energy per lane in FP64; FP32 sums each particle's few terms per
+  // lane in FP32 first (about 3 per lane at density 1) and adds them here
   double e_d[NA];
-  float e_sum[NA], e_comp[NA];  // compensated FP32 energy sums (Kahan)
 #pragma unroll
-  for (int a = 0; a < NA; a++) {
-    e_d[a] = 0.0;
-    e_sum[a] = e_comp[a] = 0.0f;
-  }
-  // ADJ: dE_r/dalpha, FP64 or compensated FP32
+  for (int a = 0; a < NA; a++) e_d[a] = 0.0;
+  // ADJ: dE_r/dalpha, likewise
   double de_d = 0.0;
-  float de_sum = 0.0f, de_comp = 0.0f;
 
   double e_dense = 0.0;
   if (N3 && !fits) {
@@ -524,11 +521,22 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
                                  reinterpret_cast<unsigned *>(spi), alpha, rcut, cs, fr, n);
     }
   }
+  // per i of the batch: its half-cell u (bits 0-2) and its own slot in
+  // the flat staged order (bits 3+)
+  __shared__ int sui[MAXI];
   for (int ib = i0; ib < ((N3 && !fits) ? i0 : i1); ib += MAXI) {
     const int ni = min(MAXI, i1 - ib);
     __syncthreads();
     float qmi = 0.0f;
     for (int t = tid; t < ni; t += PAIR_CTA) {
+      {
+        const int isorted = ib + t;
+        int u = 0;
+#pragma unroll
+        for (int v = 1; v < 8; v++)
+          if (isorted >= own_start[v]) u = v;
+        sui[t] = ((own_seg[u] + (isorted - own_start[u])) << 3) | u;
+      }
       if (DBL) {
         const double4 p = pos64[ib + t];
         spi[t] = make_float4((float)(p.x - ox), (float)(p.y - oy), (float)(p.z - oz), (float)p.w);
@@ -572,9 +580,16 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
       }
       __syncthreads();
       // FP32: fixed-point scale of the partner accumulators for this chunk,
-      // divided by |q_j| per partner
-      float fxs = 0.0f, fxs_inv = 0.0f;
+      // divided by |q_j| per partner, and the squared distance from which on
+      // every contribution stays below 2^24 units: |q_i| fxs kf r <= 2^20
+      // (1 / r^2 + pref / r) / fmul, below 2^24 for 1 / r < x = (-pref +
+      // sqrt(pref^2 + 64 fmul)) / 2 (erfc and the Gaussian at most 1); the
+      // closer pairs go to the global FP64 force
+      float fxs = 0.0f, fxs_inv = 0.0f, r2min = 0.0f;
       if (N3) {
+        const float fm = fmaxf(alphaf * alphaf, 1.0f / ((float)rcut * (float)rcut));
+        const float xr = 0.5f * (sqrtf(preff_g[0] * preff_g[0] + 64.0f * fm) - preff_g[0]);
+        r2min = 1.02f / (xr * xr);
         float qi = 0.0f;
 #pragma unroll
         for (int w = 0; w < PAIR_WARPS; w++) qi = fmaxf(qi, qmax_i_w[w]);
@@ -589,15 +604,17 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         double4 pid = make_double4(0.0, 0.0, 0.0, 0.0);
         if (DBL) pid = pos64[ib + il];
         // half-cell u of i and its own staged slot (excluded from its pairs)
-        const int isorted = ib + il;
-        int u = 0;
-#pragma unroll
-        for (int v = 1; v < 8; v++)
-          if (isorted >= own_start[v]) u = v;
-        const int kself = own_seg[u] + (isorted - own_start[u]) - k0;
+        const int uk = sui[il];
+        const int u = uk & 7;
+        const int kself = (uk >> 3) - k0;
         acc_t fx[NA], fy[NA], fz[NA], ph[NA];
+        float e_p[NA];  // FP32: this particle's energy terms of this lane
+        float de_p = 0.0f;
 #pragma unroll
-        for (int a = 0; a < NA; a++) fx[a] = fy[a] = fz[a] = ph[a] = (acc_t)0;
+        for (int a = 0; a < NA; a++) {
+          fx[a] = fy[a] = fz[a] = ph[a] = (acc_t)0;
+          e_p[a] = 0.0f;
+        }
         unsigned head = 0, tail = 0;
         // evaluate `take` queued interactions (one per lane) and pop them
         auto process = [&](int take) {
@@ -654,7 +671,7 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
                 // multiplies by |q_j| = 0)
                 const float sk = -(pif.w * (pj.w != 0.0f ? copysignf(fxs, pj.w) : 0.0f)) * kf;
                 const float sx = sk * ex, sy = sk * ey, sz = sk * ez;
-                if (fmaxf(fabsf(sx), fmaxf(fabsf(sy), fabsf(sz))) < 16777216.0f) {
+                if (rr2 >= r2min) {
                   atomicAdd(&sfji[3 * sl], __float2int_rn(sx));
                   atomicAdd(&sfji[3 * sl + 1], __float2int_rn(sy));
                   atomicAdd(&sfji[3 * sl + 2], __float2int_rn(sz));
@@ -665,16 +682,10 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
                   atomicAdd(&fr[2 * (size_t)n + o], (double)(-fak * ez));
                 }
               }
-              const float term = (N3 ? 1.0f : 0.5f) * qq * ec * rinv - e_comp[a];
-              const float tsum = e_sum[a] + term;
-              e_comp[a] = (tsum - e_sum[a]) - term;
-              e_sum[a] = tsum;
+              e_p[a] = fmaf((N3 ? 1.0f : 0.5f) * qq, ec * rinv, e_p[a]);
               if (ADJ) {
                 ph[a] += pj.w * ec * rinv;
-                const float dterm = -(float)(1.0 / wupi) * qq * gs - de_comp;
-                const float dsum = de_sum + dterm;
-                de_comp = (dsum - de_sum) - dterm;
-                de_sum = dsum;
+                de_p = fmaf(-(float)(1.0 / wupi) * qq, gs, de_p);
               }
               }
             }
@@ -752,6 +763,11 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
           for (int jb = 0; jb < kn; jb += 32) test_push(jb + lane, jb + lane < kn);
         }
         if (tail != head) process((int)(tail - head));
+        if (!DBL) {
+#pragma unroll
+          for (int a = 0; a < NA; a++) e_d[a] += (double)e_p[a];
+          if (ADJ) de_d += (double)de_p;
+        }
 #pragma unroll
         for (int a = 0; a < NA; a++) {
 #pragma unroll
@@ -812,12 +828,12 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
   }
 #pragma unroll
   for (int a = 0; a < NA; a++) {
-    double e_loc = DBL ? e_d[a] : ((double)e_sum[a] - (double)e_comp[a]) + (a == 0 ? e_dense : 0.0);
+    double e_loc = e_d[a] + (a == 0 ? e_dense : 0.0);
     for (int o = 16; o > 0; o >>= 1) e_loc += __shfl_xor_sync(0xffffffffu, e_loc, o);
     if (lane == 0) ered[warp][a] = e_loc;
   }
   if (ADJ) {
-    double d_loc = DBL ? de_d : ((double)de_sum - (double)de_comp);
+    double d_loc = de_d;
     for (int o = 16; o > 0; o >>= 1) d_loc += __shfl_xor_sync(0xffffffffu, d_loc, o);
     if (lane == 0) ered[warp][ADJ ? NA : 0] = d_loc;
   }
