@@ -155,6 +155,35 @@ struct PairAcc<true> {
   typedef double type;
 };
 
+// Exclusive prefix of the PAIR_NSEG half-cell counts held in seg_pre[1..]
+// (seg_pre[sg + 1] = count of segment sg on entry; seg_pre[sg] = the counts
+// before sg on exit), by the whole CTA: two entries per thread, a warp scan
+// of the pair sums, the warps' totals through wsum.  Ends with a barrier.
+__device__ __forceinline__ void scan_segments(int *seg_pre, int *wsum) {
+  static_assert(2 * PAIR_CTA >= PAIR_NSEG, "two segments per thread");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i1 = 2 * tid + 1, i2 = 2 * tid + 2;
+  const int a = i1 <= PAIR_NSEG ? seg_pre[i1] : 0;
+  const int b = i2 <= PAIR_NSEG ? seg_pre[i2] : 0;
+  int v = a + b;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) wsum[warp] = v;
+  __syncthreads();
+  int off = 0;
+#pragma unroll
+  for (int w = 0; w < PAIR_WARPS; w++)
+    if (w < warp) off += wsum[w];
+  const int incl = v + off;  // counts of segments 0 .. i2 - 1
+  if (i1 <= PAIR_NSEG) seg_pre[i1] = incl - b;
+  if (i2 <= PAIR_NSEG) seg_pre[i2] = incl;
+  if (tid == 0) seg_pre[0] = 0;
+  __syncthreads();
+}
+
 // FP32 Newton-3 pairs of a DENSE cell: one whose forward half-cells exceed
 // the staging arrays (the centre of a clustered system, a cell grid capped
 // to fewer, wider cells).  Instead of testing every staged candidate per
@@ -462,11 +491,10 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
     seg_pre[sg + 1] = forward ? start[key + 1] - start[key] : 0;
   }
   __syncthreads();
-  if (tid == 0) {
-    seg_pre[0] = 0;
-    for (int sg = 0; sg < PAIR_NSEG; sg++) seg_pre[sg + 1] += seg_pre[sg];
+  {
+    __shared__ int scan_w[PAIR_WARPS];
+    scan_segments(seg_pre, scan_w);
   }
-  __syncthreads();
   const int total = seg_pre[PAIR_NSEG];
   const bool fits = total <= JCH;
   const int i0 = start[cell * 8], i1 = start[cell * 8 + 8];
@@ -870,6 +898,7 @@ __global__ void __launch_bounds__(PAIR_CTA) dense_units_kernel(const float4 *__r
   __shared__ double cell_off[27][3];
   __shared__ int own_start[9];
   __shared__ int item_s;
+  __shared__ int scan_w[PAIR_WARPS];
   __shared__ double ered[PAIR_WARPS];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const double alpha = alphas ? alphas[0] : alpha_v;
@@ -903,11 +932,7 @@ __global__ void __launch_bounds__(PAIR_CTA) dense_units_kernel(const float4 *__r
     }
     if (tid < 9) own_start[tid] = start[cell * 8 + tid];
     __syncthreads();
-    if (tid == 0) {
-      seg_pre[0] = 0;
-      for (int sg = 0; sg < PAIR_NSEG; sg++) seg_pre[sg + 1] += seg_pre[sg];
-    }
-    __syncthreads();
+    scan_segments(seg_pre, scan_w);
     e_loc += dense_cell_pairs(pos32, sidx, seg_src, seg_pre, cell_off, own_start, cf, csrc, acc, queues, alpha, rcut,
                               cs, fr, n, u, u + 1, ab);
   }
