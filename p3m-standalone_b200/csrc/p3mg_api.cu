@@ -82,10 +82,10 @@ int alloc_system(Ctx *c, int n) {
   P3MG_CUDA_TRY(cudaMalloc(&c->f, 3 * cap * sizeof(double)));
   P3MG_CUDA_TRY(cudaMalloc(&c->fk, 3 * cap * sizeof(double)));
   P3MG_CUDA_TRY(cudaMalloc(&c->fr, 3 * cap * sizeof(double)));
-  P3MG_CUDA_TRY(cudaMalloc(&c->part_key, cap * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->part_key, cap * sizeof(int2)));
   P3MG_CUDA_TRY(cudaMalloc(&c->sorted_idx, cap * sizeof(int)));
   P3MG_CUDA_TRY(cudaMalloc(&c->sorted_xyzq, cap * sizeof(double4)));
-  P3MG_CUDA_TRY(cudaMalloc(&c->cell_key, cap * sizeof(int)));
+  P3MG_CUDA_TRY(cudaMalloc(&c->cell_key, cap * sizeof(int2)));
   P3MG_CUDA_TRY(cudaMalloc(&c->cell_idx, cap * sizeof(int)));
   P3MG_CUDA_TRY(cudaMalloc(&c->cell_pos, cap * sizeof(double4)));
   c->cap = (int)cap;
@@ -106,13 +106,11 @@ int free_all(Ctx *c) {
   dfree(c->d_alpha);
   dfree(c->brick_count);
   dfree(c->brick_start);
-  dfree(c->brick_fill);
   dfree(c->part_key);
   dfree(c->sorted_idx);
   dfree(c->sorted_xyzq);
   dfree(c->cell_count);
   dfree(c->cell_start);
-  dfree(c->cell_fill);
   dfree(c->cell_key);
   dfree(c->cell_idx);
   dfree(c->cell_pos);
@@ -373,7 +371,6 @@ int p3mg_create(p3mg_ctx **out, int method_id, int mesh, int cao, int mc, int pr
     ALLOC(c->d_alpha, 2 * sizeof(double));
     ALLOC(c->brick_count, nbr * sizeof(int));
     ALLOC(c->brick_start, (nbr + 1) * sizeof(int));
-    ALLOC(c->brick_fill, nbr * sizeof(int));
 #undef ALLOC
     st = scan_tmp_reserve(c, nbr);
     if (st != P3MG_OK) break;
@@ -824,11 +821,9 @@ static int set_tiles(Ctx *c, int brick, int fft_w) {
   const size_t nkey = (size_t)c->nbrick1 * c->nbrick1 * c->nbrick1 * brick * brick * brick;
   dfree(c->brick_count);
   dfree(c->brick_start);
-  dfree(c->brick_fill);
   dfree(c->scatter_tab);  // its pitches depend on the tile edge; rebuilt on the next step
   P3MG_CUDA_TRY(cudaMalloc(&c->brick_count, nkey * sizeof(int)));
   P3MG_CUDA_TRY(cudaMalloc(&c->brick_start, (nkey + 1) * sizeof(int)));
-  P3MG_CUDA_TRY(cudaMalloc(&c->brick_fill, nkey * sizeof(int)));
   return scan_tmp_reserve(c, (int)nkey);
 }
 

@@ -42,10 +42,12 @@ namespace {
 
 // Sort key of a particle: its brick (the B^3 mesh points holding the base
 // of its stencil), then the stencil base inside the brick in row-major
-// order, so that consecutive particles share mesh rows.
+// order, so that consecutive particles share mesh rows.  The count's
+// atomic returns the particle's rank among its key's particles, stored
+// beside the key: the placement then needs no second atomic.
 __global__ void bin_bricks_kernel(const double *__restrict__ x, const double *__restrict__ y,
                                   const double *__restrict__ z, int n, double Hi, double shift, int m, int B, int nb,
-                                  int *__restrict__ key, int *__restrict__ count) {
+                                  int2 *__restrict__ key, int *__restrict__ count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int b0, b1, b2, a;
@@ -54,18 +56,17 @@ __global__ void bin_bricks_kernel(const double *__restrict__ x, const double *__
   mesh_geometry(z[i], Hi, shift, 0, m, &b2, &a);
   const int brick = ((b0 / B) * nb + (b1 / B)) * nb + (b2 / B);
   const int k = brick * (B * B * B) + ((b0 % B) * B + (b1 % B)) * B + (b2 % B);
-  key[i] = k;
-  atomicAdd(&count[k], 1);
+  key[i] = make_int2(k, atomicAdd(&count[k], 1));
 }
 
 __global__ void place_bricks_kernel(const double *__restrict__ x, const double *__restrict__ y,
                                     const double *__restrict__ z, const double *__restrict__ q, int n,
-                                    const int *__restrict__ key, const int *__restrict__ start, int *__restrict__ fill,
+                                    const int2 *__restrict__ key, const int *__restrict__ start,
                                     int *__restrict__ sidx, double4 *__restrict__ sxyzq) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int k = key[i];
-  const int slot = start[k] + atomicAdd(&fill[k], 1);
+  const int2 kr = key[i];
+  const int slot = start[kr.x] + kr.y;
   sidx[slot] = i;
   sxyzq[slot] = make_double4(x[i], y[i], z[i], q[i]);
 }
@@ -226,7 +227,6 @@ int kspace_prepare(Ctx *c) {
   const double Hi = (double)c->mesh / c->L;
   const double shift = (double)((c->cao - 1) / 2);
   P3MG_CUDA_TRY(cudaMemsetAsync(c->brick_count, 0, sizeof(int) * nbr, c->stream));
-  P3MG_CUDA_TRY(cudaMemsetAsync(c->brick_fill, 0, sizeof(int) * nbr, c->stream));
   if (c->n > 0) {
     bin_bricks_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->n, Hi, shift, c->mesh, c->brick, nb,
                                                          c->part_key, c->brick_count);
@@ -236,7 +236,7 @@ int kspace_prepare(Ctx *c) {
   P3MG_TRY(exclusive_scan(c, c->brick_count, c->brick_start, nbr));
   if (c->n > 0) {
     place_bricks_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, c->n, c->part_key, c->brick_start,
-                                                           c->brick_fill, c->sorted_idx, c->sorted_xyzq);
+                                                           c->sorted_idx, c->sorted_xyzq);
     c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
   }

@@ -20,9 +20,17 @@ __host__ __device__ inline int brick_tile(int B, int cao, int nmesh) { return B 
 // particles staged per round of the scatter (weights and tile offsets)
 constexpr int SCATTER_CHUNK = 128;
 
+// staged weight record of one (particle, mesh): W_x (charge and, FP32, the
+// tile's fixed-point scale folded in), W_y, W_z, padded to a multiple of 4
+// reals so W_x reads as 16-byte vectors
+template <int CAO>
+__host__ __device__ constexpr int scatter_rec() {
+  return (3 * CAO + 3) & ~3;
+}
+
 template <typename real, int CAO, int NMESH>
 __host__ __device__ constexpr size_t scatter_stage_bytes() {
-  return (size_t)NMESH * SCATTER_CHUNK * (3 * CAO * sizeof(real) + sizeof(int));
+  return (size_t)NMESH * SCATTER_CHUNK * (scatter_rec<CAO>() * sizeof(real) + sizeof(int)) + 16;
 }
 
 // One CTA per mesh brick.  Round by round, SCATTER_CHUNK particles of the
@@ -62,10 +70,12 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int T = brick_tile(B, CAO, NMESH);
   const int T3 = T * SP;  // tile elements: T planes of pitch SP, rows of pitch SR
+  constexpr int REC = scatter_rec<CAO>();
   acc_t *tile0 = reinterpret_cast<acc_t *>(smem_raw);
   acc_t *tile1 = tile0 + T3;
-  real *sw = reinterpret_cast<real *>(tile0 + NMESH * T3);         // [NMESH*CHUNK][3][CAO]
-  int *soff = reinterpret_cast<int *>(sw + NMESH * SCATTER_CHUNK * 3 * CAO);  // tile offset of the stencil origin
+  // [NMESH*CHUNK][REC] weight records, 16-byte aligned
+  real *sw = reinterpret_cast<real *>((reinterpret_cast<uintptr_t>(tile0 + NMESH * T3) + 15) & ~(uintptr_t)15);
+  int *soff = reinterpret_cast<int *>(sw + NMESH * SCATTER_CHUNK * REC);  // tile offset of the stencil origin
   const int bid = blockIdx.x;
   const int p0 = start[bid * B * B * B], p1 = start[(bid + 1) * B * B * B];
   if (p0 == p1) return;
@@ -128,10 +138,11 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
             bspline_weights<real, CAO, false>(arg[d], w[d], nullptr);
         }
         const int v = t * NMESH + ii;
-        real *dst = sw + (size_t)v * 3 * CAO;
+        real *dst = sw + (size_t)v * REC;
 #pragma unroll
         for (int j = 0; j < CAO; j++) {
-          dst[j] = (real)r.w * w[0][j];  // q * W_x, the reference's first product
+          // q * W_x (the reference's first product), times the fixed-point scale
+          dst[j] = FIXED ? ((real)r.w * w[0][j]) * scale : (real)r.w * w[0][j];
           dst[CAO + j] = w[1][j];
           dst[2 * CAO + j] = w[2][j];
         }
@@ -140,12 +151,28 @@ __global__ void __launch_bounds__(ASSIGN_THREADS) scatter_kernel(const double4 *
     }
     __syncthreads();
     for (int v = warp; v < cnt * NMESH; v += nwarp) {
-      const real *wv = sw + (size_t)v * 3 * CAO;
+      const real *wv = sw + (size_t)v * REC;
       acc_t *tile = (NMESH == 2 && (v & 1)) ? tile1 : tile0;
       acc_t *org = tile + soff[v];
-      real wx[CAO];
+      // W_x as 16-byte vectors (the record's first CAO reals, padded)
+      real wx[(CAO + 3) & ~3];
+      if constexpr (FIXED) {
 #pragma unroll
-      for (int a = 0; a < CAO; a++) wx[a] = FIXED ? wv[a] * scale : wv[a];
+        for (int a = 0; a < CAO; a += 4) {
+          const float4 t4 = *reinterpret_cast<const float4 *>(wv + a);
+          wx[a] = t4.x;
+          wx[a + 1] = t4.y;
+          wx[a + 2] = t4.z;
+          wx[a + 3] = t4.w;
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < CAO; a += 2) {
+          const double2 t2 = *reinterpret_cast<const double2 *>(wv + a);
+          wx[a] = t2.x;
+          if (a + 1 < ((CAO + 3) & ~3)) wx[a + 1] = t2.y;
+        }
+      }
 #pragma unroll
       for (int ps = 0; ps < NPASS; ps++) {
         if (lb[ps] >= 0) {

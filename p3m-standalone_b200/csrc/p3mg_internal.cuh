@@ -98,16 +98,16 @@ struct Ctx {
   // particle counts / starts per sort key: brick, then mesh point in the
   // brick (B^3 keys per brick); the range of brick b is
   // brick_start[b B^3] .. brick_start[(b + 1) B^3]
-  int *brick_count = nullptr, *brick_start = nullptr, *brick_fill = nullptr;
-  int *part_key = nullptr;     // sort key per particle (input order)
+  int *brick_count = nullptr, *brick_start = nullptr;
+  int2 *part_key = nullptr;    // sort key per particle (input order) and its rank among that key's particles
   int *sorted_idx = nullptr;   // input index of each sorted particle
   double4 *sorted_xyzq = nullptr;
 
   // pair cell list
   int ncell1 = 0, ncell_cap = 0;
   double cell_rcut = -1.0;
-  int *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
-  int *cell_key = nullptr;
+  int *cell_count = nullptr, *cell_start = nullptr;
+  int2 *cell_key = nullptr;  // half-cell key per particle and its rank in that half-cell
   int *cell_idx = nullptr;
   void *cell_pos = nullptr;  // double4 (FP64) or float4 (FP32: position relative to the cell origin, q)
   void *pair_units = nullptr;  // FP32 dense-cell work units (int2) + 2 counters

@@ -53,9 +53,10 @@ namespace {
 
 constexpr int BRUTE_THREADS = 256;
 
-// half-cell key of a particle: cell-major, then the 2x2x2 sub-cell
+// half-cell key of a particle: cell-major, then the 2x2x2 sub-cell; beside
+// it the particle's rank in its half-cell (the count's atomic returns it)
 __global__ void bin_cells_kernel(const double *__restrict__ x, const double *__restrict__ y,
-                                 const double *__restrict__ z, int n, double L, int nc, int *__restrict__ key,
+                                 const double *__restrict__ z, int n, double L, int nc, int2 *__restrict__ key,
                                  int *__restrict__ count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -64,19 +65,19 @@ __global__ void bin_cells_kernel(const double *__restrict__ x, const double *__r
   const int h1 = wrap_full((int)floor(y[i] * s), 2 * nc);
   const int h2 = wrap_full((int)floor(z[i] * s), 2 * nc);
   const int k = (((h0 >> 1) * nc + (h1 >> 1)) * nc + (h2 >> 1)) * 8 + ((h0 & 1) << 2) + ((h1 & 1) << 1) + (h2 & 1);
-  key[i] = k;
-  atomicAdd(&count[k], 1);
+  key[i] = make_int2(k, atomicAdd(&count[k], 1));
 }
 
 template <typename V>
 __global__ void place_cells_kernel(const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ z, const double *__restrict__ q, int n, double L, int nc,
-                                   const int *__restrict__ key, const int *__restrict__ start, int *__restrict__ fill,
+                                   const int2 *__restrict__ key, const int *__restrict__ start,
                                    int *__restrict__ sidx, V *__restrict__ pos) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int k = key[i];
-  const int slot = start[k] + atomicAdd(&fill[k], 1);
+  const int2 kr = key[i];
+  const int k = kr.x;
+  const int slot = start[k] + kr.y;
   sidx[slot] = i;
   if (sizeof(V) == sizeof(double4)) {
     reinterpret_cast<double4 *>(pos)[slot] = make_double4(x[i], y[i], z[i], q[i]);
@@ -1117,12 +1118,10 @@ int pairs_reserve(Ctx *c, double rcut) {
   if (nkey > c->ncell_cap) {
     if (c->cell_count) cudaFree(c->cell_count);
     if (c->cell_start) cudaFree(c->cell_start);
-    if (c->cell_fill) cudaFree(c->cell_fill);
-    c->cell_count = c->cell_start = c->cell_fill = nullptr;
+    c->cell_count = c->cell_start = nullptr;
     c->ncell_cap = 0;
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_count, sizeof(int) * nkey));
     P3MG_CUDA_TRY(cudaMalloc(&c->cell_start, sizeof(int) * (nkey + 1)));
-    P3MG_CUDA_TRY(cudaMalloc(&c->cell_fill, sizeof(int) * nkey));
     c->ncell_cap = nkey;
     P3MG_TRY(scan_tmp_reserve(c, nkey));
   }
@@ -1143,18 +1142,17 @@ int pairs_bin(Ctx *c, double rcut, int *nc_out) {
   P3MG_TRY(pairs_reserve(c, rcut));
   c->ncell1 = nc;
   P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_count, 0, sizeof(int) * nkey, c->stream));
-  P3MG_CUDA_TRY(cudaMemsetAsync(c->cell_fill, 0, sizeof(int) * nkey, c->stream));
   bin_cells_kernel<<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, n, c->L, nc, c->cell_key, c->cell_count);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   P3MG_TRY(exclusive_scan(c, c->cell_count, c->cell_start, nkey));
   if (c->precision == P3MG_FP64)
     place_cells_kernel<double4><<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, nc, c->cell_key,
-                                                                   c->cell_start, c->cell_fill, c->cell_idx,
+                                                                   c->cell_start, c->cell_idx,
                                                                    reinterpret_cast<double4 *>(c->cell_pos));
   else
     place_cells_kernel<float4><<<blocks, threads, 0, c->stream>>>(c->x, c->y, c->z, c->q, n, c->L, nc, c->cell_key,
-                                                                  c->cell_start, c->cell_fill, c->cell_idx,
+                                                                  c->cell_start, c->cell_idx,
                                                                   reinterpret_cast<float4 *>(c->cell_pos));
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
@@ -1238,9 +1236,8 @@ constexpr size_t NA_PART_INT_BYTES = sizeof(int) * (size_t)P3MG_NOALLOC_MAX_PART
 constexpr size_t na_round(size_t b) { return (b + 255) & ~(size_t)255; }
 constexpr size_t NA_OFF_COUNT = 0;
 constexpr size_t NA_OFF_START = NA_OFF_COUNT + na_round(NA_CELL_BYTES);
-constexpr size_t NA_OFF_FILL = NA_OFF_START + na_round(NA_CELL_BYTES + sizeof(int));
-constexpr size_t NA_OFF_KEY = NA_OFF_FILL + na_round(NA_CELL_BYTES);
-constexpr size_t NA_OFF_IDX = NA_OFF_KEY + na_round(NA_PART_INT_BYTES);
+constexpr size_t NA_OFF_KEY = NA_OFF_START + na_round(NA_CELL_BYTES + sizeof(int));  // (key, rank) per particle
+constexpr size_t NA_OFF_IDX = NA_OFF_KEY + na_round(2 * NA_PART_INT_BYTES);
 constexpr size_t NA_OFF_POS = NA_OFF_IDX + na_round(NA_PART_INT_BYTES);
 constexpr size_t NA_BYTES = NA_OFF_POS + na_round(sizeof(double4) * (size_t)P3MG_NOALLOC_MAX_PARTICLES);
 static_assert(NA_BYTES <= (size_t)P3MG_NOALLOC_SCRATCH_BYTES, "no-alloc scratch layout exceeds its array");
@@ -1303,23 +1300,21 @@ extern "C" int p3mg_real_forces_noalloc(int n, const double *x, const double *y,
   const int ncell = 8 * nc * nc * nc;  // half-cell keys
   int *count = (int *)(base + NA_OFF_COUNT);
   int *start = (int *)(base + NA_OFF_START);
-  int *fill = (int *)(base + NA_OFF_FILL);
-  int *key = (int *)(base + NA_OFF_KEY);
+  int2 *key = (int2 *)(base + NA_OFF_KEY);
   int *idx = (int *)(base + NA_OFF_IDX);
   void *pos = (void *)(base + NA_OFF_POS);
   // the array keeps the previous call's counters: clear them first
   P3MG_CUDA_TRY(cudaMemsetAsync(count, 0, sizeof(int) * ncell, s));
-  P3MG_CUDA_TRY(cudaMemsetAsync(fill, 0, sizeof(int) * ncell, s));
   bin_cells_kernel<<<blocks, threads, 0, s>>>(x, y, z, n, L, nc, key, count);
   P3MG_CUDA_TRY(cudaGetLastError());
   P3MG_TRY(scan_counts(count, start, ncell, s));
   if (precision == P3MG_FP64) {
-    place_cells_kernel<double4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
+    place_cells_kernel<double4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, idx,
                                                            reinterpret_cast<double4 *>(pos));
     P3MG_CUDA_TRY(cudaGetLastError());
     P3MG_TRY(launch_pairs_cells(true, pos, idx, start, nc, L, rcut, alpha, nullptr, 1, fr, n, energy, s));
   } else {
-    place_cells_kernel<float4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, fill, idx,
+    place_cells_kernel<float4><<<blocks, threads, 0, s>>>(x, y, z, q, n, L, nc, key, start, idx,
                                                           reinterpret_cast<float4 *>(pos));
     P3MG_CUDA_TRY(cudaGetLastError());
     P3MG_TRY(launch_pairs_cells(false, pos, idx, start, nc, L, rcut, alpha, nullptr, 1, fr, n, energy, s));
