@@ -136,6 +136,8 @@ int free_all(Ctx *c) {
   dfree(c->adj_grad);
   dfree(c->adj_phi);
   c->adj_cap = 0;
+  dfree(c->infl_tab);
+  c->infl_cap = 0;
   fft_plan_free(c);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   c->gexec = nullptr;

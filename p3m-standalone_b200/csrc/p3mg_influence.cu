@@ -35,6 +35,39 @@ __device__ __forceinline__ double signed_freq(int i, int m) {
   return (double)i - round((double)i / (double)m) * (double)m;
 }
 
+// Per-axis alias factors of G_opt for an alias range mc (the three axes of
+// the cubic box share them).  For mesh index i in [0, m) and alias r in
+// [0, 2 mc + 1) -- the frequency n = n_i + m (r - mc), n_i the signed
+// frequency of i --
+//   A[3 (i NA + r)] = the sinc power ((sinc^cao)^2 or sinc^(2 cao)) at n / m,
+//   A[3 (i NA + r) + 1] = n / L,   A[3 (i NA + r) + 2] = (n / L)^2,
+//   E[(a m + i) NA + r] = exp(-(pi / alpha_a)^2 (n / L)^2) for alpha a of na
+// (alphas on the device, or alpha_v when alphas is null).  The mesh-point
+// kernels read these instead of evaluating 3 NA sines and 3 NA
+// exponentials per point.
+__global__ void influence_axis_kernel(double *__restrict__ A, double *__restrict__ E, int method, int m, int cao,
+                                      int mc, double L, const double *__restrict__ alphas, double alpha_v, int na) {
+  const int NA = 2 * mc + 1;
+  const int nA = m * NA;
+  const bool ik_sq = (method == 0 || method == 6);
+  const double Leni = 1.0 / L, fak1 = 1.0 / (double)m;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nA * (na + 1); t += gridDim.x * blockDim.x) {
+    const int a = t / nA - 1, e = t % nA;  // a = -1: the alpha-independent part
+    const int i = e / NA, r = e % NA;
+    const double n = signed_freq(i, m) + (double)(m * (r - mc));
+    const double nl = n * Leni;
+    if (a < 0) {
+      const double sx = sinc_pi(fak1 * n);
+      A[3 * e] = ik_sq ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
+      A[3 * e + 1] = nl;
+      A[3 * e + 2] = nl * nl;
+    } else {
+      const double pa = P3MG_PI / (alphas ? alphas[a] : alpha_v);
+      E[(size_t)a * nA + e] = exp(-(pa * pa) * (nl * nl));
+    }
+  }
+}
+
 // G_opt at one mesh point (NX, NY, NZ) away from the zeroed ones, and with
 // want_dg dG/dalpha (each exp(-(pi/alpha)^2 |n|^2) factor differentiated; the
 // rest of the formula is linear in those sums).  MC >= 0: the alias range
@@ -44,7 +77,8 @@ __device__ __forceinline__ double signed_freq(int i, int m) {
 // three axis factors).  MC < 0: any mc, evaluated alias by alias.
 template <int MC>
 __device__ __forceinline__ void influence_point(int method, int m, int cao, int mc, double alpha, double L, int NX,
-                                                int NY, int NZ, bool want_dg, double *g_out, double *dg_out) {
+                                                int NY, int NZ, bool want_dg, double *g_out, double *dg_out,
+                                                const double *__restrict__ A, const double *__restrict__ Ea) {
   const int half = m / 2;
   const bool ad = method_ad(method);
   const bool ik_sq = (method == 0 || method == 6);  // (sinc^cao)^2, else sinc^(2 cao)
@@ -57,7 +91,8 @@ __device__ __forceinline__ void influence_point(int method, int m, int cao, int 
   const double dfac = 2.0 * fak2 / alpha;  // d/dalpha of -fak2 NM2 is dfac NM2
   // one alias term: S3 the product of the sinc powers, NM* the shifted
   // frequencies, TE the Gaussian, par the parity of MX + MY + MZ
-  auto term = [&](double S3, double NMX, double NMY, double NMZ, double NM2, double TE, bool even) {
+  // NLX..NLZ: the shifted frequencies over L
+  auto term = [&](double S3, double NLX, double NLY, double NLZ, double NM2, double TE, bool even) {
     const double dTE = want_dg ? TE * NM2 * dfac : 0.0;
     N1 += S3;
     if (ad) {
@@ -68,35 +103,37 @@ __device__ __forceinline__ void influence_point(int method, int m, int cao, int 
       dZ += S3 * dTE;
     } else {
       const double zwi = S3 * TE / NM2;
-      Zx += NMX * zwi * Leni;
-      Zy += NMY * zwi * Leni;
-      Zz += NMZ * zwi * Leni;
+      Zx += NLX * zwi;
+      Zy += NLY * zwi;
+      Zz += NLZ * zwi;
       if (want_dg) {
         const double dzwi = S3 * dTE / NM2;
-        dZx += NMX * dzwi * Leni;
-        dZy += NMY * dzwi * Leni;
-        dZz += NMZ * dzwi * Leni;
+        dZx += NLX * dzwi;
+        dZy += NLY * dzwi;
+        dZz += NLZ * dzwi;
       }
       N2 += even ? S3 : -S3;
     }
   };
   if constexpr (MC >= 0) {
+    // the per-axis factors from influence_axis_kernel's tables
     constexpr int NA = 2 * MC + 1;
-    double Nx[NA], Ny[NA], Nz[NA], Sx[NA], Sy[NA], Sz[NA], Ex[NA], Ey[NA], Ez[NA];
+    double Lx[NA], Ly[NA], Lz[NA], Qx[NA], Qy[NA], Qz[NA], Sx[NA], Sy[NA], Sz[NA], Ex[NA], Ey[NA], Ez[NA];
 #pragma unroll
     for (int i = 0; i < NA; i++) {
-      const double shift = (double)(m * (i - MC));
-      Nx[i] = nx + shift;
-      Ny[i] = ny + shift;
-      Nz[i] = nz + shift;
-      const double sx = sinc_pi(fak1 * Nx[i]), sy = sinc_pi(fak1 * Ny[i]), sz = sinc_pi(fak1 * Nz[i]);
-      Sx[i] = ik_sq ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
-      Sy[i] = ik_sq ? ipow_d(ipow_d(sy, cao), 2) : ipow_d(sy, 2 * cao);
-      Sz[i] = ik_sq ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao);
-      const double a = Nx[i] * Leni, b = Ny[i] * Leni, c = Nz[i] * Leni;
-      Ex[i] = exp(-fak2 * (a * a));
-      Ey[i] = exp(-fak2 * (b * b));
-      Ez[i] = exp(-fak2 * (c * c));
+      const double *ax = A + 3 * (NX * NA + i), *ay = A + 3 * (NY * NA + i), *az = A + 3 * (NZ * NA + i);
+      Sx[i] = ax[0];
+      Lx[i] = ax[1];
+      Qx[i] = ax[2];
+      Sy[i] = ay[0];
+      Ly[i] = ay[1];
+      Qy[i] = ay[2];
+      Sz[i] = az[0];
+      Lz[i] = az[1];
+      Qz[i] = az[2];
+      Ex[i] = Ea[NX * NA + i];
+      Ey[i] = Ea[NY * NA + i];
+      Ez[i] = Ea[NZ * NA + i];
     }
 #pragma unroll
     for (int i = 0; i < NA; i++)
@@ -104,12 +141,10 @@ __device__ __forceinline__ void influence_point(int method, int m, int cao, int 
       for (int j = 0; j < NA; j++) {
         const double S2 = Sx[i] * Sy[j];
         const double Exy = Ex[i] * Ey[j];
+        const double Q2 = Qx[i] + Qy[j];
 #pragma unroll
-        for (int k = 0; k < NA; k++) {
-          const double a = Nx[i] * Leni, b = Ny[j] * Leni, cc = Nz[k] * Leni;
-          const double NM2 = a * a + b * b + cc * cc;
-          term(S2 * Sz[k], Nx[i], Ny[j], Nz[k], NM2, Exy * Ez[k], ((i + j + k - 3 * MC) % 2) == 0);
-        }
+        for (int k = 0; k < NA; k++)
+          term(S2 * Sz[k], Lx[i], Ly[j], Lz[k], Q2 + Qz[k], Exy * Ez[k], ((i + j + k - 3 * MC) % 2) == 0);
       }
   } else {
     for (int MX = -mc; MX <= mc; MX++) {
@@ -126,7 +161,7 @@ __device__ __forceinline__ void influence_point(int method, int m, int cao, int 
           const double S3 = S2 * (ik_sq ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao));
           const double a = NMX * Leni, b = NMY * Leni, cc = NMZ * Leni;
           const double NM2 = a * a + b * b + cc * cc;
-          term(S3, NMX, NMY, NMZ, NM2, exp(-fak2 * NM2), ((MX + MY + MZ) % 2) == 0);
+          term(S3, a, b, cc, NM2, exp(-fak2 * NM2), ((MX + MY + MZ) % 2) == 0);
         }
       }
     }
@@ -162,7 +197,8 @@ __device__ __forceinline__ void influence_point(int method, int m, int cao, int 
 // through launch_influence, which picks it from mc).
 template <int MC>
 __global__ void influence_kernel(double *__restrict__ G, int method, int m, int cao, int mc, double alpha_v,
-                                 const double *__restrict__ alphas, double L, double *__restrict__ dG) {
+                                 const double *__restrict__ alphas, double L, double *__restrict__ dG,
+                                 const double *__restrict__ A, const double *__restrict__ E) {
   const size_t M = (size_t)m * m * m;
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ind >= M) return;
@@ -190,7 +226,8 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
     return;
   }
   double g, dg;
-  influence_point<MC>(method, m, cao, mc, alpha, L, NX, NY, NZ, dG != nullptr, &g, &dg);
+  influence_point<MC>(method, m, cao, mc, alpha, L, NX, NY, NZ, dG != nullptr, &g, &dg, A,
+                      E ? E + (size_t)blockIdx.y * m * (2 * mc + 1) : nullptr);
   G[ind] = g;
   if (dG) dG[ind] = dg;
 }
@@ -202,7 +239,8 @@ __global__ void influence_kernel(double *__restrict__ G, int method, int m, int 
 // evaluated per alpha.  Same zeroing and final formula as influence_point.
 template <int MC, int AB>
 __global__ void influence_group_kernel(double *__restrict__ G, int method, int m, int cao,
-                                       const double *__restrict__ alphas, int na, double L) {
+                                       const double *__restrict__ alphas, int na, double L,
+                                       const double *__restrict__ A, const double *__restrict__ E) {
   const size_t M = (size_t)m * m * m;
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (ind >= M) return;
@@ -218,35 +256,33 @@ __global__ void influence_group_kernel(double *__restrict__ G, int method, int m
     for (int a = 0; a < nag; a++) G[(size_t)(a0 + a) * M + ind] = 0.0;
     return;
   }
-  const bool ik_sq = (method == 0 || method == 6);
-  const double Leni = 1.0 / L, fak1 = 1.0 / (double)m;
+  const double Leni = 1.0 / L;
   const double nx = signed_freq(NX, m), ny = signed_freq(NY, m), nz = signed_freq(NZ, m);
   constexpr int NA = 2 * MC + 1;
-  double Nx[NA], Ny[NA], Nz[NA], Sx[NA], Sy[NA], Sz[NA];
+  // the per-axis factors from influence_axis_kernel's tables
+  double Lx[NA], Ly[NA], Lz[NA], Qx[NA], Qy[NA], Qz[NA], Sx[NA], Sy[NA], Sz[NA];
 #pragma unroll
   for (int i = 0; i < NA; i++) {
-    const double shift = (double)(m * (i - MC));
-    Nx[i] = nx + shift;
-    Ny[i] = ny + shift;
-    Nz[i] = nz + shift;
-    const double sx = sinc_pi(fak1 * Nx[i]), sy = sinc_pi(fak1 * Ny[i]), sz = sinc_pi(fak1 * Nz[i]);
-    Sx[i] = ik_sq ? ipow_d(ipow_d(sx, cao), 2) : ipow_d(sx, 2 * cao);
-    Sy[i] = ik_sq ? ipow_d(ipow_d(sy, cao), 2) : ipow_d(sy, 2 * cao);
-    Sz[i] = ik_sq ? ipow_d(ipow_d(sz, cao), 2) : ipow_d(sz, 2 * cao);
+    const double *ax = A + 3 * (NX * NA + i), *ay = A + 3 * (NY * NA + i), *az = A + 3 * (NZ * NA + i);
+    Sx[i] = ax[0];
+    Lx[i] = ax[1];
+    Qx[i] = ax[2];
+    Sy[i] = ay[0];
+    Ly[i] = ay[1];
+    Qy[i] = ay[2];
+    Sz[i] = az[0];
+    Lz[i] = az[1];
+    Qz[i] = az[2];
   }
-  double fak2[AB];
   double Ex[AB][NA], Ey[AB][NA], Ez[AB][NA];
 #pragma unroll
   for (int a = 0; a < AB; a++) {
-    const double alpha = a < nag ? alphas[a0 + a] : 1.0;
-    const double pa = P3MG_PI / alpha;
-    fak2[a] = pa * pa;
+    const double *Eg = E + (size_t)(a < nag ? a0 + a : a0) * m * NA;
 #pragma unroll
     for (int i = 0; i < NA; i++) {
-      const double x = Nx[i] * Leni, y = Ny[i] * Leni, z = Nz[i] * Leni;
-      Ex[a][i] = exp(-fak2[a] * (x * x));
-      Ey[a][i] = exp(-fak2[a] * (y * y));
-      Ez[a][i] = exp(-fak2[a] * (z * z));
+      Ex[a][i] = Eg[NX * NA + i];
+      Ey[a][i] = Eg[NY * NA + i];
+      Ez[a][i] = Eg[NZ * NA + i];
     }
   }
   double N1 = 0.0, N2 = 0.0, N3 = 0.0, N4 = 0.0;
@@ -261,8 +297,7 @@ __global__ void influence_group_kernel(double *__restrict__ G, int method, int m
 #pragma unroll
       for (int k = 0; k < NA; k++) {
         const double S3 = S2 * Sz[k];
-        const double a_ = Nx[i] * Leni, b_ = Ny[j] * Leni, c_ = Nz[k] * Leni;
-        const double NM2 = a_ * a_ + b_ * b_ + c_ * c_;
+        const double NM2 = Qx[i] + Qy[j] + Qz[k];
         const bool even = ((i + j + k - 3 * MC) % 2) == 0;
         N1 += S3;
         if (ad) {
@@ -277,9 +312,9 @@ __global__ void influence_group_kernel(double *__restrict__ G, int method, int m
 #pragma unroll
           for (int a = 0; a < AB; a++) {
             const double zwi = w * (Ex[a][i] * Ey[a][j] * Ez[a][k]);
-            Zx[a] += Nx[i] * zwi * Leni;
-            Zy[a] += Ny[j] * zwi * Leni;
-            Zz[a] += Nz[k] * zwi * Leni;
+            Zx[a] += Lx[i] * zwi;
+            Zy[a] += Ly[j] * zwi;
+            Zz[a] += Lz[k] * zwi;
           }
         }
       }
@@ -318,14 +353,43 @@ constexpr int influence_ab(int mc) { return mc >= 2 ? 2 : 4; }
 
 // G (and dG) for grid (blocks, na) on the stream
 void launch_influence(double *G, int method, int m, int cao, int mc, double alpha, const double *alphas, double L,
-                      double *dG, unsigned blocks, int na, int threads, cudaStream_t st) {
+                      double *dG, unsigned blocks, int na, int threads, cudaStream_t st, const double *A,
+                      const double *E) {
   const dim3 grid(blocks, na);
   switch (mc) {
-    case 0: influence_kernel<0><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
-    case 1: influence_kernel<1><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
-    case 2: influence_kernel<2><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
-    default: influence_kernel<-1><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG); break;
+    case 0: influence_kernel<0><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG, A, E); break;
+    case 1: influence_kernel<1><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG, A, E); break;
+    case 2: influence_kernel<2><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG, A, E); break;
+    default:
+      influence_kernel<-1><<<grid, threads, 0, st>>>(G, method, m, cao, mc, alpha, alphas, L, dG, nullptr, nullptr);
+      break;
   }
+}
+
+// The per-axis tables of influence_axis_kernel for mc <= 2 and na alphas
+// (alphas on the device, or the single alpha_v) in the context's table
+// buffer; *A = *E = nullptr for larger mc (evaluated alias by alias).
+int influence_tables(Ctx *c, const double *alphas, double alpha_v, int na, const double **A, const double **E) {
+  *A = *E = nullptr;
+  if (c->mc > 2) return P3MG_OK;
+  const int m = c->mesh, NA = 2 * c->mc + 1;
+  const size_t need = (size_t)m * NA * (3 + (size_t)na);
+  if (need > c->infl_cap) {
+    if (c->infl_tab) cudaFree(c->infl_tab);
+    c->infl_tab = nullptr;
+    c->infl_cap = 0;
+    P3MG_CUDA_TRY(cudaMalloc(&c->infl_tab, need * sizeof(double)));
+    c->infl_cap = need;
+  }
+  const int tot = m * NA * (na + 1);
+  const int threads = 256;
+  influence_axis_kernel<<<(tot + threads - 1) / threads, threads, 0, c->stream>>>(
+      c->infl_tab, c->infl_tab + (size_t)3 * m * NA, c->method, m, c->cao, c->mc, c->L, alphas, alpha_v, na);
+  c->launches++;
+  P3MG_CUDA_TRY(cudaGetLastError());
+  *A = c->infl_tab;
+  *E = c->infl_tab + (size_t)3 * m * NA;
+  return P3MG_OK;
 }
 
 // ad self-force sums S(m') for the 26 non-zero m' in {-1,0,1}^3
@@ -434,21 +498,23 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
+  const double *A = nullptr, *E = nullptr;
+  P3MG_TRY(influence_tables(c, d_alphas, 0.0, na, &A, &E));
   if (na > 1 && c->mc <= 2) {
     const int ab = influence_ab(c->mc);
     const dim3 grid(blocks, (na + ab - 1) / ab);
     if (c->mc == 0)
       influence_group_kernel<0, influence_ab(0)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
-                                                                                 d_alphas, na, c->L);
+                                                                                 d_alphas, na, c->L, A, E);
     else if (c->mc == 1)
       influence_group_kernel<1, influence_ab(1)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
-                                                                                 d_alphas, na, c->L);
+                                                                                 d_alphas, na, c->L, A, E);
     else
       influence_group_kernel<2, influence_ab(2)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
-                                                                                 d_alphas, na, c->L);
+                                                                                 d_alphas, na, c->L, A, E);
   } else {
     launch_influence(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas, c->L, nullptr, blocks, na, threads,
-                     c->stream);
+                     c->stream, A, E);
   }
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
@@ -469,8 +535,10 @@ int influence_with_derivative(Ctx *c, double *G_out, double *dG_out) {
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
+  const double *A = nullptr, *E = nullptr;
+  P3MG_TRY(influence_tables(c, nullptr, c->alpha, 1, &A, &E));
   launch_influence(G_out, c->method, c->mesh, c->cao, c->mc, c->alpha, nullptr, c->L, dG_out, blocks, 1, threads,
-                   c->stream);
+                   c->stream, A, E);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
@@ -481,7 +549,10 @@ int influence_compute(Ctx *c, double alpha) {
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
-  launch_influence(c->G, c->method, m, c->cao, c->mc, alpha, nullptr, c->L, nullptr, blocks, 1, threads, c->stream);
+  const double *A = nullptr, *E = nullptr;
+  P3MG_TRY(influence_tables(c, nullptr, alpha, 1, &A, &E));
+  launch_influence(c->G, c->method, m, c->cao, c->mc, alpha, nullptr, c->L, nullptr, blocks, 1, threads, c->stream, A,
+                   E);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   if (c->precision != P3MG_FP64) {

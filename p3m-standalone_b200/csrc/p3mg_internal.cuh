@@ -162,6 +162,9 @@ struct Ctx {
   // alpha and box length adj_G / adj_dG were computed for (-1: none yet)
   double adj_key_alpha = -1.0, adj_key_L = -1.0;
   double *sweep_rms2 = nullptr;  // the last sweep's squared errors per alpha (device, in its workspace)
+  // per-axis alias tables of G_opt (influence_tables), kept between calls
+  double *infl_tab = nullptr;
+  size_t infl_cap = 0;
   void *adj_phi = nullptr;
   int adj_cap = 0;
   size_t sweep_cap = 0;
