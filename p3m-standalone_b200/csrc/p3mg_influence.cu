@@ -193,43 +193,59 @@ __device__ __forceinline__ void influence_point(int method, int m, int cao, int 
   *dg_out = dg;
 }
 
+// G_opt is even along each axis, G(.., m - i, ..) = G(.., i, ..), for even
+// meshes and for the ad methods (the alias set and the formulas are
+// symmetric; for odd meshes the ik zeroing of the indices that are 0 mod
+// m / 2 is not).  The kernels then evaluate only the folded points, indices
+// 0 .. m / 2 on each axis, and write each value to its up to 8 mirror images.
+__host__ __device__ inline bool influence_folds(int method, int m) { return (m % 2) == 0 || method_ad(method); }
+__host__ __device__ inline int influence_extent(int method, int m) {
+  return influence_folds(method, m) ? m / 2 + 1 : m;
+}
+
+// v to the mirror images (NX or m - NX, ...) of a folded point (one write
+// without folding)
+__device__ __forceinline__ void influence_put(double *__restrict__ G, int m, bool fold, int NX, int NY, int NZ,
+                                              double v) {
+  const int nx = (fold && NX != 0 && 2 * NX != m) ? 2 : 1;
+  const int ny = (fold && NY != 0 && 2 * NY != m) ? 2 : 1;
+  const int nz = (fold && NZ != 0 && 2 * NZ != m) ? 2 : 1;
+  for (int sx = 0; sx < nx; sx++)
+    for (int sy = 0; sy < ny; sy++)
+      for (int sz = 0; sz < nz; sz++) {
+        const int X = sx ? m - NX : NX, Y = sy ? m - NY : NY, Z = sz ? m - NZ : NZ;
+        G[((size_t)X * m + Y) * m + Z] = v;
+      }
+}
+
 // dG (may be NULL): dG/dalpha as well.  MC: see influence_point (launch
-// through launch_influence, which picks it from mc).
+// through launch_influence, which picks it from mc).  Threads cover the
+// points of influence_extent per axis.
 template <int MC>
 __global__ void influence_kernel(double *__restrict__ G, int method, int m, int cao, int mc, double alpha_v,
                                  const double *__restrict__ alphas, double L, double *__restrict__ dG,
                                  const double *__restrict__ A, const double *__restrict__ E) {
   const size_t M = (size_t)m * m * m;
+  const bool fold = influence_folds(method, m);
+  const int h = influence_extent(method, m);
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ind >= M) return;
+  if (ind >= (size_t)h * h * h) return;
   // alpha batch: grid.y = alpha index (alphas on the device), G of entry y
   const double alpha = alphas ? alphas[blockIdx.y] : alpha_v;
   G += (size_t)blockIdx.y * M;
-  const int NZ = (int)(ind % m);
-  const int NY = (int)((ind / m) % m);
-  const int NX = (int)(ind / ((size_t)m * m));
+  const int NZ = (int)(ind % h);
+  const int NY = (int)((ind / h) % h);
+  const int NX = (int)(ind / ((size_t)h * h));
   const int half = m / 2;
-  if ((NX | NY | NZ) == 0) {
-    G[ind] = 0.0;
-    if (dG) dG[ind] = 0.0;
-    return;
-  }
   const bool ad = method_ad(method);
-  if (ad && alpha == 0.0) {
-    G[ind] = 0.0;
-    if (dG) dG[ind] = 0.0;
-    return;
-  }
-  if (!ad && (NX % half == 0) && (NY % half == 0) && (NZ % half == 0)) {
-    G[ind] = 0.0;
-    if (dG) dG[ind] = 0.0;
-    return;
-  }
-  double g, dg;
-  influence_point<MC>(method, m, cao, mc, alpha, L, NX, NY, NZ, dG != nullptr, &g, &dg, A,
-                      E ? E + (size_t)blockIdx.y * m * (2 * mc + 1) : nullptr);
-  G[ind] = g;
-  if (dG) dG[ind] = dg;
+  double g = 0.0, dg = 0.0;
+  const bool zero = ((NX | NY | NZ) == 0) || (ad && alpha == 0.0) ||
+                    (!ad && (NX % half == 0) && (NY % half == 0) && (NZ % half == 0));
+  if (!zero)
+    influence_point<MC>(method, m, cao, mc, alpha, L, NX, NY, NZ, dG != nullptr, &g, &dg, A,
+                        E ? E + (size_t)blockIdx.y * m * (2 * mc + 1) : nullptr);
+  influence_put(G, m, fold, NX, NY, NZ, g);
+  if (dG) influence_put(dG, m, fold, NX, NY, NZ, dg);
 }
 
 // G_opt for a group of AB alphas per thread (alpha batches, mc <= 2):
@@ -242,18 +258,20 @@ __global__ void influence_group_kernel(double *__restrict__ G, int method, int m
                                        const double *__restrict__ alphas, int na, double L,
                                        const double *__restrict__ A, const double *__restrict__ E) {
   const size_t M = (size_t)m * m * m;
+  const bool fold = influence_folds(method, m);
+  const int h = influence_extent(method, m);
   const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (ind >= M) return;
+  if (ind >= (size_t)h * h * h) return;
   const int a0 = blockIdx.y * AB;
   const int nag = min(AB, na - a0);
-  const int NZ = (int)(ind % m);
-  const int NY = (int)((ind / m) % m);
-  const int NX = (int)(ind / ((size_t)m * m));
+  const int NZ = (int)(ind % h);
+  const int NY = (int)((ind / h) % h);
+  const int NX = (int)(ind / ((size_t)h * h));
   const int half = m / 2;
   const bool ad = method_ad(method);
   const bool zero_all = ((NX | NY | NZ) == 0) || (!ad && (NX % half == 0) && (NY % half == 0) && (NZ % half == 0));
   if (zero_all) {
-    for (int a = 0; a < nag; a++) G[(size_t)(a0 + a) * M + ind] = 0.0;
+    for (int a = 0; a < nag; a++) influence_put(G + (size_t)(a0 + a) * M, m, fold, NX, NY, NZ, 0.0);
     return;
   }
   const double Leni = 1.0 / L;
@@ -344,7 +362,7 @@ __global__ void influence_group_kernel(double *__restrict__ G, int method, int m
       }
       g = 2.0 * num / P3MG_PI;
     }
-    G[(size_t)(a0 + a) * M + ind] = g;
+    influence_put(G + (size_t)(a0 + a) * M, m, fold, NX, NY, NZ, g);
   }
 }
 
@@ -498,11 +516,13 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
   const size_t M = c->M;
   const int threads = 256;
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
+  const size_t h = (size_t)influence_extent(c->method, m);
+  const unsigned gblocks = (unsigned)((h * h * h + threads - 1) / threads);
   const double *A = nullptr, *E = nullptr;
   P3MG_TRY(influence_tables(c, d_alphas, 0.0, na, &A, &E));
   if (na > 1 && c->mc <= 2) {
     const int ab = influence_ab(c->mc);
-    const dim3 grid(blocks, (na + ab - 1) / ab);
+    const dim3 grid(gblocks, (na + ab - 1) / ab);
     if (c->mc == 0)
       influence_group_kernel<0, influence_ab(0)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
                                                                                  d_alphas, na, c->L, A, E);
@@ -513,7 +533,7 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
       influence_group_kernel<2, influence_ab(2)><<<grid, threads, 0, c->stream>>>(G_all, c->method, m, c->cao,
                                                                                  d_alphas, na, c->L, A, E);
   } else {
-    launch_influence(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas, c->L, nullptr, blocks, na, threads,
+    launch_influence(G_all, c->method, m, c->cao, c->mc, 0.0, d_alphas, c->L, nullptr, gblocks, na, threads,
                      c->stream, A, E);
   }
   c->launches++;
@@ -532,12 +552,12 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
 
 // G and dG/dalpha at the context's alpha into G_out / dG_out (M doubles each).
 int influence_with_derivative(Ctx *c, double *G_out, double *dG_out) {
-  const size_t M = c->M;
   const int threads = 256;
-  const unsigned blocks = (unsigned)((M + threads - 1) / threads);
+  const size_t h = (size_t)influence_extent(c->method, c->mesh);
+  const unsigned gblocks = (unsigned)((h * h * h + threads - 1) / threads);
   const double *A = nullptr, *E = nullptr;
   P3MG_TRY(influence_tables(c, nullptr, c->alpha, 1, &A, &E));
-  launch_influence(G_out, c->method, c->mesh, c->cao, c->mc, c->alpha, nullptr, c->L, dG_out, blocks, 1, threads,
+  launch_influence(G_out, c->method, c->mesh, c->cao, c->mc, c->alpha, nullptr, c->L, dG_out, gblocks, 1, threads,
                    c->stream, A, E);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
@@ -551,7 +571,9 @@ int influence_compute(Ctx *c, double alpha) {
   const unsigned blocks = (unsigned)((M + threads - 1) / threads);
   const double *A = nullptr, *E = nullptr;
   P3MG_TRY(influence_tables(c, nullptr, alpha, 1, &A, &E));
-  launch_influence(c->G, c->method, m, c->cao, c->mc, alpha, nullptr, c->L, nullptr, blocks, 1, threads, c->stream, A,
+  const size_t h = (size_t)influence_extent(c->method, m);
+  const unsigned gblocks = (unsigned)((h * h * h + threads - 1) / threads);
+  launch_influence(c->G, c->method, m, c->cao, c->mc, alpha, nullptr, c->L, nullptr, gblocks, 1, threads, c->stream, A,
                    E);
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
