@@ -138,6 +138,7 @@ int free_all(Ctx *c) {
   c->adj_cap = 0;
   dfree(c->infl_tab);
   c->infl_cap = 0;
+  dfree(c->self_R);
   fft_plan_free(c);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   c->gexec = nullptr;

@@ -410,6 +410,7 @@ int influence_tables(Ctx *c, const double *alphas, double alpha_v, int na, const
   return P3MG_OK;
 }
 
+
 // ad self-force sums S(m') for the 26 non-zero m' in {-1,0,1}^3
 // (p3m-ad-self-forces.c:30-91):
 //   S(m') = sum_{k: G(k) != 0} sum_{a in {-1,0,1}^3} G(k) U(k + a m) U(k + (a + m') m),
@@ -419,52 +420,73 @@ int influence_tables(Ctx *c, const double *alphas, double alpha_v, int na, const
 //   sum_a U(k + a m) U(k + (a + m') m) = T_x(m'_x) T_y(m'_y) T_z(m'_z),
 //   T_d(p) = sum_{a = -1..1} u_d[a] u_d[a + p],  p in {-1, 0, 1},
 // nine products per axis and two per m' instead of 27 x 26 triple products.
-// Block reduction, then one FP64 atomic per sum.
-__global__ void self_force_sum_kernel(const double *__restrict__ G, int m, int cao, double *__restrict__ S26) {
+// G is even along each axis (ad methods) and mirroring an index turns
+// T(p) into T(-p), so the sum runs over the folded points (indices 0 .. m/2)
+// with the per-axis factor R(p) = T(p) + T(-p) for an index with a distinct
+// mirror image (T(p) otherwise): self_axis_kernel tabulates R per index.
+__global__ void self_axis_kernel(double *__restrict__ R, int m, int cao) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > m / 2) return;
+  // sinc(x + j) = (-1)^j sin(pi x) / (pi (x + j)), x = k / m: one sine for
+  // the five alias offsets j = -2..2
+  const double x = (double)(int)signed_freq(i, m) / (double)m;
+  const double s0 = sin(P3MG_PI * x);
+  double u[5];
+#pragma unroll
+  for (int c = 0; c < 5; c++) {
+    const double dj = x + (double)(c - 2);
+    const double sc = (dj == 0.0) ? 1.0 : ((c & 1) ? -s0 : s0) / (P3MG_PI * dj);
+    u[c] = ipow_d(sc, cao);
+  }
+  double T[3];
+#pragma unroll
+  for (int p = -1; p <= 1; p++) T[p + 1] = u[1] * u[1 + p] + u[2] * u[2 + p] + u[3] * u[3 + p];
+  const bool pair = (i != 0 && 2 * i != m);
+#pragma unroll
+  for (int p = 0; p < 3; p++) R[3 * i + p] = pair ? T[p] + T[2 - p] : T[p];
+}
+
+// Block reduction of the per-thread sums (each thread takes SELF_PTS folded
+// points), then one FP64 atomic per sum.
+constexpr int SELF_PTS = 8;
+
+__global__ void self_force_sum_kernel(const double *__restrict__ G, const double *__restrict__ R, int m,
+                                      double *__restrict__ S26) {
   __shared__ double red[26][8];
   const size_t M = (size_t)m * m * m;
-  const size_t ind = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int h = m / 2 + 1;
+  const size_t H = (size_t)h * h * h;
   G += (size_t)blockIdx.y * M;  // alpha batch (grid.y)
   S26 += 26 * blockIdx.y;
   double acc[26];
 #pragma unroll
   for (int t = 0; t < 26; t++) acc[t] = 0.0;
-  if (ind < M) {
-    const double g = G[ind];
-    if (g != 0.0) {
-      const int nz = (int)(ind % m), ny = (int)((ind / m) % m), nx = (int)(ind / ((size_t)m * m));
-      const int tk[3] = {(int)signed_freq(nx, m), (int)signed_freq(ny, m), (int)signed_freq(nz, m)};
-      const double mi = 1.0 / m;
-      double T[3][3];
+  const size_t first = ((size_t)blockIdx.x * SELF_PTS) * blockDim.x + threadIdx.x;
+  for (int it = 0; it < SELF_PTS; it++) {
+    const size_t ind = first + (size_t)it * blockDim.x;
+    if (ind >= H) break;
+    const int nz = (int)(ind % h), ny = (int)((ind / h) % h), nx = (int)(ind / ((size_t)h * h));
+    const double g = G[((size_t)nx * m + ny) * m + nz];
+    if (g == 0.0) continue;
+    double Tx[3], Ty[3], Tz[3];
 #pragma unroll
-      for (int d = 0; d < 3; d++) {
-        // sinc(x + j) = (-1)^j sin(pi x) / (pi (x + j)), x = k_d / m: one
-        // sine per axis for the five alias offsets j = -2..2
-        const double x = mi * (double)tk[d];
-        const double s0 = sin(P3MG_PI * x);
-        double u[5];
-#pragma unroll
-        for (int c = 0; c < 5; c++) {
-          const double dj = x + (double)(c - 2);
-          const double sc = (dj == 0.0) ? 1.0 : ((c & 1) ? -s0 : s0) / (P3MG_PI * dj);
-          u[c] = ipow_d(sc, cao);
-        }
-#pragma unroll
-        for (int p = -1; p <= 1; p++) T[d][p + 1] = u[1] * u[1 + p] + u[2] * u[2 + p] + u[3] * u[3 + p];
-      }
-      int t = 0;
-#pragma unroll
-      for (int px = 0; px < 3; px++)
-#pragma unroll
-        for (int py = 0; py < 3; py++) {
-          const double gxy = g * (T[0][px] * T[1][py]);
-#pragma unroll
-          for (int pz = 0; pz < 3; pz++) {
-            if (px == 1 && py == 1 && pz == 1) continue;
-            acc[t++] += gxy * T[2][pz];
-          }
-        }
+    for (int p = 0; p < 3; p++) {
+      Tx[p] = R[3 * nx + p];
+      Ty[p] = R[3 * ny + p];
+      Tz[p] = R[3 * nz + p];
     }
+    int t = 0;
+#pragma unroll
+    for (int px = 0; px < 3; px++)
+#pragma unroll
+      for (int py = 0; py < 3; py++) {
+        const double gxy = g * (Tx[px] * Ty[py]);
+#pragma unroll
+        for (int pz = 0; pz < 3; pz++) {
+          if (px == 1 && py == 1 && pz == 1) continue;
+          acc[t++] += gxy * Tz[pz];
+        }
+      }
   }
   // warp reduce then across the (up to 8) warps of the block
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -505,6 +527,23 @@ __global__ void self_coeff_kernel(const double *__restrict__ S26, const double *
 
 }  // namespace
 
+// The self-force sums of na G meshes (G_all, M apart) into S26 (26 na
+// doubles, zeroed here): per-axis factors (self_axis_kernel) into the
+// context's small table, then the folded sum.
+int self_force_sums(Ctx *c, const double *G_all, int na, double *S26) {
+  const int m = c->mesh, h = m / 2 + 1;
+  if (!c->self_R) P3MG_CUDA_TRY(cudaMalloc(&c->self_R, 3 * (P3MG_MAX_MESH / 2 + 1) * sizeof(double)));
+  self_axis_kernel<<<(h + 127) / 128, 128, 0, c->stream>>>(c->self_R, m, c->cao);
+  P3MG_CUDA_TRY(cudaMemsetAsync(S26, 0, 26 * (size_t)na * sizeof(double), c->stream));
+  const int threads = 256;
+  const size_t H = (size_t)h * h * h;
+  const unsigned blocks = (unsigned)((H + (size_t)threads * SELF_PTS - 1) / ((size_t)threads * SELF_PTS));
+  self_force_sum_kernel<<<dim3(blocks, na), threads, 0, c->stream>>>(G_all, c->self_R, m, S26);
+  c->launches += 2;
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
 // G_opt (and for methods 2 and 7 the self-force coefficients) for na alphas
 // at once: G_all holds na meshes, b81_all 81 coefficients per alpha, S26
 // is 26 na doubles of scratch.  For mc <= 2 groups of alphas share the
@@ -539,10 +578,9 @@ int influence_batch(Ctx *c, const double *d_alphas, int na, double *G_all, doubl
   c->launches++;
   P3MG_CUDA_TRY(cudaGetLastError());
   if (method_self_force(c->method)) {
-    P3MG_CUDA_TRY(cudaMemsetAsync(S26, 0, 26 * (size_t)na * sizeof(double), c->stream));
-    self_force_sum_kernel<<<dim3(blocks, na), threads, 0, c->stream>>>(G_all, m, c->cao, S26);
+    P3MG_TRY(self_force_sums(c, G_all, na, S26));
     self_coeff_kernel<<<dim3(1, na), 96, 0, c->stream>>>(S26, d_alphas, m, c->L, b81_all);
-    c->launches += 2;
+    c->launches++;
     P3MG_CUDA_TRY(cudaGetLastError());
   } else {
     P3MG_CUDA_TRY(cudaMemsetAsync(b81_all, 0, 81 * (size_t)na * sizeof(double), c->stream));
@@ -586,10 +624,7 @@ int influence_compute(Ctx *c, double alpha) {
   // self-force initialisation (p3m-ad.c:120-123); keep zeros then
   if (method_self_force(c->method) && alpha != 0.0) {
     double *S26 = c->self_b;  // use the first 26 slots as the accumulator
-    P3MG_CUDA_TRY(cudaMemsetAsync(S26, 0, 26 * sizeof(double), c->stream));
-    self_force_sum_kernel<<<blocks, threads, 0, c->stream>>>(c->G, m, c->cao, S26);
-    c->launches++;
-    P3MG_CUDA_TRY(cudaGetLastError());
+    P3MG_TRY(self_force_sums(c, c->G, 1, S26));
     double S[26];
     P3MG_CUDA_TRY(cudaMemcpyAsync(S, S26, sizeof(S), cudaMemcpyDeviceToHost, c->stream));
     P3MG_CUDA_TRY(cudaStreamSynchronize(c->stream));

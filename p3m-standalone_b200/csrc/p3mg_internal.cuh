@@ -165,6 +165,7 @@ struct Ctx {
   // per-axis alias tables of G_opt (influence_tables), kept between calls
   double *infl_tab = nullptr;
   size_t infl_cap = 0;
+  double *self_R = nullptr;  // per-axis factors of the ad self-force sums
   void *adj_phi = nullptr;
   int adj_cap = 0;
   size_t sweep_cap = 0;
