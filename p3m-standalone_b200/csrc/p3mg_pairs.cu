@@ -726,7 +726,9 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
         auto test_push = [&](int kk, bool valid) {
           const float4 pj = cf[valid ? kk : 0];
           const float dx = pif.x - pj.x, dy = pif.y - pj.y, dz = pif.z - pj.z;
-          const bool ok = valid & (dx * dx + dy * dy + dz * dz <= rc2f) & (N3 ? kk > kself : kk != kself);
+          // N3 (only the pruned columns): the own column starts past i's
+          // own slot, so every candidate comes after it
+          const bool ok = valid & (dx * dx + dy * dy + dz * dz <= rc2f) & (N3 || kk != kself);
           const unsigned mask = __ballot_sync(0xffffffffu, ok);
           if (ok) q[(tail + __popc(mask & ((1u << lane) - 1u))) & (PAIR_QCAP - 1)] = (unsigned short)kk;
           tail += __popc(mask);
@@ -757,7 +759,10 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_cell_kernel(const void *__rest
               if (lo <= hi) {
                 const int base = (J0 + 2) * 36 + (J1 + 2) * 6 + 2;
                 ca = seg_pre[base + lo];
-                clen = seg_pre[base + hi + 1] - ca;
+                const int ce = seg_pre[base + hi + 1];
+                // Newton-3: i's own column from the slot after its own
+                if (N3 && lane == 12) ca = max(ca, kself + 1);
+                clen = max(ce - ca, 0);
               }
             }
           }
