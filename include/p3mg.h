@@ -379,6 +379,14 @@ int p3mg_kernel_times(p3mg_ctx *ctx, double t[3]);
  * disables it.  No reference counterpart (the reference is single-threaded C). */
 int p3mg_set_graph(p3mg_ctx *ctx, int on);
 
+/* Concurrency of a step's two halves (no reference counterpart): on (the
+ * default), p3mg_compute runs the real-space pairs on a second stream beside
+ * the k-space chain; off, the pairs run first on the context stream and the
+ * k-space chain after them, so each kernel has the GPU to itself (what
+ * p3mg_kernel_times then reports is each kernel's own duration).  The
+ * forces are the same either way. */
+int p3mg_set_overlap(p3mg_ctx *ctx, int on);
+
 /* Real-space erfc pair forces that allocate no device memory.
  * No counterpart in the reference.
  * For callers that cannot let a library allocate GPU memory: an engine

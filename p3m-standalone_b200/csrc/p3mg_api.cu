@@ -184,7 +184,7 @@ static int enqueue_step(Ctx *c, double rcut) {
     // brackets of stages that may not run this step must still be recorded
     for (int s = EV_K0; s <= EV_K5; s++) cudaEventRecord(c->ev[s], c->stream);
   }
-  const bool overlap = rcut != 0.0 && c->n > 0 && c->stream2;
+  const bool overlap = rcut != 0.0 && c->n > 0 && c->stream2 && c->overlap;
   mark(c, EV_S0);
   int st = P3MG_OK;
   if (overlap) {
@@ -591,6 +591,13 @@ int p3mg_set_graph(p3mg_ctx *h, int on) {
   if (!h) return P3MG_ERR_ARG;
   h->c.use_graph = on != 0;
   if (!h->c.use_graph) drop_graph(&h->c);
+  return P3MG_OK;
+}
+
+int p3mg_set_overlap(p3mg_ctx *h, int on) {
+  if (!h) return P3MG_ERR_ARG;
+  drop_graph(&h->c);
+  h->c.overlap = on != 0;
   return P3MG_OK;
 }
 

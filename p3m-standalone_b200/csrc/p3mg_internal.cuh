@@ -71,6 +71,7 @@ struct Ctx {
   // second stream of a step: the real-space pairs run on it beside the
   // k-space chain (fork / join events on the context stream)
   cudaStream_t stream2 = nullptr;
+  bool overlap = true;  // the pairs on stream2 beside the k-space chain (p3mg_set_overlap)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
   // particles

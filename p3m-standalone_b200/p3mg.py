@@ -123,6 +123,7 @@ def load():
     L.p3mg_error_map.argtypes = [vp, ctypes.c_int, ctypes.c_int] + [_dp] * 8
     L.p3mg_kernel_times.argtypes = [vp, _dp]
     L.p3mg_set_graph.argtypes = [vp, ctypes.c_int]
+    L.p3mg_set_overlap.argtypes = [vp, ctypes.c_int]
     L.p3mg_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.p3mg_stream.argtypes = [vp]
     L.p3mg_stream.restype = vp
@@ -390,6 +391,10 @@ class Context:
 
     def set_graph(self, on=True):
         _check(self._lib.p3mg_set_graph(self._h, int(bool(on))), "p3mg_set_graph")
+
+    def set_overlap(self, on=True):
+        """Real-space pairs beside the k-space chain (True, the default) or before it."""
+        _check(self._lib.p3mg_set_overlap(self._h, int(bool(on))), "p3mg_set_overlap")
 
     def launch_count(self):
         c = ctypes.c_longlong(0)

@@ -88,3 +88,26 @@ def test_realspace_bruteforce_branch(gpu):
         fr, e = ctx.real_forces(rcut, alpha)
     assert O.rel_rms(fr, fr_ref) <= TOL_FP64
     assert abs(e - e_ref) <= 1e-10 * abs(e_ref)
+
+
+@pytest.mark.parametrize("precision", [p3mg.FP64, p3mg.FP32_MIXED])
+def test_overlap_switch_keeps_forces(gpu, precision):
+    # the pairs beside the k-space chain (default) or before it
+    # (p3mg_set_overlap): the same forces, up to the order of the atomics;
+    # the FP64 step still matches the oracle
+    method, mesh, cao, mc, alpha, rcut, n, L = (1, 32, 7, 1, 0.9, 3.5, 20000, 20000 ** (1.0 / 3.0))
+    x, y, z, q = p3mg.generate_system(0, n, L, seed=21)
+    with p3mg.Context(method, mesh, cao, mc, precision) as ctx:
+        ctx.set_system(x, y, z, q, L)
+        ctx.influence(alpha)
+        ctx.enable_timing(True)
+        on = ctx.calculate_forces(rcut)
+        ctx.set_overlap(False)
+        off = ctx.calculate_forces(rcut)
+        kt = ctx.kernel_times()
+        ctx.set_overlap(True)
+    assert O.rel_rms(off["f"], on["f"]) <= (1e-14 if precision == p3mg.FP64 else 1e-6)
+    assert all(v > 0.0 for v in kt.values())
+    if precision == p3mg.FP64:
+        ref = O.forces(method, mesh, cao, mc, alpha, rcut, x, y, z, q, L, cells=True)
+        assert O.rel_rms(off["f"], ref["f"]) <= TOL_FP64
