@@ -747,13 +747,10 @@ inline int scatter_row_pitch(int cao, int T, int word_bytes) {
 template <typename real, int CAO, int NMESH, bool EXACT = false>
 int launch_scatter(Ctx *c, size_t smem, int SR, int SP) {
   auto kern = scatter_kernel<real, CAO, NMESH, EXACT>;
-  // raise the dynamic shared-memory limit once per instantiation (outside
-  // any graph capture: the first step of a shape always runs eagerly)
-  static size_t smem_set = 0;
-  if (smem > smem_set) {
-    P3MG_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    smem_set = 200 * 1024;
-  }
+  // raise the dynamic shared-memory limit once per instantiation and device
+  // (outside any graph capture: the first step of a shape always runs eagerly)
+  static std::atomic<int> smem_set[P3MG_MAX_DEVICES];
+  P3MG_CUDA_TRY(raise_smem_limit(kern, (int)(smem > 200 * 1024 ? smem : 200 * 1024), smem_set));
   const double Hi = (double)c->mesh / c->L;
   const double shift = (double)((c->cao - 1) / 2);
   const int nbr = c->nbrick1 * c->nbrick1 * c->nbrick1;

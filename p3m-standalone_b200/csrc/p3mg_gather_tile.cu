@@ -359,12 +359,8 @@ int launch_tile(Ctx *c, const void *Fv, double *fk, int na, double pref, bool tm
   const int TZ = gt_row_pitch(T, CAO);
   const size_t smem = gt_smem_bytes(B, CAO, NMESH);
   if (smem > 227 * 1024 || T > 16) return P3MG_ERR_ARG;
-  static size_t attr = 0;
-  if (smem > attr) {
-    P3MG_CUDA_TRY(cudaFuncSetAttribute(gather_tile_kernel<CAO, NMESH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-    attr = smem;
-  }
+  static std::atomic<int> smem_set[P3MG_MAX_DEVICES];
+  P3MG_CUDA_TRY(raise_smem_limit(gather_tile_kernel<CAO, NMESH>, (int)smem, smem_set));
   CUtensorMap tmap;
   memset(&tmap, 0, sizeof(tmap));
   int use_tma = 0;

@@ -6,6 +6,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <atomic>
+
 #include "../../include/p3mg.h"
 
 #define P3MG_PI 3.14159265358979323846264338327950288
@@ -36,6 +38,23 @@ void record_cuda_error(cudaError_t e);
     int s_ = (expr);        \
     if (s_ != P3MG_OK) return s_; \
   } while (0)
+
+// Dynamic shared-memory limit of a kernel, raised to at least `bytes` once
+// per device: the attribute belongs to each device's copy of the kernel, so a
+// process that drives several GPUs sets it on each.  `cache` (one slot per
+// device, zero-initialised static storage) holds the value set; host threads
+// racing here set the same value, and the atomic slots keep that defined.
+constexpr int P3MG_MAX_DEVICES = 64;
+template <typename T>
+inline cudaError_t raise_smem_limit(T *kernel, int bytes, std::atomic<int> *cache) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < P3MG_MAX_DEVICES && cache[dev].load(std::memory_order_relaxed) >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess && dev >= 0 && dev < P3MG_MAX_DEVICES) cache[dev].store(bytes, std::memory_order_relaxed);
+  return e;
+}
 
 // ------------------------------------------------------------ method traits
 __host__ __device__ inline bool method_interlaced(int m) { return m == 1 || m == 3; }

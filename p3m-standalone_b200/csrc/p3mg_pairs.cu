@@ -958,13 +958,9 @@ __global__ void __launch_bounds__(PAIR_CTA) dense_units_kernel(const float4 *__r
 template <bool DBL, int NA>
 int launch_cells_na(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
                     const double *alphas, int nalpha, double *fr, int n, double *energy, cudaStream_t s) {
-  static bool attr_set = false;
+  static std::atomic<int> smem_set[P3MG_MAX_DEVICES];
   const size_t smem = pair_smem_bytes(DBL, NA);
-  if (!attr_set) {
-    P3MG_CUDA_TRY(
-        cudaFuncSetAttribute(pairs_cell_kernel<DBL, NA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
+  P3MG_CUDA_TRY(raise_smem_limit(pairs_cell_kernel<DBL, NA>, (int)smem, smem_set));
   const int groups = alphas ? (nalpha + NA - 1) / NA : 1;
   const dim3 grid(nc * nc * nc, groups);
   pairs_cell_kernel<DBL, NA><<<grid, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr,
@@ -978,13 +974,9 @@ int launch_cells_na(const void *pos, const int *sidx, const int *start, int nc, 
 template <bool DBL>
 int launch_cells_adj(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
                      double *gx, double *gq, double ge, int n, double *sums, cudaStream_t s) {
-  static bool attr_set = false;
+  static std::atomic<int> smem_set[P3MG_MAX_DEVICES];
   const size_t smem = pair_smem_bytes(DBL, 1, true);
-  if (!attr_set) {
-    P3MG_CUDA_TRY(cudaFuncSetAttribute(pairs_cell_kernel<DBL, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-    attr_set = true;
-  }
+  P3MG_CUDA_TRY(raise_smem_limit(pairs_cell_kernel<DBL, 1, true>, (int)smem, smem_set));
   pairs_cell_kernel<DBL, 1, true><<<nc * nc * nc, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, nullptr, 1,
                                                                       gx, n, sums, gq, ge);
   P3MG_CUDA_TRY(cudaGetLastError());
@@ -998,14 +990,10 @@ int launch_cells_adj(const void *pos, const int *sidx, const int *start, int nc,
 int launch_cells_units(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut, double alpha,
                        const double *alphas, double *fr, int n, double *energy, int2 *units, int *counters,
                        cudaStream_t s) {
-  static bool attr_set = false;
+  static std::atomic<int> smem_set[P3MG_MAX_DEVICES], units_smem_set[P3MG_MAX_DEVICES];
   const size_t smem = pair_smem_bytes(false, 1);
-  if (!attr_set) {
-    P3MG_CUDA_TRY(
-        cudaFuncSetAttribute(pairs_cell_kernel<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    P3MG_CUDA_TRY(cudaFuncSetAttribute(dense_units_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
+  P3MG_CUDA_TRY(raise_smem_limit(pairs_cell_kernel<false, 1>, (int)smem, smem_set));
+  P3MG_CUDA_TRY(raise_smem_limit(dense_units_kernel, (int)smem, units_smem_set));
   pairs_cell_kernel<false, 1><<<nc * nc * nc, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, 1, fr,
                                                                   n, energy, nullptr, 0.0, units, counters);
   P3MG_CUDA_TRY(cudaGetLastError());
