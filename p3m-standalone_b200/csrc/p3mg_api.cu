@@ -498,7 +498,7 @@ int p3mg_kspace_forces(p3mg_ctx *h, double *fk_x, double *fk_y, double *fk_z, do
   collect_stage_times(c);
   P3MG_TRY(copy_out3(c, c->fk, fk_x, fk_y, fk_z, true));
   if (method_self_force(c->method) && (ft_x || ft_y || ft_z)) P3MG_TRY(copy_out3(c, c->f, ft_x, ft_y, ft_z, true));
-  return P3MG_OK;
+  return check_device_status(c);
 }
 
 int p3mg_real_forces(p3mg_ctx *h, double rcut, double alpha, double *fr_x, double *fr_y, double *fr_z,
@@ -709,7 +709,8 @@ extern "C" int p3mg_sweep(p3mg_ctx *h, double rcut, int nalpha, const double *al
     const size_t b = (size_t)max_batch * sweep_bytes_per_alpha(c);
     if (b < budget) budget = b;
   }
-  return sweep_run(c, rcut, nalpha, alphas, want_ref ? ref : nullptr, rms_out, f_out, budget, max_batch > 0);
+  P3MG_TRY(sweep_run(c, rcut, nalpha, alphas, want_ref ? ref : nullptr, rms_out, f_out, budget, max_batch > 0));
+  return check_device_status(c);
 }
 
 extern "C" int p3mg_sweep_grid(p3mg_ctx *const *hs, int nctx, double rcut, int nalpha, const double *alphas,
@@ -739,7 +740,9 @@ extern "C" int p3mg_sweep_grid(p3mg_ctx *const *hs, int nctx, double rcut, int n
   size_t budget = free_b / 2;
   const size_t cap = (size_t)32 << 30;
   if (budget > cap) budget = cap;
-  return sweep_grid_run(cs.data(), nctx, rcut, nalpha, alphas, ref, rms_out, budget);
+  P3MG_TRY(sweep_grid_run(cs.data(), nctx, rcut, nalpha, alphas, ref, rms_out, budget));
+  for (int i = 0; i < nctx; i++) P3MG_TRY(check_device_status(cs[i]));
+  return P3MG_OK;
 }
 
 extern "C" int p3mg_sweep_nodes(p3mg_ctx *h, int *nodes, double *check) {
@@ -1158,6 +1161,7 @@ extern "C" int p3mg_batch_synchronize(p3mg_batch *b) {
   if (!b) return P3MG_ERR_ARG;
   cudaSetDevice(b->device);
   P3MG_CUDA_TRY(cudaStreamSynchronize(b->stream));
+  for (p3mg_ctx *h : b->ctx) P3MG_TRY(check_device_status(&h->c));
   return P3MG_OK;
 }
 
