@@ -1005,10 +1005,270 @@ int launch_cells_units(const void *pos, const int *sidx, const int *start, int n
   return P3MG_OK;
 }
 
+// FP32 alpha sweeps over many alphas: lanes on alphas instead of pairs.
+// The alpha-group form of pairs_cell_kernel runs the candidate search once
+// per group of PAIR_NA32 alphas and keeps a force sum per alpha of the group
+// in every lane (119 registers).  Here one warp per particle i runs the
+// search once for up to PAIR_LA alphas; the lane that queued a pair forms
+// its geometry once (r, q_i q_j / r^3 d, q_i q_j / (2 r)) and the warp
+// broadcasts it, and lane l evaluates erfc and the Gaussian term for alphas
+// l and l + 32, summing i's force for them in its own registers -- no sum
+// across lanes, and i's forces go straight to the alphas' force rows.  Every
+// ordered pair (no Newton's third law), the staging and the column search of
+// pairs_cell_kernel's FP32 path.
+constexpr int PAIR_LA = 64;      // alphas per CTA (two per lane)
+constexpr int PAIR_LA_MIN = 17;  // fewer alphas: the alpha-group kernel
+
+__host__ __device__ constexpr size_t pair_la_smem_bytes() {
+  return (size_t)PAIR_JCH * sizeof(float4) + (size_t)PAIR_MAXI32 * sizeof(float4) +
+         (size_t)PAIR_WARPS * PAIR_QCAP * sizeof(unsigned short);
+}
+
+__global__ void __launch_bounds__(PAIR_CTA) pairs_alpha_lanes_kernel(const float4 *__restrict__ pos32,
+                                                                      const int *__restrict__ sidx,
+                                                                      const int *__restrict__ start, int nc, double L,
+                                                                      double rcut, const double *__restrict__ alphas,
+                                                                      int nalpha, double *__restrict__ fr, int n,
+                                                                      double *__restrict__ energy) {
+  // grid.y = group of PAIR_LA alphas; alpha a of the group: forces at
+  // fr + 3 n a, energy at energy[a]
+  const int a0 = blockIdx.y * PAIR_LA;
+  const int nag = min(PAIR_LA, nalpha - a0);
+  fr += (size_t)a0 * 3 * (size_t)n;
+  energy += a0;
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  float4 *cf = reinterpret_cast<float4 *>(pair_smem);  // staged candidates
+  float4 *spi = cf + PAIR_JCH;                          // the i batch
+  unsigned short *queue = reinterpret_cast<unsigned short *>(spi + PAIR_MAXI32);
+  __shared__ int seg_src[PAIR_NSEG], seg_pre[PAIR_NSEG + 1];
+  __shared__ float cell_off[27][3];
+  __shared__ double ered[PAIR_WARPS][PAIR_LA];
+  __shared__ int own_start[9], own_seg[8], sui[PAIR_MAXI32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned short *q = queue + warp * PAIR_QCAP;
+  const int cell = blockIdx.x;
+  const int c2 = cell % nc, c1 = (cell / nc) % nc, c0 = cell / (nc * nc);
+  const double cs = L / nc;
+  if (tid < 27) {
+    // neighbour cell origin relative to this one
+    cell_off[tid][0] = (float)((tid / 9 - 1) * cs);
+    cell_off[tid][1] = (float)(((tid / 3) % 3 - 1) * cs);
+    cell_off[tid][2] = (float)((tid % 3 - 1) * cs);
+  }
+  // the 6x6x6 half-cells around the cell in grid order, J2 fastest
+  for (int sg = tid; sg < PAIR_NSEG; sg += PAIR_CTA) {
+    const int J0 = sg / 36 - 2, J1 = (sg / 6) % 6 - 2, J2 = sg % 6 - 2;
+    const int d0 = (J0 + 2) / 2 - 1, d1 = (J1 + 2) / 2 - 1, d2 = (J2 + 2) / 2 - 1;
+    const int v0 = (J0 + 2) & 1, v1 = (J1 + 2) & 1, v2 = (J2 + 2) & 1;
+    const int w0 = wrap_full(c0 + d0, nc), w1 = wrap_full(c1 + d1, nc), w2 = wrap_full(c2 + d2, nc);
+    const int key = ((w0 * nc + w1) * nc + w2) * 8 + (v0 << 2) + (v1 << 1) + v2;
+    seg_src[sg] = start[key];
+    seg_pre[sg + 1] = start[key + 1] - start[key];
+  }
+  __syncthreads();
+  {
+    __shared__ int scan_w[PAIR_WARPS];
+    scan_segments(seg_pre, scan_w);
+  }
+  const int total = seg_pre[PAIR_NSEG];
+  const bool fits = total <= PAIR_JCH;
+  const int i0 = start[cell * 8], i1 = start[cell * 8 + 8];
+  if (tid < 9) own_start[tid] = start[cell * 8 + tid];
+  if (tid < 8) own_seg[tid] = seg_pre[(2 + ((tid >> 2) & 1)) * 36 + (2 + ((tid >> 1) & 1)) * 6 + 2 + (tid & 1)];
+  // this lane's alphas: a0 + lane and a0 + lane + 32 (the second only with
+  // more than 32 alphas in the group, a warp-uniform condition)
+  const double wupi = 1.77245385090551602729816748334;
+  const bool two = nag > 32;
+  float al[2], pf[2];
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    const double av = lane + 32 * s < nag ? alphas[a0 + lane + 32 * s] : 0.0;
+    al[s] = (float)av;
+    pf[s] = (float)(2.0 * av / wupi);
+  }
+  const float rc2f = (float)rcut * (float)rcut;
+  const float hf = (float)(0.5 * cs), hinvf = (float)(2.0 / cs);
+  const float prune_r2 = (float)(rcut * rcut * (1.0 + 1e-4));
+  double e_d[2] = {0.0, 0.0};
+  for (int ib = i0; ib < i1; ib += PAIR_MAXI32) {
+    const int ni = min(PAIR_MAXI32, i1 - ib);
+    __syncthreads();
+    for (int t = tid; t < ni; t += PAIR_CTA) {
+      const int isorted = ib + t;
+      int u = 0;
+#pragma unroll
+      for (int v = 1; v < 8; v++)
+        if (isorted >= own_start[v]) u = v;
+      sui[t] = ((own_seg[u] + (isorted - own_start[u])) << 3) | u;
+      spi[t] = pos32[ib + t];
+    }
+    for (int k0 = 0; k0 < total; k0 += PAIR_JCH) {
+      const int kn = min(PAIR_JCH, total - k0);
+      __syncthreads();
+      for (int kk = tid; kk < kn; kk += PAIR_CTA) {
+        const int k = k0 + kk;
+        int sg = 0;
+#pragma unroll
+        for (int step = 128; step > 0; step >>= 1)
+          if (sg + step < PAIR_NSEG && seg_pre[sg + step] <= k) sg += step;
+        const int src = seg_src[sg] + (k - seg_pre[sg]);
+        const int cidx = ((sg / 36 / 2) * 3 + (sg / 6) % 6 / 2) * 3 + (sg % 6) / 2;
+        const float4 p = pos32[src];
+        cf[kk] = make_float4(p.x + cell_off[cidx][0], p.y + cell_off[cidx][1], p.z + cell_off[cidx][2], p.w);
+      }
+      __syncthreads();
+      for (int il = warp; il < ni; il += PAIR_WARPS) {
+        const float4 pif = spi[il];
+        const int uk = sui[il];
+        const int u = uk & 7;
+        const int kself = (uk >> 3) - k0;  // i's own staged slot in this chunk
+        float fx[2] = {0.0f, 0.0f}, fy[2] = {0.0f, 0.0f}, fz[2] = {0.0f, 0.0f}, e_p[2] = {0.0f, 0.0f};
+        unsigned head = 0, tail = 0;
+        // evaluate the first `take` queued pairs for every alpha and pop them
+        auto process = [&](int take) {
+          __syncwarp();
+          float wx = 0.0f, wy = 0.0f, wz = 0.0f, r = 0.0f, qh = 0.0f;
+          if (lane < take) {
+            const float4 pj = cf[q[(head + lane) & (PAIR_QCAP - 1)]];
+            const float ex = pif.x - pj.x, ey = pif.y - pj.y, ez = pif.z - pj.z;
+            const float rr2 = ex * ex + ey * ey + ez * ez;
+            const float rinv = rsqrtf(rr2);
+            const float qq = pif.w * pj.w;
+            const float w3 = qq * (rinv * rinv * rinv);
+            r = rr2 * rinv;
+            wx = w3 * ex;
+            wy = w3 * ey;
+            wz = w3 * ez;
+            qh = 0.5f * qq * rinv;
+          }
+          for (int p = 0; p < take; p++) {
+            const float bwx = __shfl_sync(0xffffffffu, wx, p), bwy = __shfl_sync(0xffffffffu, wy, p);
+            const float bwz = __shfl_sync(0xffffffffu, wz, p), br = __shfl_sync(0xffffffffu, r, p);
+            const float bqh = __shfl_sync(0xffffffffu, qh, p);
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+              if (s == 1 && !two) break;
+              // f = q_i q_j (erfc(a r) + 2 a / sqrt(pi) r exp(-a^2 r^2)) / r^3 d
+              const float ar = al[s] * br;
+              const float gs = __expf(-ar * ar);
+              const float ec = erfc_fit(ar, gs);
+              const float sc = fmaf(pf[s] * gs, br, ec);
+              fx[s] = fmaf(sc, bwx, fx[s]);
+              fy[s] = fmaf(sc, bwy, fy[s]);
+              fz[s] = fmaf(sc, bwz, fz[s]);
+              e_p[s] = fmaf(bqh, ec, e_p[s]);
+            }
+          }
+          head += take;
+          __syncwarp();
+        };
+        // one candidate test per lane; hits go to the warp's queue
+        auto test_push = [&](int kk, bool valid) {
+          const float4 pj = cf[valid ? kk : 0];
+          const float dx = pif.x - pj.x, dy = pif.y - pj.y, dz = pif.z - pj.z;
+          const bool ok = valid & (dx * dx + dy * dy + dz * dz <= rc2f) & (kk != kself);
+          const unsigned mask = __ballot_sync(0xffffffffu, ok);
+          if (ok) q[(tail + __popc(mask & ((1u << lane) - 1u))) & (PAIR_QCAP - 1)] = (unsigned short)kk;
+          tail += __popc(mask);
+          // at most 63 queued: one full round drains it below 32
+          if (tail - head >= 32) process(32);
+        };
+        if (fits) {
+          // lane r < 25 owns the half-cell column (U0 - 2 + r / 5, U1 - 2 +
+          // r % 5), skipped beyond rcut in xy and clipped in z to the
+          // half-cells the sphere reaches (as in pairs_cell_kernel)
+          const int U0 = (u >> 2) & 1, U1 = (u >> 1) & 1, U2 = u & 1;
+          int ca = 0, clen = 0;
+          if (lane < 25) {
+            const int J0 = U0 - 2 + lane / 5, J1 = U1 - 2 + lane % 5;
+            const float x0 = J0 * hf, y0 = J1 * hf;
+            const float ddx = fmaxf(fmaxf(x0 - pif.x, pif.x - (x0 + hf)), 0.0f);
+            const float ddy = fmaxf(fmaxf(y0 - pif.y, pif.y - (y0 + hf)), 0.0f);
+            const float d2 = ddx * ddx + ddy * ddy;
+            if (d2 <= prune_r2) {
+              const float zr = sqrtf(prune_r2 - d2);
+              const int lo = max((int)floorf((pif.z - zr) * hinvf), U2 - 2);
+              const int hi = min((int)floorf((pif.z + zr) * hinvf), U2 + 2);
+              if (lo <= hi) {
+                const int base = (J0 + 2) * 36 + (J1 + 2) * 6 + 2;
+                ca = seg_pre[base + lo];
+                clen = seg_pre[base + hi + 1] - ca;
+              }
+            }
+          }
+          // concatenate the non-empty columns (prefix of the lengths; lane t
+          // then holds the start and prefix of the t-th non-empty column)
+          int incl = clen;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+          }
+          const int ntot = __shfl_sync(0xffffffffu, incl, 31);
+          const unsigned nem = __ballot_sync(0xffffffffu, clen > 0);
+          const int excl = incl - clen;
+          const int src = (int)__fns(nem, 0, lane + 1);
+          const int colA = __shfl_sync(0xffffffffu, ca, src & 31);
+          const int colE = __shfl_sync(0xffffffffu, excl, src & 31);
+          const unsigned le = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);
+          int nbefore = 0;  // non-empty columns that start before this step
+          for (int c0s = 0; c0s < ntot; c0s += 32) {
+            const bool st = (clen > 0) & (excl >= c0s) & (excl < c0s + 32);
+            const unsigned smask = __reduce_or_sync(0xffffffffu, st ? (1u << ((excl - c0s) & 31)) : 0u);
+            const int rank = nbefore + __popc(smask & le) - 1;
+            nbefore += __popc(smask);
+            const int a = __shfl_sync(0xffffffffu, colA, rank & 31);
+            const int e = __shfl_sync(0xffffffffu, colE, rank & 31);
+            const int k = c0s + lane;
+            test_push(a + (k - e), k < ntot);
+          }
+        } else {
+          // the neighbourhood did not fit: this chunk of the flat candidate order
+          for (int jb = 0; jb < kn; jb += 32) test_push(jb + lane, jb + lane < kn);
+        }
+        if (tail != head) process((int)(tail - head));
+        // i's forces for this lane's alphas (one warp owns i: no race across
+        // chunks), its energy terms summed in FP64
+        const int o = sidx[ib + il];
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          if (lane + 32 * s < nag) {
+            double *fa = fr + (size_t)(lane + 32 * s) * 3 * (size_t)n;
+            fa[o] += (double)fx[s];
+            fa[(size_t)n + o] += (double)fy[s];
+            fa[2 * (size_t)n + o] += (double)fz[s];
+          }
+          e_d[s] += (double)e_p[s];
+        }
+      }
+    }
+  }
+  ered[warp][lane] = e_d[0];
+  ered[warp][lane + 32] = e_d[1];
+  __syncthreads();
+  if (tid < nag) {
+    double s = 0.0;
+    for (int w = 0; w < PAIR_WARPS; w++) s += ered[w][tid];
+    if (s != 0.0) atomicAdd(energy + tid, s);
+  }
+}
+
+int launch_cells_alpha_lanes(const void *pos, const int *sidx, const int *start, int nc, double L, double rcut,
+                             const double *alphas, int nalpha, double *fr, int n, double *energy, cudaStream_t s) {
+  static_assert(pair_la_smem_bytes() <= 48 * 1024, "default dynamic shared-memory limit");
+  const dim3 grid(nc * nc * nc, (nalpha + PAIR_LA - 1) / PAIR_LA);
+  pairs_alpha_lanes_kernel<<<grid, PAIR_CTA, pair_la_smem_bytes(), s>>>(
+      reinterpret_cast<const float4 *>(pos), sidx, start, nc, L, rcut, alphas, nalpha, fr, n, energy);
+  P3MG_CUDA_TRY(cudaGetLastError());
+  return P3MG_OK;
+}
+
 int launch_pairs_cells(bool dbl, const void *pos, const int *sidx, const int *start, int nc, double L, double rcut,
                        double alpha, const double *alphas, int nalpha, double *fr, int n, double *energy,
                        cudaStream_t s) {
   const bool group = alphas != nullptr && nalpha > 1;
+  if (!dbl && group && nalpha >= PAIR_LA_MIN)
+    return launch_cells_alpha_lanes(pos, sidx, start, nc, L, rcut, alphas, nalpha, fr, n, energy, s);
   if (dbl)
     return group ? launch_cells_na<true, PAIR_NA64>(pos, sidx, start, nc, L, rcut, alpha, alphas, nalpha, fr, n,
                                                      energy, s)

@@ -43,6 +43,25 @@ def test_sweep_equals_single_alpha_steps(gpu, method, precision):
                 assert O.rel_rms(sw[k].ravel(), singles[k].ravel()) <= tol, (mb, k)
 
 
+@pytest.mark.parametrize("system_type,n,L,na", [
+    (0, 600, 10.0, 20),   # one alpha per lane
+    (0, 600, 10.0, 40),   # two per lane
+    (4, 4000, 20.0, 70),  # two groups; the Gaussian centre overflows the staging array (chunked candidates)
+])
+def test_fp32_many_alpha_sweep_equals_single_alpha_steps(gpu, system_type, n, L, na):
+    # 17 or more alphas in one pass: FP32 real space with the lanes on the
+    # alphas (one candidate search for up to 64 alphas)
+    x, y, z, q = p3mg.generate_system(system_type, n, L, seed=61)
+    alphas = np.linspace(0.7, 1.6, na)
+    with p3mg.Context(1, 16, 5, 1, p3mg.FP32_MIXED) as ctx:
+        ctx.set_system(x, y, z, q, L)
+        sw = ctx.sweep(2.8, alphas, want_forces=True, max_batch=na)["forces"]
+        for k in sorted({0, 31, 32, 33, na // 2, 63, 64, na - 1} & set(range(na))):
+            ctx.influence(alphas[k])
+            one = ctx.calculate_forces(2.8)["f"]
+            assert O.rel_rms(sw[k].ravel(), one.ravel()) <= 1e-6, k
+
+
 def test_sweep_golden_method7_config(gpu):
     g = np.load(os.path.join(GOLD, "sweep.npz"))
     x, y, z, q, L = g["x"], g["y"], g["z"], g["q"], float(g["L"])
