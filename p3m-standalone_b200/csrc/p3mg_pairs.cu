@@ -997,10 +997,22 @@ int launch_cells_units(const void *pos, const int *sidx, const int *start, int n
   pairs_cell_kernel<false, 1><<<nc * nc * nc, PAIR_CTA, smem, s>>>(pos, sidx, start, nc, L, rcut, alpha, alphas, 1, fr,
                                                                   n, energy, nullptr, 0.0, units, counters);
   P3MG_CUDA_TRY(cudaGetLastError());
-  // persistent CTAs, four per SM (148 SMs): a dense cell's units spread
-  // over them; without dense cells each returns after one load
-  dense_units_kernel<<<148 * 4, PAIR_CTA, smem, s>>>(reinterpret_cast<const float4 *>(pos), sidx, start, nc, L, rcut,
-                                                     alphas, alpha, fr, n, energy, units, counters, counters + 1);
+  // persistent CTAs, as many as the device holds at once (7 per SM on a
+  // B200: shared memory), counted once per device: a dense cell's units
+  // spread over them; without dense cells each returns after one load
+  static std::atomic<int> units_grid[P3MG_MAX_DEVICES];
+  int dev = 0;
+  P3MG_CUDA_TRY(cudaGetDevice(&dev));
+  int grid = (dev >= 0 && dev < P3MG_MAX_DEVICES) ? units_grid[dev].load() : 0;
+  if (grid <= 0) {
+    int per_sm = 0, sms = 0;
+    P3MG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dense_units_kernel, PAIR_CTA, smem));
+    P3MG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    grid = std::max(per_sm, 1) * std::max(sms, 1);
+    if (dev >= 0 && dev < P3MG_MAX_DEVICES) units_grid[dev].store(grid);
+  }
+  dense_units_kernel<<<grid, PAIR_CTA, smem, s>>>(reinterpret_cast<const float4 *>(pos), sidx, start, nc, L, rcut,
+                                                  alphas, alpha, fr, n, energy, units, counters, counters + 1);
   P3MG_CUDA_TRY(cudaGetLastError());
   return P3MG_OK;
 }
