@@ -683,9 +683,14 @@ def secondary_workloads(dev):
         ctxs.append(cg)
     p3mg.sweep_grid(ctxs, 3.0, al, ref)  # warm-up: workspaces, lane tables
     torch.cuda.synchronize()
-    t_all = time.perf_counter()
-    rms = p3mg.sweep_grid(ctxs, 3.0, al, ref)
-    grid_ms = (time.perf_counter() - t_all) * 1e3
+    # best of three calls: one call's host clock includes whatever else the
+    # host does meanwhile (single calls ranged 24-120 ms on shared machines)
+    grid_calls = []
+    for _ in range(3):
+        t_all = time.perf_counter()
+        rms = p3mg.sweep_grid(ctxs, 3.0, al, ref)
+        grid_calls.append((time.perf_counter() - t_all) * 1e3)
+    grid_ms = min(grid_calls)
     for cg in ctxs:
         cg.close()
     i, k = np.unravel_index(int(np.argmin(rms)), rms.shape)
@@ -694,7 +699,8 @@ def secondary_workloads(dev):
     best = (float(rms[i, k]), mesh, cao, float(al[k]), est)
     out["tuning_grid_slab_20k"] = {
         "points": 4 * 5 * 64, "grid_ms": round(grid_ms, 2),
-        "timing": "host clock around one p3mg_sweep_grid call (synchronises the device)",
+        "grid_calls_ms": [round(v, 2) for v in grid_calls],
+        "timing": "host clock around each of three p3mg_sweep_grid calls (each synchronises the device), the best",
         "best": {"rms_error": best[0], "mesh": best[1], "cao": best[2], "alpha": best[3], "estimate": best[4]}}
     return out
 
