@@ -1023,13 +1023,16 @@ int launch_cells_units(const void *pos, const int *sidx, const int *start, int n
 // in every lane (119 registers).  Here one warp per particle i runs the
 // search once for up to PAIR_LA alphas; the lane that queued a pair forms
 // its geometry once (r, q_i q_j / r^3 d, q_i q_j / (2 r)) and the warp
-// broadcasts it, and lane l evaluates erfc and the Gaussian term for alphas
-// l and l + 32, summing i's force for them in its own registers -- no sum
-// across lanes, and i's forces go straight to the alphas' force rows.  Every
-// ordered pair (no Newton's third law), the staging and the column search of
-// pairs_cell_kernel's FP32 path.
-constexpr int PAIR_LA = 64;      // alphas per CTA (two per lane)
-constexpr int PAIR_LA_MIN = 17;  // fewer alphas: the alpha-group kernel
+// broadcasts it, and each lane evaluates erfc and the Gaussian term for its
+// own alphas, summing i's force for them in its own registers.  A group of
+// more than 32 alphas takes alphas l and l + 32 on lane l; a smaller one is
+// rounded up to A = 8, 16 or 32 lanes per pair, so that a step evaluates
+// 32 / A pairs (lane = pair * A + alpha) and the sub-groups' sums are
+// folded once per particle.  i's forces go straight to the alphas' force
+// rows.  Every ordered pair (no Newton's third law), the staging and the
+// column search of pairs_cell_kernel's FP32 path.
+constexpr int PAIR_LA = 64;     // alphas per CTA (at most two per lane)
+constexpr int PAIR_LA_MIN = 9;  // fewer alphas: one group of the alpha-group kernel
 
 __host__ __device__ constexpr size_t pair_la_smem_bytes() {
   return (size_t)PAIR_JCH * sizeof(float4) + (size_t)PAIR_MAXI32 * sizeof(float4) +
@@ -1087,14 +1090,17 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_alpha_lanes_kernel(const float
   const int i0 = start[cell * 8], i1 = start[cell * 8 + 8];
   if (tid < 9) own_start[tid] = start[cell * 8 + tid];
   if (tid < 8) own_seg[tid] = seg_pre[(2 + ((tid >> 2) & 1)) * 36 + (2 + ((tid >> 1) & 1)) * 6 + 2 + (tid & 1)];
-  // this lane's alphas: a0 + lane and a0 + lane + 32 (the second only with
-  // more than 32 alphas in the group, a warp-uniform condition)
+  // lanes per pair A = 2^lgA and this lane's alphas: a0 + la and, with more
+  // than 32 alphas in the group (A = 32), a0 + la + 32; sub = the pair of a
+  // step this lane takes (all warp-uniform but sub and la)
   const double wupi = 1.77245385090551602729816748334;
   const bool two = nag > 32;
+  const int lgA = nag > 16 ? 5 : nag > 8 ? 4 : 3;
+  const int sub = lane >> lgA, la = lane & ((1 << lgA) - 1);
   float al[2], pf[2];
 #pragma unroll
   for (int s = 0; s < 2; s++) {
-    const double av = lane + 32 * s < nag ? alphas[a0 + lane + 32 * s] : 0.0;
+    const double av = la + 32 * s < nag ? alphas[a0 + la + 32 * s] : 0.0;
     al[s] = (float)av;
     pf[s] = (float)(2.0 * av / wupi);
   }
@@ -1153,10 +1159,14 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_alpha_lanes_kernel(const float
             wz = w3 * ez;
             qh = 0.5f * qq * rinv;
           }
-          for (int p = 0; p < take; p++) {
-            const float bwx = __shfl_sync(0xffffffffu, wx, p), bwy = __shfl_sync(0xffffffffu, wy, p);
-            const float bwz = __shfl_sync(0xffffffffu, wz, p), br = __shfl_sync(0xffffffffu, r, p);
-            const float bqh = __shfl_sync(0xffffffffu, qh, p);
+          for (int p = 0; p < take; p += 32 >> lgA) {
+            // pair p + sub of this step (src & 31: the shuffles run on every
+            // lane; a lane past the queued pairs discards what it receives)
+            const int src = p + sub;
+            const float bwx = __shfl_sync(0xffffffffu, wx, src & 31), bwy = __shfl_sync(0xffffffffu, wy, src & 31);
+            const float bwz = __shfl_sync(0xffffffffu, wz, src & 31), br = __shfl_sync(0xffffffffu, r, src & 31);
+            const float bqh = __shfl_sync(0xffffffffu, qh, src & 31);
+            if (src >= take) continue;
 #pragma unroll
             for (int s = 0; s < 2; s++) {
               if (s == 1 && !two) break;
@@ -1239,18 +1249,28 @@ __global__ void __launch_bounds__(PAIR_CTA) pairs_alpha_lanes_kernel(const float
           for (int jb = 0; jb < kn; jb += 32) test_push(jb + lane, jb + lane < kn);
         }
         if (tail != head) process((int)(tail - head));
+        // fewer than 32 lanes per pair: fold the sub-groups' sums of each
+        // alpha into the lanes of sub-group 0
+        for (int o = 1 << lgA; o < 32; o <<= 1) {
+          fx[0] += __shfl_xor_sync(0xffffffffu, fx[0], o);
+          fy[0] += __shfl_xor_sync(0xffffffffu, fy[0], o);
+          fz[0] += __shfl_xor_sync(0xffffffffu, fz[0], o);
+          e_p[0] += __shfl_xor_sync(0xffffffffu, e_p[0], o);
+        }
         // i's forces for this lane's alphas (one warp owns i: no race across
         // chunks), its energy terms summed in FP64
         const int o = sidx[ib + il];
+        if (sub == 0) {
 #pragma unroll
-        for (int s = 0; s < 2; s++) {
-          if (lane + 32 * s < nag) {
-            double *fa = fr + (size_t)(lane + 32 * s) * 3 * (size_t)n;
-            fa[o] += (double)fx[s];
-            fa[(size_t)n + o] += (double)fy[s];
-            fa[2 * (size_t)n + o] += (double)fz[s];
+          for (int s = 0; s < 2; s++) {
+            if (la + 32 * s < nag) {
+              double *fa = fr + (size_t)(la + 32 * s) * 3 * (size_t)n;
+              fa[o] += (double)fx[s];
+              fa[(size_t)n + o] += (double)fy[s];
+              fa[2 * (size_t)n + o] += (double)fz[s];
+            }
+            e_d[s] += (double)e_p[s];
           }
-          e_d[s] += (double)e_p[s];
         }
       }
     }

@@ -44,12 +44,14 @@ def test_sweep_equals_single_alpha_steps(gpu, method, precision):
 
 
 @pytest.mark.parametrize("system_type,n,L,na", [
+    (0, 600, 10.0, 9),    # 16 lanes per pair, two pairs per step
+    (0, 600, 10.0, 12),
     (0, 600, 10.0, 20),   # one alpha per lane
     (0, 600, 10.0, 40),   # two per lane
-    (4, 4000, 20.0, 70),  # two groups; the Gaussian centre overflows the staging array (chunked candidates)
+    (4, 4000, 20.0, 70),  # two groups (64 + 6: 8 lanes per pair); the Gaussian centre overflows the staging array
 ])
 def test_fp32_many_alpha_sweep_equals_single_alpha_steps(gpu, system_type, n, L, na):
-    # 17 or more alphas in one pass: FP32 real space with the lanes on the
+    # 9 or more alphas in one pass: FP32 real space with the lanes on the
     # alphas (one candidate search for up to 64 alphas)
     x, y, z, q = p3mg.generate_system(system_type, n, L, seed=61)
     alphas = np.linspace(0.7, 1.6, na)
