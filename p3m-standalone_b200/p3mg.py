@@ -291,7 +291,10 @@ class Context:
 
     def sweep(self, rcut, alphas, ref=None, want_forces=False, max_batch=0):
         """Batched alpha sweep (p3mg_sweep): dict rms (per alpha, when ref (3, n)
-        is given) and forces (nalpha, 3, n) when want_forces."""
+        is given) and forces (nalpha, 3, n) when want_forces; nodes (> 0: the
+        forces were interpolated from that many Chebyshev nodes in 1/alpha^2)
+        and check.  max_batch 0 lets a wide enough sweep interpolate; max_batch
+        > 0 evaluates every alpha, at most max_batch of them in one pass."""
         al = np.ascontiguousarray(alphas, dtype=np.float64)
         na = len(al)
         rms = np.zeros(na) if ref is not None else None
